@@ -1,0 +1,361 @@
+"""Benchmark of the plain stable m-way partition on B200.
+
+Workload (one "step" = one partition of one synthetic batch resident in HBM):
+plain mdiscr, N = 2^28 int32 values uniform over [0, 2^31) from a seeded
+generator, m = 8, class = value mod 8 (Mod8: value & 7), stable; outputs the
+permuted array and the 8 class sizes.  Inputs (1 GiB) and outputs (1 GiB) are
+larger than the 126 MB L2, so no flush is needed between steps.
+
+Printed JSON (rank 0, one line):
+  value      elements/s over all ranks, kernels only, inputs resident in HBM
+  e2e        the same metric through the public API with pinned host buffers:
+             host->device copy of the input, the partition, device->host copy
+             of the output and sizes, all inside the timed region
+  roofline   the partition call against the HBM roofline of reading and
+             writing each element once (2*N*4 + 4*m bytes), and each of its
+             two kernels against its own algorithmic bytes
+  cpu_baseline  the reference's OpenmpMdiscr (compiled from its sources,
+             oracle/_ref) on a bounded sample, on this host's cores
+
+--impl reference runs the reference's own CPU implementation (OpenmpMdiscr)
+instead, on rank 0 only, with every host thread, on bounded samples of the
+same workload.
+
+Multi-GPU (torchrun, one process per GPU): every rank partitions its own
+N = 2^28 array (independent units, no data-path collective; weak scaling);
+the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_DEFAULT = 1 << 28
+M_DEFAULT = 8
+WORKLOAD = "plain mdiscr int32 N=2^28 uniform[0,2^31) m=8 (class = v mod 8)"
+METRIC = "Gelem/s & % HBM roofline (N=2^28, m=8)"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy burst)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def traffic_from_profiles():
+    """DRAM bytes per call of the two kernels from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "plain_partition_n2p28_m8_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            if ":" in line and line.split(":")[0].strip() in ("count_kernel_bytes",
+                                                              "scatter_kernel_bytes"):
+                k, v = line.split(":", 1)
+                try:
+                    out[k.strip()] = float(v.split()[0])
+                except ValueError:
+                    pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_input(torch, n, seed, device):
+    g = torch.Generator(device=device).manual_seed(seed)
+    return torch.randint(0, 1 << 31, (n,), device=device, dtype=torch.int64,
+                         generator=g).to(torch.int32)
+
+
+def cpu_baseline(n_sample: int, m: int, reps: int):
+    """The reference's openmpMdiscr on a bounded sample (rank 0, N=1 only)."""
+    import numpy as np
+
+    import oracle
+    if not oracle.ref_available():
+        return None, "oracle/_ref not built"
+    x = oracle.fill_uniform_u32(n_sample, 7)
+    threads = os.cpu_count() or 1
+    best = None
+    for _ in range(reps):
+        _, _, us = oracle.ref_openmp(x, m, threads=threads)
+        if us > 0 and (best is None or us < best):
+            best = us
+    if best is None:
+        return None, "reference run failed"
+    return {"value": n_sample / (best * 1e-6) / 1e9, "unit": "Gelem/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"openmpMdiscr (cuda_code/OpenmpMdiscr.h) on {n_sample} uniform int32, m={m}, "
+                      f"best of {reps}, its own gettimeofday timer, OMP threads={threads}"}, None
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's "
+                          "OpenmpMdiscr build) is missing"}))
+        return 0
+    n_sample = args.ref_sample
+    x = oracle.fill_uniform_u32(n_sample, 7)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.ref_openmp(x, args.m, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        _, _, us = oracle.ref_openmp(x, args.m, threads=threads)
+        times.append(us * 1e-6)
+    t = statistics.mean(times)
+    value = n_sample / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gelem/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": args.n, "m": args.m,
+                   "sample_per_step": n_sample, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "Gelem/s", "cores": threads, "kind": "reference",
+                         "sample": f"openmpMdiscr on {n_sample} of the workload's elements per step"},
+        "e2e": {"value": value, "unit": "Gelem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mdx", choices=["mdx", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--m", type=int, default=M_DEFAULT)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-sample", type=int, default=1 << 25)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import mdiscriminator_b200 as mdx
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    n, m = args.n, args.m
+    discr = ("mask", m) if (m & (m - 1)) == 0 else ("mod", m)
+    d_in = make_input(torch, n, 1234 + rank, dev)
+    d_out = torch.empty_like(d_in)
+    sizes = torch.empty(m, dtype=torch.uint32, device=dev)
+    ws = mdx.new_workspace(mdx.workspace_size(n, mdx.ELEM_U32, m), dev)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for _ in range(args.warmup):
+        mdx.partition(d_in, discr, out=d_out, sizes=sizes, ws=ws)
+    barrier()
+
+    # timed region: K partitions, events on the launching stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        mdx.partition(d_in, discr, out=d_out, sizes=sizes, ws=ws, count_done_event=ev[i][1])
+        ev[i][2].record(stream)
+    t_end.record(stream)
+    barrier()
+    clk = clocks.stop()
+    total_s = t_start.elapsed_time(t_end) * 1e-3
+    if world > 1:
+        tt = torch.tensor([total_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_s = float(tt.item())
+    err = ws.error()
+    if err != mdx.MDX_OK:
+        raise SystemExit(f"device error during the timed region: {mdx.strerror(err)}")
+    step_s = total_s / args.steps
+    count_ms = [a.elapsed_time(b) for a, b, _ in ev]
+    scat_ms = [b.elapsed_time(c) for _, b, c in ev]
+    call_ms = [a.elapsed_time(c) for a, _, c in ev]
+    value = world * n / step_s / 1e9
+
+    # end to end through the public API: pinned host in -> partition -> host out
+    h_in = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    h_in.copy_(d_in)
+    h_out = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    h_sizes = torch.empty(m, dtype=torch.uint32, pin_memory=True)
+    d_in2 = torch.empty_like(d_in)
+    for _ in range(2):
+        d_in2.copy_(h_in, non_blocking=True)
+        mdx.partition(d_in2, discr, out=d_out, sizes=sizes, ws=ws)
+        h_out.copy_(d_out, non_blocking=True)
+        h_sizes.copy_(sizes, non_blocking=True)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        d_in2.copy_(h_in, non_blocking=True)
+        mdx.partition(d_in2, discr, out=d_out, sizes=sizes, ws=ws)
+        h_out.copy_(d_out, non_blocking=True)
+        h_sizes.copy_(sizes, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_s = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_value = world * n * args.e2e_steps / e2e_s / 1e9
+    # sanity: the last result equals the device result of the same input
+    assert torch.equal(h_out.to(dev), d_out)
+
+    if rank == 0:
+        peak, peak_src = peaks()
+        call_s = statistics.mean(call_ms) * 1e-3
+        alg = 2 * n * 4 + 4 * m
+        achieved = alg / call_s / 1e9
+        cnt_s = statistics.mean(count_ms) * 1e-3
+        sct_s = statistics.mean(scat_ms) * 1e-3
+        tr = traffic_from_profiles()
+        traffic = (tr["count_kernel_bytes"] + tr["scatter_kernel_bytes"]) if len(tr) == 2 else None
+        roofline = {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "peak_source": peak_src,
+            "what": "one partition call (count + scatter kernels) against 2*N*4 + 4*m bytes",
+            "frac_of_two_pass_bound": (3 * n * 4 + 4 * m) / call_s / 1e9 / peak,
+            "kernels": {
+                "count": {"ms": cnt_s * 1e3, "alg_bytes": n * 4,
+                          "achieved_gbs": n * 4 / cnt_s / 1e9,
+                          "frac": n * 4 / cnt_s / 1e9 / peak,
+                          "traffic": tr.get("count_kernel_bytes")},
+                "scatter": {"ms": sct_s * 1e3, "alg_bytes": 2 * n * 4,
+                            "achieved_gbs": 2 * n * 4 / sct_s / 1e9,
+                            "frac": 2 * n * 4 / sct_s / 1e9 / peak,
+                            "traffic": tr.get("scatter_kernel_bytes")},
+            },
+        }
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu, why = cpu_baseline(args.ref_sample, m, reps=3)
+            if cpu is None:
+                cpu = {"value": None, "unavailable": why}
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gelem/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": n, "m": m, "discr": f"{discr[0]} {m}",
+                       "l2": "inputs and outputs (1 GiB each) larger than L2; no flush",
+                       "parallelism": f"independent arrays per rank x{world}" if world > 1
+                       else "single GPU"},
+            "e2e": {"value": e2e_value, "unit": "Gelem/s", "h2d_bytes_per_step": n * 4,
+                    "d2h_bytes_per_step": n * 4 + m * 4},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": 2 * args.steps,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,153 @@
+/*
+ * mdx.h -- C ABI of the B200-native m-discriminator (stable m-way partition).
+ *
+ * The operation (reference spec haskell_code/Mdiscr.hs:9-54, CPU ground truth
+ * cuda_code/SeqMdiscr.h:10-57): every element maps to a class in [0, m); the
+ * output holds all class-0 elements, then all class-1 elements, ..., each class
+ * in input order, plus the m class sizes.
+ *
+ * Every entry point is asynchronous on the given stream, never calls exit(),
+ * never allocates device memory per call (the caller passes a workspace sized
+ * by mdx_workspace_size and initialised once by mdx_workspace_init), and
+ * returns an mdx_status.  Device-side failures (a bounded wait that ran out)
+ * are latched in the workspace and read back by mdx_workspace_error.
+ *
+ * A workspace serves one call at a time: calls that share a workspace must be
+ * ordered (same stream, or synchronised).
+ */
+#ifndef MDX_H
+#define MDX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* mdx_stream_t; /* == cudaStream_t; NULL = legacy default stream */
+
+typedef enum {
+    MDX_OK = 0,
+    MDX_ERR_INVALID = 1,     /* bad argument (null pointer, m out of range, n too large, ...) */
+    MDX_ERR_WORKSPACE = 2,   /* workspace too small or misaligned */
+    MDX_ERR_CUDA = 3,        /* a CUDA runtime call failed (launch, copy, attribute query) */
+    MDX_ERR_TIMEOUT = 4,     /* a device-side bounded wait ran out (latched in the workspace) */
+    MDX_ERR_UNSUPPORTED = 5, /* valid request this build does not handle */
+    MDX_ERR_SEGMENTS = 6     /* malformed segment description */
+} mdx_status;
+
+/* Element layouts.  U32: one unsigned 32-bit value, class from the value
+ * (InType = unsigned int of Mod4/Mod8/Mod<N>, HelpersCommon.h:587-596,840-849,
+ * 1200-1210).  REC8: 8-byte record {u32 key; u32 payload}, class from the key
+ * (ModArray<N,2>, MdiscrHost_arrays.cu.h:26-36 with LEN = 2). */
+typedef enum { MDX_ELEM_U32 = 0, MDX_ELEM_REC8 = 1 } mdx_elem;
+
+/* Discriminator families.  MOD: class = key % m (Mod<N>::apply,
+ * HelpersCommon.h:1207-1209).  MASK: class = key & (m-1), m a power of two
+ * (Mod4::apply / Mod8::apply, HelpersCommon.h:593-595, 846-848). */
+typedef enum { MDX_DISCR_MOD = 0, MDX_DISCR_MASK = 1 } mdx_discr_kind;
+
+typedef struct {
+    int32_t kind;    /* mdx_discr_kind */
+    uint32_t m;      /* number of classes, 1 <= m <= MDX_MAX_CLASSES (TupleType::cardinal) */
+} mdx_discr;
+
+#define MDX_MAX_CLASSES 64u
+#define MDX_MAX_ELEMS 0xFFFFFFFFull /* class sizes are u32, as the reference's TupleType */
+
+/* Bytes of workspace mdx_partition needs for n elements of `elem` with m
+ * classes.  Replaces the per-call cudaMalloc of d_tr_in / cond_res / inds_res
+ * in mdiscr (cuda_code/MdiscrHost_optimized_clean.cu.h:43-45). */
+size_t mdx_workspace_size(uint64_t n, mdx_elem elem, uint32_t m);
+
+/* Bytes of workspace the segmented entry points need. */
+size_t mdx_segmented_workspace_size(uint64_t n, uint64_t num_segments, mdx_elem elem, uint32_t m);
+
+/* Zero a freshly allocated workspace (once, before its first use). */
+mdx_status mdx_workspace_init(void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+/* Synchronise `stream`, return the latched device error of the workspace
+ * (MDX_OK or MDX_ERR_TIMEOUT) and clear it. */
+mdx_status mdx_workspace_error(void* d_ws, mdx_stream_t stream);
+
+/*
+ * Plain stable partition of n elements.  Replaces
+ *   template<class DISCR> DISCR::TupleType mdiscr(n, num_hwd_thds, d_in, d_out)
+ *     (cuda_code/MdiscrHost_optimized_clean.cu.h:9-15)
+ * and
+ *   template<class DISCR> void mdiscr(n, in, out, int* sizes)
+ *     (cuda_code/MdiscrHost_baseline.cu.h:23-28).
+ *
+ * d_in, d_out : device arrays of n elements (distinct, non-overlapping).
+ * d_sizes     : device array of m u32 -- the class sizes (tuple form); may be NULL.
+ * d_headflags : device array of n u32 -- sizes in the reference's head-flag form
+ *               (count_c at offset_c for every non-empty class, 0 elsewhere,
+ *               SeqMdiscr.h:44-49); may be NULL.
+ */
+mdx_status mdx_partition(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                         mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                         void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+/* mdx_partition that also records `ev_count_done` (a cudaEvent_t, may be
+ * NULL) on the stream between its counting and its scattering kernel, so a
+ * caller can time the two phases separately with CUDA events. */
+mdx_status mdx_partition_timed(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                               mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                               void* d_ws, size_t ws_bytes, mdx_stream_t stream,
+                               void* ev_count_done);
+
+/*
+ * Reference-shaped synchronous form of mdx_partition: returns the m class
+ * sizes on the host in h_sizes, as mdiscr<DISCR> returns its TupleType by value
+ * (MdiscrHost_optimized_clean.cu.h:149).  num_hwd_thds is accepted for
+ * signature parity and ignored (it only shaped the reference's transposed
+ * layout, MdiscrHost_optimized_clean.cu.h:24-26).
+ */
+mdx_status mdx_mdiscr(uint32_t n, uint32_t num_hwd_thds, const void* d_in, void* d_out,
+                      mdx_elem elem, mdx_discr discr, uint32_t* h_sizes,
+                      void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+/*
+ * Segmented stable partition: each segment [d_offsets[s], d_offsets[s+1]) of
+ * the n elements is partitioned independently (mdiscrSegm,
+ * cuda_code/MdiscrSegmHost.cu.h:36-42; validated per segment against seqMdiscr
+ * by MdiscrSegmTest.cu:8-41).
+ *
+ * d_offsets      : device u64[num_segments + 1], non-decreasing, [0] = 0, [S] = n.
+ * d_seg_sizes    : device u32[num_segments * m], row s = class sizes of segment s; may be NULL.
+ * d_headflags    : device u32[n] -- per-segment head-flag sizes relative to the
+ *                  segment start, the form mdiscrSegm writes into new_sizes
+ *                  (MdiscrSegmKernels.cu.h:89-114); may be NULL.
+ */
+mdx_status mdx_partition_segmented(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                   mdx_discr discr, const uint64_t* d_offsets,
+                                   uint64_t num_segments, uint32_t* d_seg_sizes,
+                                   uint32_t* d_headflags, void* d_ws, size_t ws_bytes,
+                                   mdx_stream_t stream);
+
+/*
+ * Reference-shaped segmented form with head-flag segment sizes in and out:
+ *   template<class DISCR> void mdiscrSegm(n, in, int* segment_sizes, out, int* new_sizes)
+ *     (cuda_code/MdiscrSegmHost.cu.h:36-42)
+ * d_segment_sizes: device i32[n], length of the segment at each segment start,
+ * 0 elsewhere.  d_new_sizes: device i32[n] (head-flag output).  Needs a
+ * workspace of mdx_segmented_workspace_size(n, n, elem, m) bytes (the segment
+ * count is only known on the device).  Malformed flags latch
+ * MDX_ERR_SEGMENTS in the workspace.
+ */
+mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segment_sizes,
+                           void* d_out, int32_t* d_new_sizes, mdx_elem elem, mdx_discr discr,
+                           void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+/* Human-readable text of a status. */
+const char* mdx_strerror(mdx_status s);
+
+/* Library version string, e.g. "mdx 0.1.0 sm_100a". */
+const char* mdx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDX_H */

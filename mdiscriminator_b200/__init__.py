@@ -1,0 +1,341 @@
+"""mdiscriminator_b200 -- B200-native stable m-way partition (m-discriminator).
+
+The Python layer mirrors the reference's host entry points and forwards to the
+C ABI of ``libmdx.so`` (``include/mdx.h``); torch tensors only carry device
+memory and streams.  There is no CPU fallback: if the CUDA library is missing
+or a tensor is not on a CUDA device, the call raises.
+
+Reference entry points and their counterparts here:
+
+* ``mdiscr<DISCR>(n, num_hwd_thds, d_in, d_out) -> TupleType``
+  (cuda_code/MdiscrHost_optimized_clean.cu.h:9-15)  ->  :func:`mdiscr`
+* ``mdiscr<DISCR>(n, in, out, int* sizes)`` with head-flag sizes
+  (cuda_code/MdiscrHost_baseline.cu.h:23-28)        ->  :func:`partition` (``headflags=True``)
+* ``mdiscrSegm<DISCR>(n, in, segment_sizes, out, new_sizes)``
+  (cuda_code/MdiscrSegmHost.cu.h:36-42)             ->  :func:`mdiscr_segm`,
+  and the offsets form :func:`partition_segmented`.
+
+A discriminator is ``("mod", m)`` -- ``Mod<N>::apply = x % N``
+(HelpersCommon.h:1200-1210) -- or ``("mask", m)`` -- ``Mod4``/``Mod8``
+``apply = x & (m-1)`` (HelpersCommon.h:587-596, 840-849).  4-byte elements
+are u32 values; 8-byte elements are ``{u32 key, u32 payload}`` records whose
+class comes from the key (``ModArray<N,2>``, MdiscrHost_arrays.cu.h:26-36).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from dataclasses import dataclass
+from typing import Optional, Tuple
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmdx.so")
+
+MDX_OK = 0
+MDX_ERR_INVALID = 1
+MDX_ERR_WORKSPACE = 2
+MDX_ERR_CUDA = 3
+MDX_ERR_TIMEOUT = 4
+MDX_ERR_UNSUPPORTED = 5
+MDX_ERR_SEGMENTS = 6
+
+ELEM_U32 = 0
+ELEM_REC8 = 1
+DISCR_MOD = 0
+DISCR_MASK = 1
+MAX_CLASSES = 64
+
+
+class MdxError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {strerror(status)} (status {status})" if what else strerror(status))
+
+
+class Discr(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("m", ctypes.c_uint32)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def lib() -> ctypes.CDLL:
+    """Load libmdx.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(f"{LIB_PATH} is missing: run mdiscriminator_b200.build.build()")
+            L = ctypes.CDLL(LIB_PATH)
+            vp, u64, u32, sz = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_size_t
+            st = ctypes.c_int
+            L.mdx_workspace_size.argtypes = [u64, ctypes.c_int, u32]
+            L.mdx_workspace_size.restype = sz
+            L.mdx_segmented_workspace_size.argtypes = [u64, u64, ctypes.c_int, u32]
+            L.mdx_segmented_workspace_size.restype = sz
+            L.mdx_workspace_init.argtypes = [vp, sz, vp]
+            L.mdx_workspace_init.restype = st
+            L.mdx_workspace_error.argtypes = [vp, vp]
+            L.mdx_workspace_error.restype = st
+            L.mdx_partition.argtypes = [vp, vp, u64, ctypes.c_int, Discr, vp, vp, vp, sz, vp]
+            L.mdx_partition.restype = st
+            L.mdx_partition_timed.argtypes = [vp, vp, u64, ctypes.c_int, Discr, vp, vp, vp, sz, vp,
+                                              vp]
+            L.mdx_partition_timed.restype = st
+            L.mdx_mdiscr.argtypes = [u32, u32, vp, vp, ctypes.c_int, Discr, vp, vp, sz, vp]
+            L.mdx_mdiscr.restype = st
+            L.mdx_partition_segmented.argtypes = [vp, vp, u64, ctypes.c_int, Discr, vp, u64, vp,
+                                                  vp, vp, sz, vp]
+            L.mdx_partition_segmented.restype = st
+            L.mdx_mdiscr_segm.argtypes = [u32, vp, vp, vp, vp, ctypes.c_int, Discr, vp, sz, vp]
+            L.mdx_mdiscr_segm.restype = st
+            L.mdx_strerror.argtypes = [st]
+            L.mdx_strerror.restype = ctypes.c_char_p
+            L.mdx_version.argtypes = []
+            L.mdx_version.restype = ctypes.c_char_p
+            _lib = L
+    return _lib
+
+
+def strerror(status: int) -> str:
+    try:
+        return lib().mdx_strerror(status).decode()
+    except ImportError:
+        return f"status {status}"
+
+
+def version() -> str:
+    return lib().mdx_version().decode()
+
+
+def _check(status: int, what: str) -> None:
+    if status != MDX_OK:
+        raise MdxError(status, what)
+
+
+def make_discr(discr) -> Discr:
+    """``("mod", m)`` / ``("mask", m)`` / ``m`` (= mod) -> the C struct."""
+    if isinstance(discr, Discr):
+        return discr
+    if isinstance(discr, int):
+        return Discr(DISCR_MOD, discr)
+    kind, m = discr
+    k = {"mod": DISCR_MOD, "mask": DISCR_MASK}.get(kind, kind)
+    return Discr(int(k), int(m))
+
+
+# --------------------------------------------------------------- workspaces --
+@dataclass
+class Workspace:
+    """A device workspace for the C ABI, zero-initialised once (mdx_workspace_init)."""
+    tensor: object
+    nbytes: int
+
+    @property
+    def ptr(self) -> int:
+        return self.tensor.data_ptr()
+
+    def error(self, stream=None) -> int:
+        """Synchronise and return (and clear) the latched device error status."""
+        return lib().mdx_workspace_error(ctypes.c_void_p(self.ptr), _stream_ptr(stream))
+
+
+_ws_cache = {}
+_ws_lock = threading.Lock()
+
+
+def _torch():
+    import torch  # plumbing: device memory and streams
+    return torch
+
+
+def _stream_ptr(stream) -> ctypes.c_void_p:
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def workspace(nbytes: int, device=None, stream=None) -> Workspace:
+    """The cached workspace of at least ``nbytes`` on ``device`` (grown on demand).
+
+    A cached workspace serves one call at a time; calls on different streams
+    that run concurrently need their own (:func:`new_workspace`).
+    """
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else
+                       torch.device(device).index or 0)
+    with _ws_lock:
+        ws = _ws_cache.get(dev.index)
+        if ws is None or ws.nbytes < nbytes:
+            ws = new_workspace(max(nbytes, 1 << 20), dev, stream)
+            _ws_cache[dev.index] = ws
+        return ws
+
+
+def new_workspace(nbytes: int, device=None, stream=None) -> Workspace:
+    torch = _torch()
+    t = torch.empty(int(nbytes), dtype=torch.uint8, device=device or "cuda")
+    _check(lib().mdx_workspace_init(ctypes.c_void_p(t.data_ptr()), int(nbytes),
+                                    _stream_ptr(stream)), "mdx_workspace_init")
+    return Workspace(t, int(nbytes))
+
+
+def _elem_of(t) -> int:
+    es = t.element_size()
+    if es == 4:
+        return ELEM_U32
+    if es == 8:
+        return ELEM_REC8
+    raise TypeError(f"unsupported element size {es} (4-byte values or 8-byte records)")
+
+
+def _require_cuda(*tensors) -> None:
+    for t in tensors:
+        if t is None:
+            continue
+        if not t.is_cuda:
+            raise ValueError("mdiscriminator_b200 operates on CUDA tensors only (no CPU path)")
+        if not t.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+
+
+# --------------------------------------------------------------- plain path --
+def workspace_size(n: int, elem: int, m: int) -> int:
+    return int(lib().mdx_workspace_size(int(n), int(elem), int(m)))
+
+
+def partition(d_in, discr, out=None, sizes=None, headflags=False, ws: Optional[Workspace] = None,
+              stream=None, count_done_event=None):
+    """Stable partition of a 1-D CUDA tensor (async on the current stream).
+
+    Returns ``(out, sizes)`` with ``sizes`` a device u32 tensor of m class
+    sizes, plus the head-flag array when ``headflags`` is true (a tensor, or
+    True to allocate one).  ``count_done_event`` (a ``torch.cuda.Event``) is
+    recorded between the counting and the scattering kernel.
+    """
+    torch = _torch()
+    _require_cuda(d_in)
+    dc = make_discr(discr)
+    n = d_in.numel()
+    elem = _elem_of(d_in)
+    if out is None:
+        out = torch.empty_like(d_in)
+    if sizes is None:
+        sizes = torch.empty(dc.m, dtype=torch.uint32, device=d_in.device)
+    hf = None
+    if headflags is True:
+        hf = torch.empty(n, dtype=torch.uint32, device=d_in.device)
+    elif headflags is not False and headflags is not None:
+        hf = headflags
+    _require_cuda(out, sizes, hf)
+    need = workspace_size(n, elem, dc.m)
+    if need == 0:
+        raise MdxError(MDX_ERR_INVALID, "mdx_workspace_size")
+    ws = ws or workspace(need, d_in.device, stream)
+    ev = ctypes.c_void_p(count_done_event.cuda_event if count_done_event is not None else 0)
+    st = lib().mdx_partition_timed(ctypes.c_void_p(d_in.data_ptr()),
+                                   ctypes.c_void_p(out.data_ptr()), n, elem, dc,
+                                   ctypes.c_void_p(sizes.data_ptr()),
+                                   ctypes.c_void_p(hf.data_ptr() if hf is not None else 0),
+                                   ctypes.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(stream), ev)
+    _check(st, "mdx_partition")
+    return (out, sizes, hf) if hf is not None else (out, sizes)
+
+
+def mdiscr(d_in, discr, d_out=None, num_hwd_thds: int = 1 << 16, ws: Optional[Workspace] = None,
+           stream=None) -> Tuple[object, list]:
+    """Reference-shaped ``mdiscr``: partitions into ``d_out`` and returns the
+    m class sizes on the host (synchronous), as ``mdiscr<DISCR>`` returns its
+    ``TupleType`` (MdiscrHost_optimized_clean.cu.h:149).  Raises
+    :class:`MdxError` where the reference's ``gpuErrchk`` would exit."""
+    torch = _torch()
+    _require_cuda(d_in)
+    dc = make_discr(discr)
+    n = d_in.numel()
+    elem = _elem_of(d_in)
+    if d_out is None:
+        d_out = torch.empty_like(d_in)
+    _require_cuda(d_out)
+    need = workspace_size(n, elem, dc.m)
+    ws = ws or workspace(need, d_in.device, stream)
+    h_sizes = (ctypes.c_uint32 * dc.m)()
+    st = lib().mdx_mdiscr(n, num_hwd_thds, ctypes.c_void_p(d_in.data_ptr()),
+                          ctypes.c_void_p(d_out.data_ptr()), elem, dc,
+                          ctypes.cast(h_sizes, ctypes.c_void_p), ctypes.c_void_p(ws.ptr),
+                          ws.nbytes, _stream_ptr(stream))
+    _check(st, "mdx_mdiscr")
+    return d_out, list(h_sizes)
+
+
+# ----------------------------------------------------------- segmented path --
+def segmented_workspace_size(n: int, num_segments: int, elem: int, m: int) -> int:
+    return int(lib().mdx_segmented_workspace_size(int(n), int(num_segments), int(elem), int(m)))
+
+
+def partition_segmented(d_in, d_offsets, discr, out=None, seg_sizes=None, headflags=False,
+                        ws: Optional[Workspace] = None, stream=None):
+    """Per-segment stable partition; ``d_offsets`` is a CUDA u64/i64 tensor of
+    S+1 non-decreasing offsets (0 first, n last).  Returns ``(out, seg_sizes)``
+    with seg_sizes of shape (S, m) [, head flags]."""
+    torch = _torch()
+    _require_cuda(d_in, d_offsets)
+    if d_offsets.element_size() != 8:
+        raise TypeError("segment offsets are 64-bit")
+    dc = make_discr(discr)
+    n = d_in.numel()
+    S = d_offsets.numel() - 1
+    if S < 0:
+        raise ValueError("offsets need at least one entry")
+    elem = _elem_of(d_in)
+    if out is None:
+        out = torch.empty_like(d_in)
+    if seg_sizes is None:
+        seg_sizes = torch.empty((S, dc.m), dtype=torch.uint32, device=d_in.device)
+    hf = None
+    if headflags is True:
+        hf = torch.empty(n, dtype=torch.uint32, device=d_in.device)
+    elif headflags is not False and headflags is not None:
+        hf = headflags
+    _require_cuda(out, seg_sizes, hf)
+    need = segmented_workspace_size(n, S, elem, dc.m)
+    if need == 0:
+        raise MdxError(MDX_ERR_INVALID, "mdx_segmented_workspace_size")
+    ws = ws or workspace(need, d_in.device, stream)
+    st = lib().mdx_partition_segmented(
+        ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(out.data_ptr()), n, elem, dc,
+        ctypes.c_void_p(d_offsets.data_ptr()), S, ctypes.c_void_p(seg_sizes.data_ptr()),
+        ctypes.c_void_p(hf.data_ptr() if hf is not None else 0), ctypes.c_void_p(ws.ptr),
+        ws.nbytes, _stream_ptr(stream))
+    _check(st, "mdx_partition_segmented")
+    return (out, seg_sizes, hf) if hf is not None else (out, seg_sizes)
+
+
+def mdiscr_segm(d_in, d_segment_sizes, discr, d_out=None, d_new_sizes=None,
+                ws: Optional[Workspace] = None, stream=None):
+    """Reference-shaped ``mdiscrSegm``: head-flag segment sizes in (i32, the
+    length at each segment start, 0 elsewhere), per-segment head-flag class
+    sizes out (i32 ``new_sizes``).  Returns ``(d_out, d_new_sizes)``."""
+    torch = _torch()
+    _require_cuda(d_in, d_segment_sizes)
+    dc = make_discr(discr)
+    n = d_in.numel()
+    elem = _elem_of(d_in)
+    if d_out is None:
+        d_out = torch.empty_like(d_in)
+    if d_new_sizes is None:
+        d_new_sizes = torch.empty(n, dtype=torch.int32, device=d_in.device)
+    _require_cuda(d_out, d_new_sizes)
+    need = segmented_workspace_size(n, n, elem, dc.m)
+    ws = ws or workspace(need, d_in.device, stream)
+    st = lib().mdx_mdiscr_segm(n, ctypes.c_void_p(d_in.data_ptr()),
+                               ctypes.c_void_p(d_segment_sizes.data_ptr()),
+                               ctypes.c_void_p(d_out.data_ptr()),
+                               ctypes.c_void_p(d_new_sizes.data_ptr()), elem, dc,
+                               ctypes.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(stream))
+    _check(st, "mdx_mdiscr_segm")
+    return d_out, d_new_sizes

@@ -1,0 +1,324 @@
+// mdx_capi.cu -- the C ABI (include/mdx.h) over pre-instantiated kernels.
+//
+// Instantiated families: element U32 / REC8 x discriminator MOD / MASK x class
+// bound M in {2, 4, 8, 16, 32, 64} (the smallest bound >= m is used; m itself
+// is a run-time parameter of the functor).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/mdx.h"
+#include "mdx_plain.cuh"
+#include "mdx_segm.cuh"
+
+namespace mdx {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kMaxChunks = 4096;
+constexpr int kStages = 2;
+constexpr size_t kHeaderBytes = 256;  // done, error, ... (see WsHeader)
+constexpr size_t kAlign = 256;
+
+struct WsHeader {  // first bytes of every workspace
+    uint32_t done;
+    uint32_t error;
+};
+
+template <class V>
+struct ElemCfg;
+template <>
+struct ElemCfg<uint32_t> {
+    static constexpr int kItems = 16;  // 4096-element tiles, 16 KB
+};
+template <>
+struct ElemCfg<uint64_t> {
+    static constexpr int kItems = 8;  // 2048-record tiles, 16 KB
+};
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+inline uint32_t class_bound(uint32_t m) {
+    uint32_t b = 2;
+    while (b < m) b <<= 1;
+    return b;
+}
+
+inline size_t elem_bytes(mdx_elem e) { return e == MDX_ELEM_REC8 ? 8 : 4; }
+inline uint32_t tile_elems(mdx_elem e) {
+    return kThreads * (e == MDX_ELEM_REC8 ? ElemCfg<uint64_t>::kItems : ElemCfg<uint32_t>::kItems);
+}
+
+inline uint32_t num_tiles_of(uint64_t n, mdx_elem e) {
+    const uint64_t t = tile_elems(e);
+    return static_cast<uint32_t>((n + t - 1) / t);
+}
+
+inline uint32_t max_chunks_of(uint64_t n, mdx_elem e) {
+    const uint32_t nt = num_tiles_of(n, e);
+    return nt < kMaxChunks ? (nt == 0 ? 1u : nt) : kMaxChunks;
+}
+
+struct PlainLayout {
+    size_t class_base, class_tot, chunk_cnt, chunk_pre, total;
+};
+
+inline PlainLayout plain_layout(uint64_t n, mdx_elem e, uint32_t m) {
+    const uint32_t M = class_bound(m);
+    const size_t G = max_chunks_of(n, e);
+    PlainLayout L;
+    L.class_base = kHeaderBytes;
+    L.class_tot = L.class_base + kMaxClasses * 4;
+    L.chunk_cnt = align_up(L.class_tot + kMaxClasses * 4, kAlign);
+    L.chunk_pre = align_up(L.chunk_cnt + M * G * 4, kAlign);
+    L.total = align_up(L.chunk_pre + M * G * 4, kAlign);
+    return L;
+}
+
+inline bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+
+mdx_status check_discr(mdx_discr d) {
+    if (d.m < 1 || d.m > MDX_MAX_CLASSES) return MDX_ERR_INVALID;
+    if (d.kind != MDX_DISCR_MOD && d.kind != MDX_DISCR_MASK) return MDX_ERR_INVALID;
+    if (d.kind == MDX_DISCR_MASK && !is_pow2(d.m)) return MDX_ERR_INVALID;
+    return MDX_OK;
+}
+
+mdx_status check_elem(mdx_elem e) {
+    return (e == MDX_ELEM_U32 || e == MDX_ELEM_REC8) ? MDX_OK : MDX_ERR_INVALID;
+}
+
+// Resident CTAs per SM of a kernel, cached per (device, kernel).
+struct OccEntry {
+    int device;
+    const void* fn;
+    int blocks;
+    int sms;
+};
+std::mutex g_occ_mu;
+OccEntry g_occ[256];
+int g_occ_n = 0;
+
+cudaError_t occupancy(const void* fn, size_t dyn_smem, int* blocks, int* sms) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        for (int i = 0; i < g_occ_n; i++)
+            if (g_occ[i].device == dev && g_occ[i].fn == fn) {
+                *blocks = g_occ[i].blocks;
+                *sms = g_occ[i].sms;
+                return cudaSuccess;
+            }
+    }
+    if (dyn_smem > 48 * 1024) {
+        err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(dyn_smem));
+        if (err != cudaSuccess) return err;
+    }
+    int b = 0, s = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, dyn_smem);
+    if (err != cudaSuccess) return err;
+    err = cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev);
+    if (err != cudaSuccess) return err;
+    if (b < 1) b = 1;
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    if (g_occ_n < 256) g_occ[g_occ_n++] = OccEntry{dev, fn, b, s};
+    *blocks = b;
+    *sms = s;
+    return cudaSuccess;
+}
+
+template <class V, class D, int M>
+mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
+                     uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
+                     cudaStream_t stream, cudaEvent_t ev_mid) {
+    constexpr int ITEMS = ElemCfg<V>::kItems;
+    constexpr int TILE = kThreads * ITEMS;
+    auto scatter = plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages>;
+    auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
+    constexpr size_t smem = plain_scatter_smem<V, TILE, kStages>();
+    int blocks = 0, sms = 0;
+    if (occupancy(reinterpret_cast<const void*>(scatter), smem, &blocks, &sms) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    const uint32_t nt = static_cast<uint32_t>((n + TILE - 1) / TILE);
+    uint32_t G = static_cast<uint32_t>(blocks) * static_cast<uint32_t>(sms);
+    if (G > nt) G = nt;
+    if (G > kMaxChunks) G = kMaxChunks;
+
+    PlainArgs a;
+    a.in = d_in;
+    a.out = d_out;
+    a.n = n;
+    a.num_tiles = nt;
+    a.num_chunks = G;
+    a.chunk_cnt = reinterpret_cast<uint32_t*>(ws + L.chunk_cnt);
+    a.chunk_pre = reinterpret_cast<uint32_t*>(ws + L.chunk_pre);
+    a.class_base = reinterpret_cast<uint32_t*>(ws + L.class_base);
+    a.class_tot = reinterpret_cast<uint32_t*>(ws + L.class_tot);
+    a.sizes = d_sizes;
+    a.headflags = d_headflags;
+    a.done = &reinterpret_cast<WsHeader*>(ws)->done;
+    a.error = &reinterpret_cast<WsHeader*>(ws)->error;
+    a.m = m;
+    count<<<G, kThreads, 0, stream>>>(a, d);
+    if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
+    scatter<<<G, kThreads, smem, stream>>>(a, d);
+    return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+}
+
+template <class V, class D>
+mdx_status dispatch_plain_m(const void* in, void* out, uint64_t n, D d, uint32_t m, uint32_t* sz,
+                            uint32_t* hf, unsigned char* ws, const PlainLayout& L,
+                            cudaStream_t st, cudaEvent_t ev) {
+    switch (class_bound(m)) {
+        case 2: return run_plain<V, D, 2>(in, out, n, d, m, sz, hf, ws, L, st, ev);
+        case 4: return run_plain<V, D, 4>(in, out, n, d, m, sz, hf, ws, L, st, ev);
+        case 8: return run_plain<V, D, 8>(in, out, n, d, m, sz, hf, ws, L, st, ev);
+        case 16: return run_plain<V, D, 16>(in, out, n, d, m, sz, hf, ws, L, st, ev);
+        case 32: return run_plain<V, D, 32>(in, out, n, d, m, sz, hf, ws, L, st, ev);
+        case 64: return run_plain<V, D, 64>(in, out, n, d, m, sz, hf, ws, L, st, ev);
+        default: return MDX_ERR_INVALID;
+    }
+}
+
+template <class V>
+mdx_status dispatch_plain(const void* in, void* out, uint64_t n, mdx_discr dc, uint32_t* sz,
+                          uint32_t* hf, unsigned char* ws, const PlainLayout& L, cudaStream_t st,
+                          cudaEvent_t ev) {
+    if (dc.kind == MDX_DISCR_MASK)
+        return dispatch_plain_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, sz, hf, ws, L, st, ev);
+    return dispatch_plain_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, sz, hf, ws, L, st, ev);
+}
+
+}  // namespace
+}  // namespace mdx
+
+using namespace mdx;
+
+extern "C" {
+
+size_t mdx_workspace_size(uint64_t n, mdx_elem elem, uint32_t m) {
+    if (check_elem(elem) != MDX_OK || m < 1 || m > MDX_MAX_CLASSES) return 0;
+    return plain_layout(n, elem, m).total;
+}
+
+mdx_status mdx_workspace_init(void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
+    if (d_ws == nullptr || ws_bytes < kHeaderBytes) return MDX_ERR_WORKSPACE;
+    if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
+    return cudaMemsetAsync(d_ws, 0, ws_bytes, reinterpret_cast<cudaStream_t>(stream)) == cudaSuccess
+               ? MDX_OK
+               : MDX_ERR_CUDA;
+}
+
+mdx_status mdx_workspace_error(void* d_ws, mdx_stream_t stream) {
+    if (d_ws == nullptr) return MDX_ERR_WORKSPACE;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MDX_ERR_CUDA;
+    uint32_t err = 0;
+    uint32_t* d_err = &reinterpret_cast<WsHeader*>(d_ws)->error;
+    if (cudaMemcpy(&err, d_err, sizeof(err), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    if (err != 0 && cudaMemset(d_err, 0, sizeof(err)) != cudaSuccess) return MDX_ERR_CUDA;
+    if (err & kErrTimeout) return MDX_ERR_TIMEOUT;
+    if (err & kErrSegments) return MDX_ERR_SEGMENTS;
+    return MDX_OK;
+}
+
+mdx_status mdx_partition_timed(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                               mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                               void* d_ws, size_t ws_bytes, mdx_stream_t stream,
+                               void* ev_count_done) {
+    cudaEvent_t ev = reinterpret_cast<cudaEvent_t>(ev_count_done);
+    mdx_status s = check_elem(elem);
+    if (s != MDX_OK) return s;
+    if ((s = check_discr(discr)) != MDX_OK) return s;
+    if (n > MDX_MAX_ELEMS) return MDX_ERR_INVALID;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        if (d_sizes && cudaMemsetAsync(d_sizes, 0, discr.m * sizeof(uint32_t), st) != cudaSuccess)
+            return MDX_ERR_CUDA;
+        return MDX_OK;
+    }
+    if (d_in == nullptr || d_out == nullptr) return MDX_ERR_INVALID;
+    const size_t w = elem_bytes(elem);
+    const char* ib = static_cast<const char*>(d_in);
+    const char* ob = static_cast<const char*>(d_out);
+    if (ib < ob + n * w && ob < ib + n * w) return MDX_ERR_INVALID;  // overlapping in/out
+    const PlainLayout L = plain_layout(n, elem, discr.m);
+    if (d_ws == nullptr || ws_bytes < L.total) return MDX_ERR_WORKSPACE;
+    if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
+    unsigned char* ws = static_cast<unsigned char*>(d_ws);
+    if (elem == MDX_ELEM_U32)
+        return dispatch_plain<uint32_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
+    return dispatch_plain<uint64_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
+}
+
+mdx_status mdx_partition(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                         mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags, void* d_ws,
+                         size_t ws_bytes, mdx_stream_t stream) {
+    return mdx_partition_timed(d_in, d_out, n, elem, discr, d_sizes, d_headflags, d_ws, ws_bytes,
+                               stream, nullptr);
+}
+
+mdx_status mdx_mdiscr(uint32_t n, uint32_t num_hwd_thds, const void* d_in, void* d_out,
+                      mdx_elem elem, mdx_discr discr, uint32_t* h_sizes, void* d_ws,
+                      size_t ws_bytes, mdx_stream_t stream) {
+    (void)num_hwd_thds;
+    if (h_sizes == nullptr) return MDX_ERR_INVALID;
+    mdx_status s = check_discr(discr);
+    if (s != MDX_OK) return s;
+    const PlainLayout L = plain_layout(n, elem, discr.m);
+    if (d_ws == nullptr || ws_bytes < L.total) return MDX_ERR_WORKSPACE;
+    // The class totals land in the workspace (class_tot); copy them back.
+    s = mdx_partition(d_in, d_out, n, elem, discr, nullptr, nullptr, d_ws, ws_bytes, stream);
+    if (s != MDX_OK) return s;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        memset(h_sizes, 0, discr.m * sizeof(uint32_t));
+        return MDX_OK;
+    }
+    const uint32_t* tot = reinterpret_cast<const uint32_t*>(static_cast<unsigned char*>(d_ws) +
+                                                            L.class_tot);
+    if (cudaMemcpyAsync(h_sizes, tot, discr.m * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) !=
+        cudaSuccess)
+        return MDX_ERR_CUDA;
+    return mdx_workspace_error(d_ws, stream);
+}
+
+size_t mdx_segmented_workspace_size(uint64_t n, uint64_t num_segments, mdx_elem elem,
+                                    uint32_t m) {
+    (void)n; (void)num_segments; (void)elem; (void)m;
+    return 0;
+}
+
+mdx_status mdx_partition_segmented(const void*, void*, uint64_t, mdx_elem, mdx_discr,
+                                   const uint64_t*, uint64_t, uint32_t*, uint32_t*, void*, size_t,
+                                   mdx_stream_t) {
+    return MDX_ERR_UNSUPPORTED;
+}
+
+mdx_status mdx_mdiscr_segm(uint32_t, const void*, const int32_t*, void*, int32_t*, mdx_elem,
+                           mdx_discr, void*, size_t, mdx_stream_t) {
+    return MDX_ERR_UNSUPPORTED;
+}
+
+const char* mdx_strerror(mdx_status s) {
+    switch (s) {
+        case MDX_OK: return "ok";
+        case MDX_ERR_INVALID: return "invalid argument";
+        case MDX_ERR_WORKSPACE: return "workspace too small or misaligned";
+        case MDX_ERR_CUDA: return "CUDA runtime error";
+        case MDX_ERR_TIMEOUT: return "device-side bounded wait timed out";
+        case MDX_ERR_UNSUPPORTED: return "unsupported request";
+        case MDX_ERR_SEGMENTS: return "malformed segment description";
+    }
+    return "unknown status";
+}
+
+const char* mdx_version(void) { return "mdx 0.1.0 sm_100a"; }
+
+}  // extern "C"

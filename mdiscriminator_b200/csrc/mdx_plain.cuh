@@ -1,0 +1,406 @@
+// mdx_plain.cuh -- plain (unsegmented) stable m-way partition for sm_100a.
+//
+// Replaces the reference's four-phase pipeline of mdiscr<DISCR>
+// (cuda_code/MdiscrHost_optimized_clean.cu.h:9-150: transposePad ->
+// mapVctKernel -> recursive scanInc with a mid-pipeline D2H copy ->
+// writeMultiKernel, ~32 B of HBM traffic per int32 element, four host syncs and
+// per-call cudaMalloc) by two kernels and no host round trip:
+//
+//   plain_count_kernel   reads each element once (4 B/elem for int32) and
+//                        counts classes per chunk; the last CTA to finish
+//                        (ticket on a workspace counter, no waiting) scans the
+//                        per-chunk counts into per-chunk class prefixes, the
+//                        class bases (exclusive scan of the totals, the
+//                        `offsets` of SeqMdiscr.h:34-38) and the class sizes.
+//   plain_scatter_kernel re-reads each element (4 B) and writes it once (4 B):
+//                        per tile, warp ranks from __match_any_sync + __popc,
+//                        a block scan of the per-warp class counts, a
+//                        shared-memory staged scatter so every class run leaves
+//                        the SM as coalesced stores.  Tiles are staged into
+//                        shared memory by TMA bulk copies (cp.async.bulk, no
+//                        multicast) through an mbarrier ring.  Each CTA walks
+//                        its chunk from the end backwards, so the tiles the
+//                        count kernel read last are still in L2.
+//
+// Why two passes: the output position of a class-c element is
+// base_c + prefix_c(tile) + rank, and base_c = sum of the totals of classes
+// below c depends on every element of the input, the last one included.  With
+// on-chip storage (~33 MB shared memory + 126 MB L2) far below the 1 GiB input
+// of N = 2^28 int32, no element of class >= 1 can be stored before the whole
+// input has been read, so the minimum traffic is read + re-read + write
+// (12 B/elem), minus whatever the re-read finds in L2.
+#pragma once
+
+#include "mdx_device.cuh"
+
+namespace mdx {
+
+struct PlainArgs {
+    const void* in;
+    void* out;
+    uint64_t n;
+    uint32_t num_tiles;   // ceil(n / TILE)
+    uint32_t num_chunks;  // G: one chunk of consecutive tiles per CTA
+    uint32_t* chunk_cnt;  // [M][G] class counts per chunk
+    uint32_t* chunk_pre;  // [M][G] exclusive prefix of chunk_cnt over chunks
+    uint32_t* class_base; // [M]    exclusive scan of the class totals
+    uint32_t* class_tot;  // [M]    class totals
+    uint32_t* sizes;      // [m]    user output (tuple form) or null
+    uint32_t* headflags;  // [n]    user output (head-flag form) or null
+    uint32_t* done;       // chunk ticket counter (0 on entry, reset to 0 by the last CTA)
+    uint32_t* error;      // latched error bits
+    uint32_t m;
+};
+
+// Chunk k covers tiles [k*T/G, (k+1)*T/G).
+__device__ __forceinline__ void chunk_tiles(uint32_t k, uint32_t T, uint32_t G, uint32_t& t0,
+                                            uint32_t& t1) {
+    t0 = static_cast<uint32_t>(static_cast<uint64_t>(k) * T / G);
+    t1 = static_cast<uint32_t>(static_cast<uint64_t>(k + 1) * T / G);
+}
+
+template <class V>
+__device__ __forceinline__ void unpack16(const uint4& r, V (&e)[16 / sizeof(V)]);
+template <>
+__device__ __forceinline__ void unpack16<uint32_t>(const uint4& r, uint32_t (&e)[4]) {
+    e[0] = r.x; e[1] = r.y; e[2] = r.z; e[3] = r.w;
+}
+template <>
+__device__ __forceinline__ void unpack16<uint64_t>(const uint4& r, uint64_t (&e)[2]) {
+    e[0] = static_cast<uint64_t>(r.x) | (static_cast<uint64_t>(r.y) << 32);
+    e[1] = static_cast<uint64_t>(r.z) | (static_cast<uint64_t>(r.w) << 32);
+}
+
+// Per-thread class counters for M <= 16: 8-bit lanes packed in u64 words,
+// flushed into u32 accumulators before any lane can reach 256.
+template <int M>
+struct PackedCounts {
+    static_assert(M <= 16, "packed counters cover at most 16 classes");
+    static constexpr int NW = (M + 7) / 8;
+    uint64_t pk[NW];
+    uint32_t acc[M];
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int w = 0; w < NW; w++) pk[w] = 0;
+#pragma unroll
+        for (int c = 0; c < M; c++) acc[c] = 0;
+    }
+    __device__ __forceinline__ void add(uint32_t c) {
+        if constexpr (NW == 1) {
+            pk[0] += 1ull << (c << 3);
+        } else {
+            const uint64_t inc = 1ull << ((c & 7u) << 3);
+            pk[0] += (c < 8u) ? inc : 0ull;
+            pk[1] += (c < 8u) ? 0ull : inc;
+        }
+    }
+    __device__ __forceinline__ void flush() {
+#pragma unroll
+        for (int c = 0; c < M; c++)
+            acc[c] += static_cast<uint32_t>(pk[c >> 3] >> ((c & 7) * 8)) & 0xffu;
+#pragma unroll
+        for (int w = 0; w < NW; w++) pk[w] = 0;
+    }
+};
+
+// After every CTA has published its chunk counts, the last CTA turns them into
+// per-chunk exclusive prefixes, class totals, class bases and the user's sizes,
+// then resets the ticket counter for the next call.
+template <int M, int THREADS>
+__device__ void plain_finish_scan(const PlainArgs& a, uint32_t* tot_sh) {
+    constexpr int W = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t G = a.num_chunks;
+    for (int c = warp; c < M; c += W) {
+        uint32_t run = 0;
+        for (uint32_t k0 = 0; k0 < G; k0 += 32) {
+            const uint32_t kk = k0 + lane;
+            const uint32_t x = kk < G ? __ldcg(&a.chunk_cnt[c * G + kk]) : 0u;
+            const uint32_t incl = warp_incl_scan(x);
+            if (kk < G) a.chunk_pre[c * G + kk] = run + incl - x;
+            run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) tot_sh[c] = run;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int c = 0; c < M; c++) {
+            a.class_base[c] = acc;
+            a.class_tot[c] = tot_sh[c];
+            if (a.sizes != nullptr && static_cast<uint32_t>(c) < a.m) a.sizes[c] = tot_sh[c];
+            acc += tot_sh[c];
+        }
+        *a.done = 0u;
+    }
+}
+
+template <class V, class D, int M, int THREADS, int TILE>
+__global__ void __launch_bounds__(THREADS) plain_count_kernel(PlainArgs a, D d) {
+    constexpr int W = THREADS / 32;
+    constexpr int VEC = 16 / static_cast<int>(sizeof(V));
+    constexpr int UNROLL = 4;
+    __shared__ uint32_t red[W][M];
+    __shared__ uint32_t tot_sh[M];
+    __shared__ int am_last;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t G = a.num_chunks, k = blockIdx.x;
+    uint32_t t0, t1;
+    chunk_tiles(k, a.num_tiles, G, t0, t1);
+    const uint64_t e0 = static_cast<uint64_t>(t0) * TILE;
+    const uint64_t e1 = min(static_cast<uint64_t>(t1) * TILE, a.n);
+    const V* in = static_cast<const V*>(a.in);
+    const bool vec_ok = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
+
+    if constexpr (M <= 16) {
+        PackedCounts<M> pc;
+        pc.init();
+        if (vec_ok) {
+            const uint4* vp = reinterpret_cast<const uint4*>(in + e0);
+            const uint64_t nv = (e1 - e0) / VEC;
+            int since_flush = 0;
+            for (uint64_t i = tid; i < nv; i += static_cast<uint64_t>(THREADS) * UNROLL) {
+                uint4 r[UNROLL];
+#pragma unroll
+                for (int u = 0; u < UNROLL; u++) {
+                    const uint64_t j = i + static_cast<uint64_t>(u) * THREADS;
+                    if (j < nv) r[u] = __ldg(vp + j);
+                }
+#pragma unroll
+                for (int u = 0; u < UNROLL; u++) {
+                    const uint64_t j = i + static_cast<uint64_t>(u) * THREADS;
+                    if (j < nv) {
+                        V e[VEC];
+                        unpack16<V>(r[u], e);
+#pragma unroll
+                        for (int q = 0; q < VEC; q++) pc.add(d(e[q]));
+                    }
+                }
+                if (++since_flush == 15) {  // <= 15 * 16 = 240 increments per lane
+                    pc.flush();
+                    since_flush = 0;
+                }
+            }
+            for (uint64_t e = e0 + nv * VEC + tid; e < e1; e += THREADS) pc.add(d(in[e]));
+        } else {
+            int since_flush = 0;
+            for (uint64_t e = e0 + tid; e < e1; e += THREADS) {
+                pc.add(d(in[e]));
+                if (++since_flush == 255) {
+                    pc.flush();
+                    since_flush = 0;
+                }
+            }
+        }
+        pc.flush();
+#pragma unroll
+        for (int c = 0; c < M; c++) {
+            const uint32_t s = warp_sum(pc.acc[c]);
+            if (lane == 0) red[warp][c] = s;
+        }
+    } else {
+        for (int c = lane; c < M; c += 32) red[warp][c] = 0;
+        __syncwarp();
+        if (vec_ok) {
+            const uint4* vp = reinterpret_cast<const uint4*>(in + e0);
+            const uint64_t nv = (e1 - e0) / VEC;
+            for (uint64_t i = tid; i < nv; i += static_cast<uint64_t>(THREADS) * UNROLL) {
+                uint4 r[UNROLL];
+#pragma unroll
+                for (int u = 0; u < UNROLL; u++) {
+                    const uint64_t j = i + static_cast<uint64_t>(u) * THREADS;
+                    if (j < nv) r[u] = __ldg(vp + j);
+                }
+#pragma unroll
+                for (int u = 0; u < UNROLL; u++) {
+                    const uint64_t j = i + static_cast<uint64_t>(u) * THREADS;
+                    if (j < nv) {
+                        V e[VEC];
+                        unpack16<V>(r[u], e);
+#pragma unroll
+                        for (int q = 0; q < VEC; q++) atomicAdd(&red[warp][d(e[q])], 1u);
+                    }
+                }
+            }
+            for (uint64_t e = e0 + nv * VEC + tid; e < e1; e += THREADS)
+                atomicAdd(&red[warp][d(in[e])], 1u);
+        } else {
+            for (uint64_t e = e0 + tid; e < e1; e += THREADS) atomicAdd(&red[warp][d(in[e])], 1u);
+        }
+    }
+    __syncthreads();
+    if (tid < M) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int w = 0; w < W; w++) s += red[w][tid];
+        a.chunk_cnt[tid * G + k] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) am_last = (atomicAdd(a.done, 1u) == G - 1u);
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    plain_finish_scan<M, THREADS>(a, tot_sh);
+}
+
+// Shared-memory bytes of plain_scatter_kernel's dynamic part.
+template <class V, int TILE, int STAGES>
+constexpr size_t plain_scatter_smem() {
+    return static_cast<size_t>(STAGES + 1) * TILE * sizeof(V) + TILE;  // ring + stage + class bytes
+}
+
+template <class V, class D, int M, int THREADS, int ITEMS, int STAGES>
+__global__ void __launch_bounds__(THREADS) plain_scatter_kernel(PlainArgs a, D d) {
+    constexpr int TILE = THREADS * ITEMS;
+    constexpr int W = THREADS / 32;
+    constexpr int WSPAN = 32 * ITEMS;  // elements per warp per tile
+    static_assert(WSPAN <= 65536, "warp-local ranks are packed in 16 bits");
+    static_assert(M <= 64 && M >= 2, "class bound");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    V* ring = reinterpret_cast<V*>(smem_raw);       // STAGES tiles, filled by TMA
+    V* stage = ring + STAGES * TILE;                // one tile, class-sorted
+    uint8_t* stage_cls = reinterpret_cast<uint8_t*>(stage + TILE);
+
+    __shared__ __align__(8) uint64_t bars[STAGES];
+    __shared__ uint32_t whist[W][M];  // per-warp running class counts
+    __shared__ uint32_t wbase[W][M];  // tile-local start of warp w's class-c run
+    __shared__ uint32_t cursor[M];    // global end cursor of this chunk's class-c run
+    __shared__ uint32_t delta[M];     // dst = slot + delta[c] (mod 2^32)
+    __shared__ uint32_t hf_base[M], hf_size[M];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t G = a.num_chunks, k = blockIdx.x;
+    uint32_t t0, t1;
+    chunk_tiles(k, a.num_tiles, G, t0, t1);
+    const uint32_t cnt = t1 - t0;
+    if (cnt == 0) return;
+    const V* in = static_cast<const V*>(a.in);
+    V* out = static_cast<V*>(a.out);
+    uint32_t* hf = a.headflags;
+    const bool tma_ok = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
+
+    if (tid < M) {
+        cursor[tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
+        hf_base[tid] = a.class_base[tid];
+        hf_size[tid] = a.class_tot[tid];
+    }
+    if (tid == 0) {
+#pragma unroll
+        for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    // Issue the load of the i-th tile in processing order (tile t1-1-i) into
+    // ring slot i % STAGES.  Full tiles go by TMA; the partial last tile of
+    // the array (or any tile when `in` is not 16-byte aligned) is read by the
+    // threads straight from global memory, and the barrier is only arrived on
+    // so that its phase still advances once per use.
+    auto issue = [&](uint32_t i) {
+        const uint32_t tile = t1 - 1u - i;
+        const uint64_t ts = static_cast<uint64_t>(tile) * TILE;
+        uint64_t* bar = &bars[i % STAGES];
+        if (tma_ok && ts + TILE <= a.n) {
+            mbar_arrive_expect_tx(bar, TILE * sizeof(V));
+            bulk_load_g2s(ring + (i % STAGES) * TILE, in + ts, TILE * sizeof(V), bar);
+        } else {
+            mbar_arrive(bar);
+        }
+    };
+    if (tid == 0)
+        for (uint32_t i = 0; i < STAGES && i < cnt; i++) issue(i);
+
+    for (uint32_t i = 0; i < cnt; i++) {
+        const uint32_t tile = t1 - 1u - i;
+        const uint64_t ts = static_cast<uint64_t>(tile) * TILE;
+        const uint32_t valid = static_cast<uint32_t>(min(static_cast<uint64_t>(TILE), a.n - ts));
+        const bool from_ring = tma_ok && valid == TILE;
+        const V* src = ring + (i % STAGES) * TILE;
+        const bool ok = mbar_wait_bounded(&bars[i % STAGES], (i / STAGES) & 1u);
+
+        // ---- warp ranks: element (warp, j, lane) is tile slot warp*WSPAN + j*32 + lane
+        for (int c = lane; c < M; c += 32) whist[warp][c] = 0;
+        __syncwarp();
+        V vals[ITEMS];
+        uint32_t info[ITEMS];  // class << 16 | warp-local rank
+        const uint32_t lt = lanemask_lt();
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const uint32_t idx = warp * WSPAN + j * 32 + lane;
+            const bool live = idx < valid;
+            V v = V();
+            if (live) v = from_ring ? src[idx] : in[ts + idx];
+            const uint32_t c = live ? d(v) : static_cast<uint32_t>(M);
+            const uint32_t peers = __match_any_sync(0xffffffffu, c);
+            const uint32_t before = live ? whist[warp][c] : 0u;
+            const uint32_t rank = before + __popc(peers & lt);
+            __syncwarp();
+            if (live && (peers >> lane) == 1u) whist[warp][c] = rank + 1u;  // last lane of its class
+            __syncwarp();
+            vals[j] = v;
+            info[j] = (c << 16) | rank;
+        }
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(a.error, kErrTimeout);
+            // drain: wait (bounded) for the copies this CTA still has in flight
+            for (uint32_t q = i + 1; q < cnt && q < i + STAGES; q++)
+                if (tid == 0) (void)mbar_wait_bounded(&bars[q % STAGES], (q / STAGES) & 1u);
+            return;
+        }
+
+        // ---- block scan: per class, over warps (wprefix) and over classes (tile start)
+        if (warp == 0) {
+            uint32_t carry = 0;
+#pragma unroll
+            for (int c0 = 0; c0 < M; c0 += 32) {
+                const int c = c0 + lane;
+                uint32_t tcnt = 0;
+                if (c < M) {
+#pragma unroll
+                    for (int w = 0; w < W; w++) {
+                        const uint32_t x = whist[w][c];
+                        wbase[w][c] = tcnt;
+                        tcnt += x;
+                    }
+                }
+                const uint32_t incl = warp_incl_scan(tcnt);
+                const uint32_t tstart = carry + incl - tcnt;
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+                if (c < M) {
+                    const uint32_t cur = cursor[c] - tcnt;
+                    cursor[c] = cur;
+                    delta[c] = cur - tstart;
+#pragma unroll
+                    for (int w = 0; w < W; w++) wbase[w][c] += tstart;
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- scatter into the class-sorted stage
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const uint32_t c = info[j] >> 16;
+            if (c < static_cast<uint32_t>(M)) {
+                const uint32_t slot = wbase[warp][c] + (info[j] & 0xffffu);
+                stage[slot] = vals[j];
+                stage_cls[slot] = static_cast<uint8_t>(c);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
+
+        // ---- coalesced write-out of the class runs
+        for (uint32_t slot = tid; slot < valid; slot += THREADS) {
+            const uint32_t c = stage_cls[slot];
+            const uint32_t dst = slot + delta[c];
+            out[dst] = stage[slot];
+            if (hf != nullptr) hf[dst] = (dst == hf_base[c]) ? hf_size[c] : 0u;
+        }
+    }
+}
+
+}  // namespace mdx

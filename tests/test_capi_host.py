@@ -1,0 +1,99 @@
+"""The C-ABI library on the host (no GPU): it loads, exports every symbol
+include/*.h declares, and rejects bad arguments before touching the device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import mdiscriminator_b200 as mdx
+from mdiscriminator_b200 import build as mdx_build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def L():
+    mdx_build.build()
+    return mdx.lib()
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for root, _, files in os.walk(inc):
+        for f in files:
+            if not f.endswith(".h"):
+                continue
+            text = open(os.path.join(root, f)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(mdx_\w+)\s*\(", text, re.M):
+                names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    for required in ("mdx_partition", "mdx_mdiscr", "mdx_partition_segmented", "mdx_mdiscr_segm",
+                     "mdx_workspace_size", "mdx_workspace_init", "mdx_strerror"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol(L):
+    for name in declared_symbols():
+        assert hasattr(L, name), f"libmdx.so does not export {name}"
+
+
+def test_version_and_strerror(L):
+    assert "sm_100a" in mdx.version()
+    for s in range(7):
+        assert mdx.strerror(s)
+    assert mdx.strerror(mdx.MDX_ERR_TIMEOUT).startswith("device-side")
+
+
+def test_workspace_size_rules(L):
+    assert mdx.workspace_size(1 << 28, mdx.ELEM_U32, 8) > 0
+    assert mdx.workspace_size(1 << 20, mdx.ELEM_U32, 0) == 0
+    assert mdx.workspace_size(1 << 20, mdx.ELEM_U32, 65) == 0
+    assert mdx.workspace_size(1 << 20, 7, 4) == 0
+    # grows with m and n, bounded by the chunk cap
+    assert mdx.workspace_size(1 << 28, mdx.ELEM_U32, 64) >= mdx.workspace_size(1 << 28, mdx.ELEM_U32, 8)
+    assert mdx.workspace_size(1 << 30, mdx.ELEM_U32, 8) == mdx.workspace_size(1 << 28, mdx.ELEM_U32, 8)
+
+
+def _call_partition(L, n, elem, discr, ws=0, ws_bytes=0, inp=1 << 20, out=1 << 30):
+    return L.mdx_partition(ctypes.c_void_p(inp), ctypes.c_void_p(out), n, elem, discr, None, None,
+                           ctypes.c_void_p(ws), ws_bytes, None)
+
+
+def test_argument_validation_happens_before_any_device_work(L):
+    D = mdx.Discr
+    # bad class counts / kinds / element layouts
+    assert _call_partition(L, 10, mdx.ELEM_U32, D(mdx.DISCR_MOD, 0)) == mdx.MDX_ERR_INVALID
+    assert _call_partition(L, 10, mdx.ELEM_U32, D(mdx.DISCR_MOD, 65)) == mdx.MDX_ERR_INVALID
+    assert _call_partition(L, 10, mdx.ELEM_U32, D(mdx.DISCR_MASK, 3)) == mdx.MDX_ERR_INVALID
+    assert _call_partition(L, 10, mdx.ELEM_U32, D(9, 4)) == mdx.MDX_ERR_INVALID
+    assert _call_partition(L, 10, 5, D(mdx.DISCR_MOD, 4)) == mdx.MDX_ERR_INVALID
+    # n beyond u32 class sizes
+    assert _call_partition(L, 1 << 32, mdx.ELEM_U32, D(mdx.DISCR_MOD, 4)) == mdx.MDX_ERR_INVALID
+    # overlapping input and output
+    assert _call_partition(L, 100, mdx.ELEM_U32, D(mdx.DISCR_MOD, 4), inp=4096,
+                           out=4096 + 64) == mdx.MDX_ERR_INVALID
+    # null arrays
+    assert _call_partition(L, 100, mdx.ELEM_U32, D(mdx.DISCR_MOD, 4), inp=0) == mdx.MDX_ERR_INVALID
+    # workspace missing / too small / misaligned
+    assert _call_partition(L, 100, mdx.ELEM_U32, D(mdx.DISCR_MOD, 4)) == mdx.MDX_ERR_WORKSPACE
+    assert _call_partition(L, 100, mdx.ELEM_U32, D(mdx.DISCR_MOD, 4), ws=1 << 24,
+                           ws_bytes=16) == mdx.MDX_ERR_WORKSPACE
+    need = mdx.workspace_size(100, mdx.ELEM_U32, 4)
+    assert _call_partition(L, 100, mdx.ELEM_U32, D(mdx.DISCR_MOD, 4), ws=(1 << 24) + 8,
+                           ws_bytes=need) == mdx.MDX_ERR_WORKSPACE
+    # n == 0 with no outputs is a no-op
+    assert _call_partition(L, 0, mdx.ELEM_U32, D(mdx.DISCR_MOD, 4)) == mdx.MDX_OK
+
+
+def test_no_cpu_fallback_for_host_tensors():
+    torch = pytest.importorskip("torch")
+    x = torch.zeros(16, dtype=torch.int32)
+    with pytest.raises(ValueError, match="CUDA tensors only"):
+        mdx.partition(x, ("mod", 4))
