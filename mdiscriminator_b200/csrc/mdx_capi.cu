@@ -5,6 +5,8 @@
 // is a run-time parameter of the functor).
 #include <cuda_runtime.h>
 
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched from the runtime)
+
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -132,18 +134,69 @@ cudaError_t occupancy(const void* fn, size_t dyn_smem, int* blocks, int* sms) {
     return cudaSuccess;
 }
 
+// cuTensorMapEncodeTiled, fetched through the runtime so the library needs no
+// direct libcuda link.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                             &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// The n elements viewed as rows of 128 bytes (n * sizeof(V) / 128 whole rows),
+// boxes of `box_rows` rows, 128-byte swizzle.  False if TMA cannot be used
+// (unaligned base, fewer rows than one box, encoder unavailable).
+bool make_row_map(CUtensorMap* map, const void* base, uint64_t n, size_t elem, uint32_t box_rows) {
+    std::memset(map, 0, sizeof(*map));
+    if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return false;
+    const uint64_t per_row = 128 / elem;
+    const uint64_t rows = n / per_row;
+    if (rows < box_rows) return false;
+    EncodeTiledFn enc = tensor_map_encoder();
+    if (enc == nullptr) return false;
+    const cuuint64_t dims[2] = {per_row, rows};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(per_row), box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapDataType dt =
+        elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_UINT64;
+    return enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class V, class D, int M>
 mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
                      uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
                      cudaStream_t stream, cudaEvent_t ev_mid) {
     constexpr int ITEMS = ElemCfg<V>::kItems;
     constexpr int TILE = kThreads * ITEMS;
-    auto scatter = plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages>;
     auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
-    constexpr size_t smem = plain_scatter_smem<V, TILE, kStages>();
+    const void* scatter_fn;
+    size_t smem;
+    if constexpr (M <= 16) {
+        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
+        static_assert(SL::kTile == TILE, "both kernels use the same tiles");
+        scatter_fn = reinterpret_cast<const void*>(plain_scatter_tma_kernel<V, D, M, kThreads, kStages>);
+        smem = SL::kBytes;
+    } else {
+        scatter_fn = reinterpret_cast<const void*>(plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages>);
+        smem = plain_scatter_smem<V, TILE, kStages>();
+    }
     int blocks = 0, sms = 0;
-    if (occupancy(reinterpret_cast<const void*>(scatter), smem, &blocks, &sms) != cudaSuccess)
-        return MDX_ERR_CUDA;
+    if (occupancy(scatter_fn, smem, &blocks, &sms) != cudaSuccess) return MDX_ERR_CUDA;
     const uint32_t nt = static_cast<uint32_t>((n + TILE - 1) / TILE);
     uint32_t G = static_cast<uint32_t>(blocks) * static_cast<uint32_t>(sms);
     if (G > nt) G = nt;
@@ -164,9 +217,22 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.done = &reinterpret_cast<WsHeader*>(ws)->done;
     a.error = &reinterpret_cast<WsHeader*>(ws)->error;
     a.m = m;
+    a.use_tma = 0;
+    // head flags: all zero but for count_c at offset_c, which the last
+    // counting CTA writes
+    if (d_headflags != nullptr &&
+        cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess)
+        return MDX_ERR_CUDA;
     count<<<G, kThreads, 0, stream>>>(a, d);
     if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
-    scatter<<<G, kThreads, smem, stream>>>(a, d);
+    if constexpr (M <= 16) {
+        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
+        CUtensorMap map;
+        a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
+        plain_scatter_tma_kernel<V, D, M, kThreads, kStages><<<G, kThreads, smem, stream>>>(a, d, map);
+    } else {
+        plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages><<<G, kThreads, smem, stream>>>(a, d);
+    }
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
 }
 
@@ -248,6 +314,8 @@ mdx_status mdx_partition_timed(const void* d_in, void* d_out, uint64_t n, mdx_el
     const char* ib = static_cast<const char*>(d_in);
     const char* ob = static_cast<const char*>(d_out);
     if (ib < ob + n * w && ob < ib + n * w) return MDX_ERR_INVALID;  // overlapping in/out
+    if (reinterpret_cast<uintptr_t>(d_in) % w || reinterpret_cast<uintptr_t>(d_out) % w)
+        return MDX_ERR_INVALID;  // elements must be naturally aligned
     const PlainLayout L = plain_layout(n, elem, discr.m);
     if (d_ws == nullptr || ws_bytes < L.total) return MDX_ERR_WORKSPACE;
     if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
@@ -292,7 +360,7 @@ mdx_status mdx_mdiscr(uint32_t n, uint32_t num_hwd_thds, const void* d_in, void*
 size_t mdx_segmented_workspace_size(uint64_t n, uint64_t num_segments, mdx_elem elem,
                                     uint32_t m) {
     (void)n; (void)num_segments; (void)elem; (void)m;
-    return 0;
+    return kHeaderBytes;
 }
 
 mdx_status mdx_partition_segmented(const void*, void*, uint64_t, mdx_elem, mdx_discr,
