@@ -405,32 +405,32 @@ __global__ void __launch_bounds__(THREADS) plain_scatter_kernel(PlainArgs a, D d
     }
 }
 
-// Per-thread class counters for at most 16 classes in 8-bit lanes of u64
-// words (a thread ranks at most 16 elements per tile).
+// Per-thread class counters in 4-bit lanes: one u32 holds 8 classes, two
+// hold 16.  A lane never reaches 16: with 16 elements per thread only the
+// first 15 are counted in the lanes and the 16th is added when the counts are
+// published.
 template <int M>
-struct ByteCounts {
-    static_assert(M <= 16, "byte counters cover at most 16 classes");
+struct NibbleCounts {
+    static_assert(M <= 16, "nibble counters cover at most 16 classes");
     static constexpr int NW = (M + 7) / 8;
-    uint64_t w[NW];
+    uint32_t w[NW];
     __device__ __forceinline__ void init() {
 #pragma unroll
         for (int q = 0; q < NW; q++) w[q] = 0;
     }
     __device__ __forceinline__ uint32_t get(uint32_t c) const {
         if constexpr (NW == 1) {
-            return static_cast<uint32_t>(w[0] >> (c << 3)) & 0xffu;
+            return (w[0] >> (c << 2)) & 15u;
         } else {
-            const uint64_t x = (c < 8u) ? w[0] : w[1];
-            return static_cast<uint32_t>(x >> ((c & 7u) << 3)) & 0xffu;
+            return (((c < 8u) ? w[0] : w[1]) >> ((c & 7u) << 2)) & 15u;
         }
     }
     __device__ __forceinline__ void inc(uint32_t c) {
         if constexpr (NW == 1) {
-            w[0] += 1ull << (c << 3);
+            w[0] += 1u << (c << 2);
         } else {
-            const uint64_t one = 1ull << ((c & 7u) << 3);
-            w[0] += (c < 8u) ? one : 0ull;
-            w[1] += (c < 8u) ? 0ull : one;
+            const uint32_t one = 1u << ((c & 7u) << 2);
+            if (c < 8u) w[0] += one; else w[1] += one;
         }
     }
 };
@@ -453,7 +453,8 @@ struct ScatterTmaSmem {
     static constexpr int kTile = THREADS * kItems;
     static constexpr int kRows = kTile * static_cast<int>(sizeof(V)) / 128;  // 128-byte rows
     static constexpr uint32_t kAU = 16 / sizeof(V);                 // elements per 16 bytes
-    static constexpr int kStageElems = kTile + static_cast<int>(kAU) * (M + 1);
+    // every class run gets kAU slots of slack for its 16-byte phase
+    static constexpr int kStageElems = kTile + static_cast<int>(kAU) * M;
     static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
     static constexpr size_t kStageBytes = 2ull * kStageElems * sizeof(V);
     static constexpr size_t kCntBytes = static_cast<size_t>(M) * THREADS * 4;
@@ -466,15 +467,16 @@ struct ScatterTmaSmem {
 //  * tiles arrive by tensor TMA (one 2-D box of 128-byte rows per tile) with
 //    the 128-byte swizzle, so the four 16-byte shared loads with which a thread
 //    takes its 64 contiguous bytes are free of bank conflicts;
-//  * a thread ranks its own consecutive elements with 8-bit counters in
-//    registers (local rank = count of its earlier same-class elements), then a
-//    block scan over the [class][thread] count matrix in shared memory gives
-//    each thread's exclusive class prefix (stable: thread order = input order);
+//  * a thread ranks its own consecutive elements with 4-bit counters in a
+//    register (local rank = count of its earlier same-class elements); a block
+//    scan over the [class][thread] count matrix in shared memory then gives
+//    every thread its exclusive class prefix (stable: thread order = input
+//    order), with the tile's class-run start folded in;
 //  * every class run is placed in the stage at the same 16-byte phase as its
 //    destination, so its aligned interior leaves by one bulk store
-//    (cp.async.bulk shared->global) and only <= 2*(16/sizeof(V)) head and tail
-//    elements per run are written by threads.  The stage is double buffered
-//    and a buffer is rewritten only after its bulk stores have read it.
+//    (cp.async.bulk shared->global) and only the < 16-byte head and tail of a
+//    run are written by threads.  The stage is double buffered and a buffer is
+//    rewritten only after its bulk stores have read it.
 template <class V, class D, int M, int THREADS, int STAGES>
 __global__ void __launch_bounds__(THREADS)
     plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
@@ -485,8 +487,10 @@ __global__ void __launch_bounds__(THREADS)
     constexpr uint32_t AU = L::kAU;
     constexpr int W = THREADS / 32;
     constexpr int PER = THREADS / 32;  // count-matrix entries per lane in a row scan
+    constexpr int LR = (ITEMS + 7) / 8;
     static_assert(M <= 16 && M >= 2, "class bound");
-    static_assert(ITEMS <= 16, "local ranks are 4-bit");
+    static_assert(M <= W * 2, "each warp scans at most two rows");
+    static_assert(ITEMS == 16 || ITEMS == 8, "64 bytes of 4- or 8-byte elements");
     static_assert(PER == 8, "row scan loads 8 entries per lane");
     static_assert(ROWS <= 256, "TMA box height");
 
@@ -498,7 +502,8 @@ __global__ void __launch_bounds__(THREADS)
     uint32_t* cnt_sm = reinterpret_cast<uint32_t*>(base + L::kRingBytes + L::kStageBytes);
 
     __shared__ __align__(8) uint64_t bars[STAGES];
-    __shared__ uint32_t cursor[M], run_start[M], run_cnt[M], run_dst[M], rowtot[M];
+    __shared__ uint32_t cursor[2][M];  // ping-pong by tile parity
+    __shared__ uint32_t run_start[M], run_cnt[M], run_dst[M], rowtot[M];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t G = a.num_chunks, k = blockIdx.x;
@@ -512,7 +517,8 @@ __global__ void __launch_bounds__(THREADS)
         static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
     const bool tma_ok = a.use_tma != 0;
 
-    if (tid < M) cursor[tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
+    if (tid < M)
+        cursor[0][tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
     if (tid == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
@@ -535,16 +541,17 @@ __global__ void __launch_bounds__(THREADS)
         for (uint32_t i = 0; i < STAGES && i < cnt; i++) issue(i);
 
     const uint32_t e0 = tid * ITEMS;  // this thread's first tile-local element
+    uint32_t* my_cnt = cnt_sm + tid;  // column of this thread: my_cnt[c * THREADS]
     for (uint32_t i = 0; i < cnt; i++) {
         const uint32_t tile = t1 - 1u - i;
         const uint64_t ts = static_cast<uint64_t>(tile) * TILE;
         const uint32_t valid = static_cast<uint32_t>(min(static_cast<uint64_t>(TILE), a.n - ts));
-        const bool from_ring = tma_ok && valid == TILE;
+        const bool full = valid == TILE;
         const bool ok = mbar_wait_bounded(&bars[i % STAGES], (i / STAGES) & 1u);
 
         // ---- pass 1: take 64 contiguous bytes, classify, local ranks
         V v[ITEMS];
-        if (from_ring) {
+        if (tma_ok && full) {
             const unsigned char* tb =
                 reinterpret_cast<const unsigned char*>(ring + (i % STAGES) * TILE);
             const uint32_t row = static_cast<uint32_t>(tid) >> 1;
@@ -554,26 +561,39 @@ __global__ void __launch_bounds__(THREADS)
                 const uint4 r = *reinterpret_cast<const uint4*>(tb + row * 128u + chunk * 16u);
                 unpack16_to<V>(r, &v[q * AU]);
             }
+        } else if (full) {
+#pragma unroll
+            for (int j = 0; j < ITEMS; j++) v[j] = in[ts + e0 + j];
         } else {
 #pragma unroll
-            for (int j = 0; j < ITEMS; j++)
-                v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
+            for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
         }
-        ByteCounts<M> bc;
-        bc.init();
-        uint32_t lr[(ITEMS + 7) / 8];
+        NibbleCounts<M> nc;
+        nc.init();
+        uint32_t lr[LR];
 #pragma unroll
-        for (int q = 0; q < (ITEMS + 7) / 8; q++) lr[q] = 0;
+        for (int q = 0; q < LR; q++) lr[q] = 0;
+        uint32_t last_c = M;  // class of element 15 (not in the nibbles)
+        if (full) {
 #pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            if (e0 + j < valid) {
+            for (int j = 0; j < ITEMS; j++) {
                 const uint32_t c = d(v[j]);
-                lr[j >> 3] |= bc.get(c) << (4 * (j & 7));
-                bc.inc(c);
+                lr[j >> 3] += nc.get(c) << (4 * (j & 7));
+                if (j < 15) nc.inc(c); else last_c = c;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < ITEMS; j++) {
+                if (e0 + j < valid) {
+                    const uint32_t c = d(v[j]);
+                    lr[j >> 3] += nc.get(c) << (4 * (j & 7));
+                    if (j < 15) nc.inc(c); else last_c = c;
+                }
             }
         }
 #pragma unroll
-        for (int c = 0; c < M; c++) cnt_sm[c * THREADS + tid] = bc.get(c);
+        for (int c = 0; c < M; c++)
+            my_cnt[c * THREADS] = nc.get(c) + (static_cast<uint32_t>(c) == last_c ? 1u : 0u);
         if (__syncthreads_or(!ok)) {  // (A)
             if (tid == 0) {
                 atomicOr(a.error, kErrTimeout);
@@ -586,60 +606,89 @@ __global__ void __launch_bounds__(THREADS)
         // The ring slot is consumed (values are in registers): refill it now.
         if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
 
-        // ---- row scans of the [class][thread] count matrix -> exclusive prefixes
-        for (int c = warp; c < M; c += W) {
-            uint32_t* rowp = cnt_sm + c * THREADS + lane * PER;
-            const uint4 x0 = *reinterpret_cast<const uint4*>(rowp);
-            const uint4 x1 = *reinterpret_cast<const uint4*>(rowp + 4);
-            const uint32_t x[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-            uint32_t tot = 0;
+        // ---- row scans of the [class][thread] count matrix: warp w owns
+        // rows w and w + W; the prefixes stay in registers until the class
+        // runs are known
+        uint32_t pre[2][PER];
+        uint32_t rtot[2] = {0u, 0u};
 #pragma unroll
-            for (int q = 0; q < 8; q++) tot += x[q];
-            const uint32_t incl = warp_incl_scan(tot);
-            uint32_t run = incl - tot;
-            uint32_t y[8];
+        for (int h = 0; h < 2; h++) {
+            const int c = warp + h * W;
+            if (c < M) {
+                const uint32_t* rowp = cnt_sm + c * THREADS + lane * PER;
+                const uint4 x0 = *reinterpret_cast<const uint4*>(rowp);
+                const uint4 x1 = *reinterpret_cast<const uint4*>(rowp + 4);
+                const uint32_t x[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                uint32_t tot = 0;
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                y[q] = run;
-                run += x[q];
+                for (int q = 0; q < 8; q++) tot += x[q];
+                const uint32_t incl = warp_incl_scan(tot);
+                uint32_t run = incl - tot;
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    pre[h][q] = run;
+                    run += x[q];
+                }
+                rtot[h] = __shfl_sync(0xffffffffu, incl, 31);
+                if (lane == 31) rowtot[c] = incl;
             }
-            *reinterpret_cast<uint4*>(rowp) = make_uint4(y[0], y[1], y[2], y[3]);
-            *reinterpret_cast<uint4*>(rowp + 4) = make_uint4(y[4], y[5], y[6], y[7]);
-            if (lane == 31) rowtot[c] = incl;
         }
         // the stage buffer about to be rewritten was last read by the bulk
         // stores of tile i-2: let them finish reading it
         if (tid < M) bulk_wait_read<1>();
         __syncthreads();  // (B)
 
-        // ---- class runs: destination (chunk walked backwards) and stage slot
-        // with the same 16-byte phase as the destination
-        if (tid == 0) {
-            uint32_t end = 0;
+        // ---- class runs (every warp, lanes = classes): destination of run c
+        // (chunk walked backwards) and its stage slot, at the destination's
+        // 16-byte phase within kAU slots of slack per run
+        {
+            const uint32_t par = i & 1u;
+            const uint32_t c = static_cast<uint32_t>(lane);
+            const uint32_t cc = c < static_cast<uint32_t>(M) ? rowtot[c] : 0u;
+            const uint32_t dst = c < static_cast<uint32_t>(M) ? cursor[par][c] - cc : 0u;
+            const uint32_t room = cc + (c < static_cast<uint32_t>(M) ? AU : 0u);
+            const uint32_t q0 = warp_incl_scan(room) - room;
+            const uint32_t st = q0 + (((out_phase + dst) - q0) & (AU - 1u));
 #pragma unroll
-            for (int c = 0; c < M; c++) {
-                const uint32_t cc = rowtot[c];
-                const uint32_t dst = cursor[c] - cc;
-                cursor[c] = dst;
-                const uint32_t want = (out_phase + dst) & (AU - 1u);
-                const uint32_t s = end + ((want - end) & (AU - 1u));
-                run_start[c] = s;
+            for (int h = 0; h < 2; h++) {
+                const int row = warp + h * W;
+                if (row < M) {
+                    const uint32_t add = __shfl_sync(0xffffffffu, st, row);
+                    uint32_t* rowp = cnt_sm + row * THREADS + lane * PER;
+                    *reinterpret_cast<uint4*>(rowp) =
+                        make_uint4(pre[h][0] + add, pre[h][1] + add, pre[h][2] + add, pre[h][3] + add);
+                    *reinterpret_cast<uint4*>(rowp + 4) =
+                        make_uint4(pre[h][4] + add, pre[h][5] + add, pre[h][6] + add, pre[h][7] + add);
+                }
+            }
+            if (warp == 0 && c < static_cast<uint32_t>(M)) {
+                cursor[par ^ 1u][c] = dst;
+                run_start[c] = st;
                 run_cnt[c] = cc;
                 run_dst[c] = dst;
-                end = s + cc;
             }
+            (void)rtot;
         }
         __syncthreads();  // (C)
 
         // ---- pass 2: scatter into the class-sorted stage
         V* stg = stage + (i & 1u) * L::kStageElems;
+        if (full) {
 #pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            if (e0 + j < valid) {
+            for (int j = 0; j < ITEMS; j++) {
                 const uint32_t c = d(v[j]);
-                const uint32_t slot = run_start[c] + cnt_sm[c * THREADS + tid] +
-                                      ((lr[j >> 3] >> (4 * (j & 7))) & 15u);
+                const uint32_t slot = my_cnt[c * THREADS] + ((lr[j >> 3] >> (4 * (j & 7))) & 15u);
                 stg[slot] = v[j];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < ITEMS; j++) {
+                if (e0 + j < valid) {
+                    const uint32_t c = d(v[j]);
+                    const uint32_t slot =
+                        my_cnt[c * THREADS] + ((lr[j >> 3] >> (4 * (j & 7))) & 15u);
+                    stg[slot] = v[j];
+                }
             }
         }
         fence_proxy_async_smem();
