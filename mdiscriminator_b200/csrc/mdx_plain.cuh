@@ -456,8 +456,8 @@ struct ScatterTmaSmem {
     // every class run gets kAU slots of slack for its 16-byte phase
     static constexpr int kStageElems = kTile + static_cast<int>(kAU) * M;
     static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
-    static constexpr size_t kStageBytes = 2ull * kStageElems * sizeof(V);
-    static constexpr size_t kCntBytes = static_cast<size_t>(M) * THREADS * 4;
+    static constexpr size_t kStageBytes = static_cast<size_t>(kStageElems) * sizeof(V);
+    static constexpr size_t kCntBytes = static_cast<size_t>(M) * THREADS * 2;  // u16 counts
     // +1024: the ring is re-aligned to 1024 bytes (128-byte swizzle atoms)
     static constexpr size_t kBytes = 1024 + kRingBytes + kStageBytes + kCntBytes;
 };
@@ -475,10 +475,11 @@ struct ScatterTmaSmem {
 //  * every class run is placed in the stage at the same 16-byte phase as its
 //    destination, so its aligned interior leaves by one bulk store
 //    (cp.async.bulk shared->global) and only the < 16-byte head and tail of a
-//    run are written by threads.  The stage is double buffered and a buffer is
-//    rewritten only after its bulk stores have read it.
+//    run are written by threads.  The stage is rewritten only after the bulk
+//    stores of the previous tile have read it (they have the whole next pass 1
+//    and row scan to do so).
 template <class V, class D, int M, int THREADS, int STAGES>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 64 registers
     plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
     using L = ScatterTmaSmem<V, THREADS, STAGES, M>;
     constexpr int ITEMS = L::kItems;
@@ -493,13 +494,14 @@ __global__ void __launch_bounds__(THREADS)
     static_assert(ITEMS == 16 || ITEMS == 8, "64 bytes of 4- or 8-byte elements");
     static_assert(PER == 8, "row scan loads 8 entries per lane");
     static_assert(ROWS <= 256, "TMA box height");
+    static_assert(L::kStageElems < 65536, "stage slots are kept in 16 bits");
 
     extern __shared__ unsigned char smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     unsigned char* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
     V* ring = reinterpret_cast<V*>(base);
     V* stage = reinterpret_cast<V*>(base + L::kRingBytes);
-    uint32_t* cnt_sm = reinterpret_cast<uint32_t*>(base + L::kRingBytes + L::kStageBytes);
+    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(base + L::kRingBytes + L::kStageBytes);
 
     __shared__ __align__(8) uint64_t bars[STAGES];
     __shared__ uint32_t cursor[2][M];  // ping-pong by tile parity
@@ -541,7 +543,7 @@ __global__ void __launch_bounds__(THREADS)
         for (uint32_t i = 0; i < STAGES && i < cnt; i++) issue(i);
 
     const uint32_t e0 = tid * ITEMS;  // this thread's first tile-local element
-    uint32_t* my_cnt = cnt_sm + tid;  // column of this thread: my_cnt[c * THREADS]
+    uint16_t* my_cnt = cnt_sm + tid;  // column of this thread: my_cnt[c * THREADS]
     for (uint32_t i = 0; i < cnt; i++) {
         const uint32_t tile = t1 - 1u - i;
         const uint64_t ts = static_cast<uint64_t>(tile) * TILE;
@@ -592,8 +594,8 @@ __global__ void __launch_bounds__(THREADS)
             }
         }
 #pragma unroll
-        for (int c = 0; c < M; c++)
-            my_cnt[c * THREADS] = nc.get(c) + (static_cast<uint32_t>(c) == last_c ? 1u : 0u);
+        for (int c = 0; c < M; c++) my_cnt[c * THREADS] = static_cast<uint16_t>(nc.get(c));
+        if (last_c < static_cast<uint32_t>(M)) my_cnt[last_c * THREADS] += 1;
         if (__syncthreads_or(!ok)) {  // (A)
             if (tid == 0) {
                 atomicOr(a.error, kErrTimeout);
@@ -615,10 +617,9 @@ __global__ void __launch_bounds__(THREADS)
         for (int h = 0; h < 2; h++) {
             const int c = warp + h * W;
             if (c < M) {
-                const uint32_t* rowp = cnt_sm + c * THREADS + lane * PER;
-                const uint4 x0 = *reinterpret_cast<const uint4*>(rowp);
-                const uint4 x1 = *reinterpret_cast<const uint4*>(rowp + 4);
-                const uint32_t x[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                const uint4 xw = *reinterpret_cast<const uint4*>(cnt_sm + c * THREADS + lane * PER);
+                const uint32_t x[8] = {xw.x & 0xffffu, xw.x >> 16, xw.y & 0xffffu, xw.y >> 16,
+                                       xw.z & 0xffffu, xw.z >> 16, xw.w & 0xffffu, xw.w >> 16};
                 uint32_t tot = 0;
 #pragma unroll
                 for (int q = 0; q < 8; q++) tot += x[q];
@@ -633,9 +634,6 @@ __global__ void __launch_bounds__(THREADS)
                 if (lane == 31) rowtot[c] = incl;
             }
         }
-        // the stage buffer about to be rewritten was last read by the bulk
-        // stores of tile i-2: let them finish reading it
-        if (tid < M) bulk_wait_read<1>();
         __syncthreads();  // (B)
 
         // ---- class runs (every warp, lanes = classes): destination of run c
@@ -653,12 +651,14 @@ __global__ void __launch_bounds__(THREADS)
             for (int h = 0; h < 2; h++) {
                 const int row = warp + h * W;
                 if (row < M) {
+                    // slots < kStageElems < 2^16: pairs of u16 prefixes per word
                     const uint32_t add = __shfl_sync(0xffffffffu, st, row);
-                    uint32_t* rowp = cnt_sm + row * THREADS + lane * PER;
-                    *reinterpret_cast<uint4*>(rowp) =
-                        make_uint4(pre[h][0] + add, pre[h][1] + add, pre[h][2] + add, pre[h][3] + add);
-                    *reinterpret_cast<uint4*>(rowp + 4) =
-                        make_uint4(pre[h][4] + add, pre[h][5] + add, pre[h][6] + add, pre[h][7] + add);
+                    const uint32_t add2 = add | (add << 16);
+                    *reinterpret_cast<uint4*>(cnt_sm + row * THREADS + lane * PER) =
+                        make_uint4((pre[h][0] | (pre[h][1] << 16)) + add2,
+                                   (pre[h][2] | (pre[h][3] << 16)) + add2,
+                                   (pre[h][4] | (pre[h][5] << 16)) + add2,
+                                   (pre[h][6] | (pre[h][7] << 16)) + add2);
                 }
             }
             if (warp == 0 && c < static_cast<uint32_t>(M)) {
@@ -669,10 +669,13 @@ __global__ void __launch_bounds__(THREADS)
             }
             (void)rtot;
         }
+        // the stage is about to be rewritten: the bulk stores of the previous
+        // tile must have finished reading it
+        if (tid < M) bulk_wait_read<0>();
         __syncthreads();  // (C)
 
         // ---- pass 2: scatter into the class-sorted stage
-        V* stg = stage + (i & 1u) * L::kStageElems;
+        V* stg = stage;
         if (full) {
 #pragma unroll
             for (int j = 0; j < ITEMS; j++) {
