@@ -61,8 +61,13 @@ typedef struct {
  * in mdiscr (cuda_code/MdiscrHost_optimized_clean.cu.h:43-45). */
 size_t mdx_workspace_size(uint64_t n, mdx_elem elem, uint32_t m);
 
-/* Bytes of workspace the segmented entry points need. */
+/* Bytes of workspace mdx_partition_segmented needs.  Replaces the nine
+ * per-call N-sized cudaMallocs of mdiscrSegm (cuda_code/MdiscrSegmHost.cu.h:60-68). */
 size_t mdx_segmented_workspace_size(uint64_t n, uint64_t num_segments, mdx_elem elem, uint32_t m);
+
+/* Bytes of workspace mdx_mdiscr_segm (head-flag segment input) needs: the
+ * segmented workspace for up to n segments plus room for the offsets. */
+size_t mdx_mdiscr_segm_workspace_size(uint64_t n, mdx_elem elem, uint32_t m);
 
 /* Zero a freshly allocated workspace (once, before its first use). */
 mdx_status mdx_workspace_init(void* d_ws, size_t ws_bytes, mdx_stream_t stream);
@@ -119,6 +124,8 @@ mdx_status mdx_mdiscr(uint32_t n, uint32_t num_hwd_thds, const void* d_in, void*
  * d_headflags    : device u32[n] -- per-segment head-flag sizes relative to the
  *                  segment start, the form mdiscrSegm writes into new_sizes
  *                  (MdiscrSegmKernels.cu.h:89-114); may be NULL.
+ * Segments that do not tile [0, n) exactly latch MDX_ERR_SEGMENTS in the
+ * workspace (read it with mdx_workspace_error).  m <= 16 in this build.
  */
 mdx_status mdx_partition_segmented(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
                                    mdx_discr discr, const uint64_t* d_offsets,
@@ -132,9 +139,9 @@ mdx_status mdx_partition_segmented(const void* d_in, void* d_out, uint64_t n, md
  *     (cuda_code/MdiscrSegmHost.cu.h:36-42)
  * d_segment_sizes: device i32[n], length of the segment at each segment start,
  * 0 elsewhere.  d_new_sizes: device i32[n] (head-flag output).  Needs a
- * workspace of mdx_segmented_workspace_size(n, n, elem, m) bytes (the segment
+ * workspace of mdx_mdiscr_segm_workspace_size(n, elem, m) bytes (the segment
  * count is only known on the device).  Malformed flags latch
- * MDX_ERR_SEGMENTS in the workspace.
+ * MDX_ERR_SEGMENTS in the workspace (read it with mdx_workspace_error).
  */
 mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segment_sizes,
                            void* d_out, int32_t* d_new_sizes, mdx_elem elem, mdx_discr discr,

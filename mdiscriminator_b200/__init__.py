@@ -77,6 +77,8 @@ def lib() -> ctypes.CDLL:
             L.mdx_workspace_size.restype = sz
             L.mdx_segmented_workspace_size.argtypes = [u64, u64, ctypes.c_int, u32]
             L.mdx_segmented_workspace_size.restype = sz
+            L.mdx_mdiscr_segm_workspace_size.argtypes = [u64, ctypes.c_int, u32]
+            L.mdx_mdiscr_segm_workspace_size.restype = sz
             L.mdx_workspace_init.argtypes = [vp, sz, vp]
             L.mdx_workspace_init.restype = st
             L.mdx_workspace_error.argtypes = [vp, vp]
@@ -330,7 +332,9 @@ def mdiscr_segm(d_in, d_segment_sizes, discr, d_out=None, d_new_sizes=None,
     if d_new_sizes is None:
         d_new_sizes = torch.empty(n, dtype=torch.int32, device=d_in.device)
     _require_cuda(d_out, d_new_sizes)
-    need = segmented_workspace_size(n, n, elem, dc.m)
+    need = int(lib().mdx_mdiscr_segm_workspace_size(n, elem, dc.m))
+    if need == 0:
+        raise MdxError(MDX_ERR_INVALID, "mdx_mdiscr_segm_workspace_size")
     ws = ws or workspace(need, d_in.device, stream)
     st = lib().mdx_mdiscr_segm(n, ctypes.c_void_p(d_in.data_ptr()),
                                ctypes.c_void_p(d_segment_sizes.data_ptr()),

@@ -260,6 +260,127 @@ mdx_status dispatch_plain(const void* in, void* out, uint64_t n, mdx_discr dc, u
     return dispatch_plain_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, sz, hf, ws, L, st, ev);
 }
 
+// ------------------------------------------------------------- segmented --
+constexpr int kPlanThreads = 256;
+constexpr uint32_t kMaxPlanBlocks = 1024;
+constexpr int kFlagsTile = 4096;
+
+inline uint32_t window_elems(mdx_elem e) { return tile_elems(e); }
+
+struct SegLayout {
+    size_t span_loc, blk_tot, lw, status, excl, offsets, flag_status, total;
+    uint64_t max_entries;
+};
+
+// flags_form: room for n+1 offsets and the converter's tile status words.
+inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool flags_form) {
+    const uint32_t M = class_bound(m);
+    const uint64_t P = window_elems(e);
+    const uint64_t NW = (n + P - 1) / P;
+    SegLayout L;
+    L.max_entries = 2 * NW + 2;
+    L.span_loc = kHeaderBytes;
+    L.blk_tot = align_up(L.span_loc + 4 * (S + 1), kAlign);
+    L.lw = align_up(L.blk_tot + 4 * kMaxPlanBlocks, kAlign);
+    L.status = align_up(L.lw + sizeof(LwEntry) * L.max_entries, kAlign);
+    L.excl = align_up(L.status + 8ull * M * L.max_entries, kAlign);
+    L.offsets = align_up(L.excl + 4ull * M * L.max_entries, kAlign);
+    L.flag_status = L.offsets;
+    L.total = L.offsets;
+    if (flags_form) {
+        L.flag_status = align_up(L.offsets + 8 * (n + 1), kAlign);
+        L.total = align_up(L.flag_status + 8 * ((n + kFlagsTile - 1) / kFlagsTile + 1), kAlign);
+    }
+    return L;
+}
+
+inline uint32_t plan_blocks_for(uint64_t S_bound) {
+    uint64_t g = (S_bound + 2047) / 2048;
+    if (g < 1) g = 1;
+    if (g > kMaxPlanBlocks) g = kMaxPlanBlocks;
+    return static_cast<uint32_t>(g);
+}
+
+template <class V, class D, int M>
+mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
+                    const uint64_t* d_offsets, uint64_t S, uint64_t S_bound, const int32_t* in_flags,
+                    uint32_t* d_seg_sizes, uint32_t* d_headflags, unsigned char* ws,
+                    const SegLayout& L, cudaStream_t st) {
+    using SL = SegSmem<V, M, kThreads>;
+    constexpr int P = SL::kTile;
+    auto main_fn = seg_main<V, D, M, kThreads>;
+    int blocks = 0, sms = 0;
+    if (occupancy(reinterpret_cast<const void*>(main_fn), SL::kBytes, &blocks, &sms) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    SegArgs a;
+    a.in = d_in;
+    a.out = d_out;
+    a.n = n;
+    a.offsets = d_offsets;
+    a.num_segs = S;
+    a.seg_sizes = d_seg_sizes;
+    a.headflags = d_headflags;
+    a.in_flags = in_flags;
+    a.m = m;
+    a.hdr = reinterpret_cast<SegHeader*>(ws);
+    a.span_loc = reinterpret_cast<uint32_t*>(ws + L.span_loc);
+    a.blk_tot = reinterpret_cast<uint32_t*>(ws + L.blk_tot);
+    a.lw = reinterpret_cast<LwEntry*>(ws + L.lw);
+    a.status = reinterpret_cast<uint64_t*>(ws + L.status);
+    a.excl = reinterpret_cast<uint32_t*>(ws + L.excl);
+    a.plan_blocks = plan_blocks_for(S_bound);
+    a.max_entries = static_cast<uint32_t>(L.max_entries);
+    if (d_headflags != nullptr &&
+        cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), st) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    // Look-back words start from zero every call: the workspace's layout moves
+    // with n, S and m, so the epoch tag alone cannot tell a status word from
+    // another call's data.
+    if (cudaMemsetAsync(a.status, 0, L.max_entries * M * sizeof(uint64_t), st) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    seg_plan_spans<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
+    seg_plan_emit<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
+    main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d);
+    return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+}
+
+template <class V, class D>
+mdx_status dispatch_segm_m(const void* in, void* out, uint64_t n, D d, uint32_t m,
+                           const uint64_t* offs, uint64_t S, uint64_t Sb, const int32_t* fl,
+                           uint32_t* sz, uint32_t* hf, unsigned char* ws, const SegLayout& L,
+                           cudaStream_t st) {
+    switch (class_bound(m)) {
+        case 2: return run_segm<V, D, 2>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
+        case 4: return run_segm<V, D, 4>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
+        case 8: return run_segm<V, D, 8>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
+        case 16: return run_segm<V, D, 16>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
+        default: return MDX_ERR_UNSUPPORTED;
+    }
+}
+
+template <class V>
+mdx_status dispatch_segm(const void* in, void* out, uint64_t n, mdx_discr dc, const uint64_t* offs,
+                         uint64_t S, uint64_t Sb, const int32_t* fl, uint32_t* sz, uint32_t* hf,
+                         unsigned char* ws, const SegLayout& L, cudaStream_t st) {
+    if (dc.kind == MDX_DISCR_MASK)
+        return dispatch_segm_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, offs, S, Sb, fl, sz, hf,
+                                  ws, L, st);
+    return dispatch_segm_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, offs, S, Sb, fl, sz, hf, ws,
+                              L, st);
+}
+
+mdx_status check_io(const void* d_in, void* d_out, uint64_t n, mdx_elem elem) {
+    if (n == 0) return MDX_OK;
+    if (d_in == nullptr || d_out == nullptr) return MDX_ERR_INVALID;
+    const size_t w = elem_bytes(elem);
+    const char* ib = static_cast<const char*>(d_in);
+    const char* ob = static_cast<const char*>(d_out);
+    if (ib < ob + n * w && ob < ib + n * w) return MDX_ERR_INVALID;
+    if (reinterpret_cast<uintptr_t>(d_in) % w || reinterpret_cast<uintptr_t>(d_out) % w)
+        return MDX_ERR_INVALID;
+    return MDX_OK;
+}
+
 }  // namespace
 }  // namespace mdx
 
@@ -359,19 +480,74 @@ mdx_status mdx_mdiscr(uint32_t n, uint32_t num_hwd_thds, const void* d_in, void*
 
 size_t mdx_segmented_workspace_size(uint64_t n, uint64_t num_segments, mdx_elem elem,
                                     uint32_t m) {
-    (void)n; (void)num_segments; (void)elem; (void)m;
-    return kHeaderBytes;
+    if (check_elem(elem) != MDX_OK || m < 1 || m > MDX_MAX_CLASSES) return 0;
+    return seg_layout(n, num_segments, elem, m, false).total;
 }
 
-mdx_status mdx_partition_segmented(const void*, void*, uint64_t, mdx_elem, mdx_discr,
-                                   const uint64_t*, uint64_t, uint32_t*, uint32_t*, void*, size_t,
-                                   mdx_stream_t) {
-    return MDX_ERR_UNSUPPORTED;
+size_t mdx_mdiscr_segm_workspace_size(uint64_t n, mdx_elem elem, uint32_t m) {
+    if (check_elem(elem) != MDX_OK || m < 1 || m > MDX_MAX_CLASSES) return 0;
+    return seg_layout(n, n, elem, m, true).total;
 }
 
-mdx_status mdx_mdiscr_segm(uint32_t, const void*, const int32_t*, void*, int32_t*, mdx_elem,
-                           mdx_discr, void*, size_t, mdx_stream_t) {
-    return MDX_ERR_UNSUPPORTED;
+mdx_status mdx_partition_segmented(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                   mdx_discr discr, const uint64_t* d_offsets,
+                                   uint64_t num_segments, uint32_t* d_seg_sizes,
+                                   uint32_t* d_headflags, void* d_ws, size_t ws_bytes,
+                                   mdx_stream_t stream) {
+    mdx_status s = check_elem(elem);
+    if (s != MDX_OK) return s;
+    if ((s = check_discr(discr)) != MDX_OK) return s;
+    if (n > MDX_MAX_ELEMS || num_segments > MDX_MAX_ELEMS) return MDX_ERR_INVALID;
+    if ((s = check_io(d_in, d_out, n, elem)) != MDX_OK) return s;
+    if (num_segments == 0) return n == 0 ? MDX_OK : MDX_ERR_SEGMENTS;
+    if (d_offsets == nullptr) return MDX_ERR_INVALID;
+    if (class_bound(discr.m) > 16) return MDX_ERR_UNSUPPORTED;
+    const SegLayout L = seg_layout(n, num_segments, elem, discr.m, false);
+    if (d_ws == nullptr || ws_bytes < L.total) return MDX_ERR_WORKSPACE;
+    if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    unsigned char* ws = static_cast<unsigned char*>(d_ws);
+    if (elem == MDX_ELEM_U32)
+        return dispatch_segm<uint32_t>(d_in, d_out, n, discr, d_offsets, num_segments, num_segments,
+                                       nullptr, d_seg_sizes, d_headflags, ws, L, st);
+    return dispatch_segm<uint64_t>(d_in, d_out, n, discr, d_offsets, num_segments, num_segments,
+                                   nullptr, d_seg_sizes, d_headflags, ws, L, st);
+}
+
+mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segment_sizes,
+                           void* d_out, int32_t* d_new_sizes, mdx_elem elem, mdx_discr discr,
+                           void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
+    mdx_status s = check_elem(elem);
+    if (s != MDX_OK) return s;
+    if ((s = check_discr(discr)) != MDX_OK) return s;
+    if ((s = check_io(d_in, d_out, n, elem)) != MDX_OK) return s;
+    if (n == 0) return MDX_OK;
+    if (d_segment_sizes == nullptr) return MDX_ERR_INVALID;
+    if (class_bound(discr.m) > 16) return MDX_ERR_UNSUPPORTED;
+    const SegLayout L = seg_layout(n, n, elem, discr.m, true);
+    if (d_ws == nullptr || ws_bytes < L.total) return MDX_ERR_WORKSPACE;
+    if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    unsigned char* ws = static_cast<unsigned char*>(d_ws);
+    uint64_t* offs = reinterpret_cast<uint64_t*>(ws + L.offsets);
+    int blocks = 0, sms = 0;
+    auto conv = seg_flags_to_offsets<kThreads, kFlagsTile>;
+    if (occupancy(reinterpret_cast<const void*>(conv), 0, &blocks, &sms) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    const uint32_t tiles = static_cast<uint32_t>((n + kFlagsTile - 1) / kFlagsTile);
+    uint32_t G = static_cast<uint32_t>(blocks) * sms;
+    if (G > tiles) G = tiles;
+    if (cudaMemsetAsync(ws + L.flag_status, 0, sizeof(uint64_t) * (tiles + 1), st) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    conv<<<G, kThreads, 0, st>>>(d_segment_sizes, n, offs, reinterpret_cast<SegHeader*>(ws),
+                                 reinterpret_cast<uint64_t*>(ws + L.flag_status));
+    if (cudaGetLastError() != cudaSuccess) return MDX_ERR_CUDA;
+    uint32_t* hf = reinterpret_cast<uint32_t*>(d_new_sizes);
+    if (elem == MDX_ELEM_U32)
+        return dispatch_segm<uint32_t>(d_in, d_out, n, discr, offs, kSegsOnDevice, n,
+                                       d_segment_sizes, nullptr, hf, ws, L, st);
+    return dispatch_segm<uint64_t>(d_in, d_out, n, discr, offs, kSegsOnDevice, n, d_segment_sizes,
+                                   nullptr, hf, ws, L, st);
 }
 
 const char* mdx_strerror(mdx_status s) {

@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     static_assert(ROWS <= 256, "TMA box height");
     static_assert(L::kStageElems < 65536, "stage slots are kept in 16 bits");
 
-    extern __shared__ unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     unsigned char* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
     V* ring = reinterpret_cast<V*>(base);

@@ -1,0 +1,197 @@
+"""Parity of the segmented CUDA partition with the CPU oracle (seqMdiscr per
+segment, as the reference's MdiscrSegmTest.cu:8-41 validates mdiscrSegm).
+
+Bit-exact on the permuted array, the per-segment class sizes (S x m) and the
+per-segment head-flag sizes, for the offsets form and the reference's
+head-flag form.  Windows are 4096 elements for u32 and 2048 for records, so
+the lengths below straddle the small/large boundary on purpose.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+P_U32 = 4096
+
+
+def offsets_from_lengths(lengths):
+    return np.concatenate([[0], np.cumsum(np.asarray(lengths, dtype=np.uint64))]).astype(np.uint64)
+
+
+def lognormal_lengths(S, seed, mu=np.log(1024), sigma=1.5, hi=1 << 22):
+    rng = np.random.default_rng(seed)
+    return np.clip(np.rint(rng.lognormal(mu, sigma, size=S)), 1, hi).astype(np.int64)
+
+
+def run_offsets(torch, x, offs, m, kind="mod"):
+    import mdiscriminator_b200 as mdx
+    d = torch.from_numpy(x).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    out, seg_sizes, hf = mdx.partition_segmented(d, do, (kind, m), headflags=True)
+    torch.cuda.synchronize()
+    err = mdx.workspace(0).error()
+    return out.cpu().numpy(), seg_sizes.cpu().numpy(), hf.cpu().numpy(), err
+
+
+def check(torch, x, offs, m, kind="mod"):
+    import mdiscriminator_b200 as mdx
+    k = oracle.DISCR_MASK if kind == "mask" else oracle.DISCR_MOD
+    eo, es, ef = oracle.partition_segmented(x, offs, m, kind=k, headflags=True)
+    go, gs, gf, err = run_offsets(torch, x, offs, m, kind)
+    assert err == mdx.MDX_OK, mdx.strerror(err)
+    assert np.array_equal(gs, es), "segment class sizes differ"
+    if not np.array_equal(go, eo):
+        bad = np.nonzero(go != eo)[0]
+        seg = np.searchsorted(offs, bad[0], side="right") - 1
+        raise AssertionError(f"output differs at {bad.size} positions, first {bad[:6]} "
+                             f"(segment {seg}, length {int(offs[seg + 1] - offs[seg])})")
+    assert np.array_equal(gf, ef), "head flags differ"
+
+
+def test_known_answer_head_flag_form(cuda_ready):
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    with open(os.path.join(HERE, "golden", "known_answers.json")) as f:
+        ka = json.load(f)["segmented"]
+    x = torch.tensor(ka["in"], dtype=torch.int32, device="cuda")
+    flags = torch.tensor(ka["segment_sizes"], dtype=torch.int32, device="cuda")
+    out, new_sizes = mdx.mdiscr_segm(x, flags, ("mod", ka["m"]))
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == ka["out"]
+    assert new_sizes.cpu().tolist() == ka["new_sizes"]
+
+
+@pytest.mark.parametrize("m", [1, 2, 3, 4, 8, 16])
+def test_lognormal_batch(cuda_ready, m):
+    lengths = lognormal_lengths(1500, 10 + m)
+    offs = offsets_from_lengths(lengths)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 20 + m)
+    check(cuda_ready, x, offs, m)
+
+
+@pytest.mark.parametrize("m", [2, 4, 8, 16])
+def test_window_edges(cuda_ready, m):
+    P = P_U32
+    lengths = [1, P - 1, P, P + 1, 2 * P, 2 * P + 1, 3, 5 * P + 7, 31, 32, 33, P, 1, 7 * P - 3,
+               2, P + 2, 64, 10 * P, 1, 1, 1, 3 * P + 1]
+    offs = offsets_from_lengths(lengths)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 77 + m)
+    check(cuda_ready, x, offs, m, "mask")
+    # the same lengths shifted by one element, so every window boundary moves
+    offs2 = offsets_from_lengths([1] + lengths)
+    x2 = oracle.fill_uniform_u32(int(offs2[-1]), 78 + m)
+    check(cuda_ready, x2, offs2, m, "mask")
+
+
+def test_empty_and_tiny_segments(cuda_ready):
+    rng = np.random.default_rng(3)
+    lengths = rng.integers(0, 6, size=20000)  # includes zero-length segments
+    offs = offsets_from_lengths(lengths)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 5)
+    for m in (2, 3, 4):
+        check(cuda_ready, x, offs, m)
+
+
+def test_single_huge_segment_equals_plain(cuda_ready):
+    n = (1 << 22) + 123
+    x = oracle.fill_uniform_u32(n, 9)
+    offs = np.array([0, n], dtype=np.uint64)
+    check(cuda_ready, x, offs, 8, "mask")
+
+
+def test_mixed_large_and_small(cuda_ready):
+    rng = np.random.default_rng(4)
+    lengths = []
+    for _ in range(300):
+        r = rng.random()
+        lengths.append(int(rng.integers(1, 200)) if r < 0.6 else
+                       int(rng.integers(200, 5000)) if r < 0.9 else int(rng.integers(5000, 60000)))
+    offs = offsets_from_lengths(lengths)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 6)
+    for m, kind in ((4, "mod"), (5, "mod"), (16, "mask")):
+        check(cuda_ready, x, offs, m, kind)
+
+
+@pytest.mark.parametrize("m", [2, 4, 16])
+def test_records(cuda_ready, m):
+    lengths = lognormal_lengths(800, 30 + m, mu=np.log(700))
+    offs = offsets_from_lengths(lengths)
+    n = int(offs[-1])
+    keys = oracle.fill_uniform_u32(n, 40 + m).astype(np.uint64)
+    x = keys | (np.arange(n, dtype=np.uint64) << np.uint64(32))
+    check(cuda_ready, x, offs, m, "mask")
+
+
+def test_head_flag_form_matches_offsets_form(cuda_ready):
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    lengths = lognormal_lengths(2000, 55)
+    offs = offsets_from_lengths(lengths)
+    n = int(offs[-1])
+    x = oracle.fill_uniform_u32(n, 56)
+    flags = np.zeros(n, dtype=np.int32)
+    flags[offs[:-1].astype(np.int64)] = lengths
+    out, new_sizes = mdx.mdiscr_segm(torch.from_numpy(x).cuda(), torch.from_numpy(flags).cuda(),
+                                     ("mod", 4))
+    torch.cuda.synchronize()
+    assert mdx.workspace(0).error() == mdx.MDX_OK
+    eo, es, ef = oracle.partition_segmented(x, offs, 4, headflags=True)
+    assert np.array_equal(out.cpu().numpy(), eo)
+    assert np.array_equal(new_sizes.cpu().numpy().astype(np.uint32), ef)
+
+
+def test_repeated_calls_reuse_workspace(cuda_ready):
+    # epoch-tagged look-back words: back-to-back calls on one workspace
+    lengths = lognormal_lengths(400, 61)
+    offs = offsets_from_lengths(lengths)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 62)
+    for _ in range(4):
+        check(cuda_ready, x, offs, 4)
+
+
+def test_malformed_offsets_are_reported(cuda_ready):
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    x = torch.zeros(1000, dtype=torch.int32, device="cuda")
+    bad = torch.tensor([0, 500, 400, 1000], dtype=torch.int64, device="cuda")  # decreasing
+    mdx.partition_segmented(x, bad, ("mod", 4))
+    assert mdx.workspace(0).error() == mdx.MDX_ERR_SEGMENTS
+    short = torch.tensor([0, 500, 900], dtype=torch.int64, device="cuda")  # does not reach n
+    mdx.partition_segmented(x, short, ("mod", 4))
+    assert mdx.workspace(0).error() == mdx.MDX_ERR_SEGMENTS
+    flags = torch.zeros(1000, dtype=torch.int32, device="cuda")
+    flags[0] = 600  # next start at 600 expected, found at 500
+    flags[500] = 500
+    mdx.mdiscr_segm(x, flags, ("mod", 4))
+    assert mdx.workspace(0).error() == mdx.MDX_ERR_SEGMENTS
+    # and a good call afterwards is clean
+    lengths = lognormal_lengths(50, 1)
+    offs = offsets_from_lengths(lengths)
+    check(torch, oracle.fill_uniform_u32(int(offs[-1]), 2), offs, 4)
+
+
+def test_full_size_100k_lognormal_segments(cuda_ready):
+    """100,000 segments, lengths LogNormal(ln 1024, 1.5) clamped to [1, 2^22],
+    m = 4: checked against a segment-aware torch stable argsort (bit-exact)."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    lengths = lognormal_lengths(100_000, 2024)
+    offs = offsets_from_lengths(lengths)
+    n = int(offs[-1])
+    g = torch.Generator(device="cuda").manual_seed(7)
+    d = torch.randint(0, 1 << 31, (n,), device="cuda", dtype=torch.int64, generator=g)
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    out, seg_sizes = mdx.partition_segmented(d.to(torch.int32), do, ("mod", 4))
+    assert mdx.workspace(0).error() == mdx.MDX_OK
+    seg_id = torch.repeat_interleave(torch.arange(len(lengths), device="cuda"),
+                                     torch.from_numpy(lengths).cuda())
+    key = seg_id * 4 + (d % 4)
+    order = torch.argsort(key, stable=True)
+    assert torch.equal(out, d.to(torch.int32)[order])
+    counts = torch.bincount(key, minlength=len(lengths) * 4).view(-1, 4)
+    assert torch.equal(seg_sizes.to(torch.int64), counts)
