@@ -139,6 +139,91 @@ def make_input(torch, n, seed, device):
                          generator=g).to(torch.int32)
 
 
+def lognormal_lengths(S: int, seed: int, mu: float, sigma: float, hi: int):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return np.clip(np.rint(rng.lognormal(mu, sigma, size=S)), 1, hi).astype(np.int64)
+
+
+def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segments=2000):
+    """Batched segmented partition: 100,000 segments, lengths
+    LogNormal(ln 1024, 1.5) clamped to [1, 2^22] (~3e8 int32), m = 4,
+    class = v mod 4, as one segmented call replayed from a CUDA graph, against
+    one plain partition per segment (a CUDA graph of per-segment calls over a
+    sample of consecutive segments)."""
+    import math
+
+    import numpy as np
+    S, m = 100_000, 4
+    lengths = lognormal_lengths(S, 2024, math.log(1024), 1.5, 1 << 22)
+    offs = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)
+    n = int(offs[-1])
+    d_in = make_input(torch, n, 99, dev)
+    d_out = torch.empty_like(d_in)
+    d_offs = torch.from_numpy(offs).to(dev)
+    seg_sizes = torch.empty((S, m), dtype=torch.uint32, device=dev)
+    ws = mdx.new_workspace(mdx.segmented_workspace_size(n, S, mdx.ELEM_U32, m), dev)
+    stream = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            mdx.partition_segmented(d_in, d_offs, ("mod", m), out=d_out, seg_sizes=seg_sizes, ws=ws)
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            mdx.partition_segmented(d_in, d_offs, ("mod", m), out=d_out, seg_sizes=seg_sizes, ws=ws)
+        g.replay()
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            g.replay()
+        e1.record(stream)
+        stream.synchronize()
+    if ws.error() != mdx.MDX_OK:
+        raise SystemExit("device error in the batched measurement")
+    t_b = e0.elapsed_time(e1) * 1e-3 / steps
+    alg = 2 * n * 4 + 8 * (S + 1) + 4 * m * S
+    # one plain launch per segment, on a sample of consecutive segments
+    s0 = S // 2
+    s1 = s0 + sample_segments
+    a0, a1 = int(offs[s0]), int(offs[s1])
+    pws = mdx.new_workspace(max(mdx.workspace_size(int(lengths[s0:s1].max()), mdx.ELEM_U32, m), 1 << 20), dev)
+    sizes = torch.empty(m, dtype=torch.uint32, device=dev)
+    views = [(int(offs[s]), int(offs[s + 1])) for s in range(s0, s1)]
+    with torch.cuda.stream(stream):
+        for a, b in views[:8]:
+            mdx.partition(d_in[a:b], ("mod", m), out=d_out[a:b], sizes=sizes, ws=pws)
+        stream.synchronize()
+        gp = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gp, stream=stream):
+            for a, b in views:
+                mdx.partition(d_in[a:b], ("mod", m), out=d_out[a:b], sizes=sizes, ws=pws)
+        gp.replay()
+        stream.synchronize()
+        e0.record(stream)
+        reps = 3
+        for _ in range(reps):
+            gp.replay()
+        e1.record(stream)
+        stream.synchronize()
+    t_p = e0.elapsed_time(e1) * 1e-3 / reps
+    v_b = n / t_b / 1e9
+    v_p = (a1 - a0) / t_p / 1e9
+    del g, gp
+    return {
+        "workload": "100,000 segments, LogNormal(ln 1024, 1.5) clamped [1, 2^22], int32, m=4, "
+                    "segment offsets, one segmented launch sequence replayed from a CUDA graph",
+        "n": n, "segments": S, "value": v_b, "unit": "Gelem/s", "ms": t_b * 1e3,
+        "roofline": {"bound": "hbm", "achieved": alg / t_b / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / t_b / 1e9 / peak,
+                     "alg_bytes": "2*N*4 + 8*(S+1) + 4*m*S"},
+        "per_segment_plain": {"value": v_p, "unit": "Gelem/s",
+                              "sample": f"segments {s0}..{s1 - 1} ({a1 - a0} elements), one "
+                                        "mdx_partition per segment, CUDA graph of the calls"},
+        "speedup_vs_per_segment": v_b / v_p,
+    }
+
+
 def cpu_baseline(n_sample: int, m: int, reps: int):
     """The reference's openmpMdiscr on a bounded sample (rank 0, N=1 only)."""
     import numpy as np
@@ -208,6 +293,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-sample", type=int, default=1 << 25)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched segmented measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -336,6 +423,9 @@ def main():
                             "traffic": tr.get("scatter_kernel_bytes")},
             },
         }
+        batched = None
+        if world == 1 and not args.no_batched:
+            batched = batched_measurement(torch, mdx, dev, peak)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu, why = cpu_baseline(args.ref_sample, m, reps=3)
@@ -354,6 +444,7 @@ def main():
                     "d2h_bytes_per_step": n * 4 + m * 4},
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "batched": batched,
             "clocks": clk,
             "gpu_launches": 2 * args.steps,
         }

@@ -14,6 +14,7 @@
 #include "../../include/mdx.h"
 #include "mdx_plain.cuh"
 #include "mdx_segm.cuh"
+#include "mdx_tile.cuh"
 
 namespace mdx {
 namespace {
@@ -251,11 +252,15 @@ mdx_status dispatch_plain_m(const void* in, void* out, uint64_t n, D d, uint32_t
     }
 }
 
+// key % m == key & (m - 1) for unsigned keys when m is a power of two (Mod<4>
+// and Mod4 agree), so such MOD requests take the mask functor.
+inline bool use_mask(mdx_discr dc) { return dc.kind == MDX_DISCR_MASK || is_pow2(dc.m); }
+
 template <class V>
 mdx_status dispatch_plain(const void* in, void* out, uint64_t n, mdx_discr dc, uint32_t* sz,
                           uint32_t* hf, unsigned char* ws, const PlainLayout& L, cudaStream_t st,
                           cudaEvent_t ev) {
-    if (dc.kind == MDX_DISCR_MASK)
+    if (use_mask(dc))
         return dispatch_plain_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, sz, hf, ws, L, st, ev);
     return dispatch_plain_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, sz, hf, ws, L, st, ev);
 }
@@ -268,8 +273,9 @@ constexpr int kFlagsTile = 4096;
 inline uint32_t window_elems(mdx_elem e) { return tile_elems(e); }
 
 struct SegLayout {
-    size_t span_loc, blk_tot, lw, status, excl, offsets, flag_status, total;
-    uint64_t max_entries;
+    size_t run_loc, grp_loc, blk_runs, blk_grps, runs, groups, groups_end, status, excl, offsets,
+        flag_status, total;
+    uint64_t max_runs, max_groups;
 };
 
 // flags_form: room for n+1 offsets and the converter's tile status words.
@@ -278,13 +284,18 @@ inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool
     const uint64_t P = window_elems(e);
     const uint64_t NW = (n + P - 1) / P;
     SegLayout L;
-    L.max_entries = 2 * NW + 2;
-    L.span_loc = kHeaderBytes;
-    L.blk_tot = align_up(L.span_loc + 4 * (S + 1), kAlign);
-    L.lw = align_up(L.blk_tot + 4 * kMaxPlanBlocks, kAlign);
-    L.status = align_up(L.lw + sizeof(LwEntry) * L.max_entries, kAlign);
-    L.excl = align_up(L.status + 8ull * M * L.max_entries, kAlign);
-    L.offsets = align_up(L.excl + 4ull * M * L.max_entries, kAlign);
+    L.max_runs = 2 * NW + 2;    // runs of segments that tile [0, n): far fewer
+    L.max_groups = 2 * NW + 2;  // at most one group per half tile (+ trailing empty segments)
+    L.run_loc = kHeaderBytes;
+    L.grp_loc = align_up(L.run_loc + 4 * (S + 1), kAlign);
+    L.blk_runs = align_up(L.grp_loc + 4 * (S + 1), kAlign);
+    L.blk_grps = align_up(L.blk_runs + 4 * kMaxPlanBlocks, kAlign);
+    L.runs = align_up(L.blk_grps + 4 * kMaxPlanBlocks, kAlign);
+    L.groups = align_up(L.runs + sizeof(RunEntry) * L.max_runs, kAlign);
+    L.groups_end = align_up(L.groups + 4 * L.max_groups, kAlign);
+    L.status = align_up(L.groups_end + 4 * L.max_groups, kAlign);
+    L.excl = align_up(L.status + 8ull * M * L.max_runs, kAlign);
+    L.offsets = align_up(L.excl + 4ull * M * L.max_runs, kAlign);
     L.flag_status = L.offsets;
     L.total = L.offsets;
     if (flags_form) {
@@ -295,7 +306,7 @@ inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool
 }
 
 inline uint32_t plan_blocks_for(uint64_t S_bound) {
-    uint64_t g = (S_bound + 2047) / 2048;
+    uint64_t g = (S_bound + 511) / 512;
     if (g < 1) g = 1;
     if (g > kMaxPlanBlocks) g = kMaxPlanBlocks;
     return static_cast<uint32_t>(g);
@@ -306,9 +317,9 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
                     const uint64_t* d_offsets, uint64_t S, uint64_t S_bound, const int32_t* in_flags,
                     uint32_t* d_seg_sizes, uint32_t* d_headflags, unsigned char* ws,
                     const SegLayout& L, cudaStream_t st) {
-    using SL = SegSmem<V, M, kThreads>;
+    using SL = SegSmem<V, M, kThreads, kStages>;
     constexpr int P = SL::kTile;
-    auto main_fn = seg_main<V, D, M, kThreads>;
+    auto main_fn = seg_main<V, D, M, kThreads, kStages>;
     int blocks = 0, sms = 0;
     if (occupancy(reinterpret_cast<const void*>(main_fn), SL::kBytes, &blocks, &sms) != cudaSuccess)
         return MDX_ERR_CUDA;
@@ -323,24 +334,33 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.in_flags = in_flags;
     a.m = m;
     a.hdr = reinterpret_cast<SegHeader*>(ws);
-    a.span_loc = reinterpret_cast<uint32_t*>(ws + L.span_loc);
-    a.blk_tot = reinterpret_cast<uint32_t*>(ws + L.blk_tot);
-    a.lw = reinterpret_cast<LwEntry*>(ws + L.lw);
+    a.run_loc = reinterpret_cast<uint32_t*>(ws + L.run_loc);
+    a.grp_loc = reinterpret_cast<uint32_t*>(ws + L.grp_loc);
+    a.blk_runs = reinterpret_cast<uint32_t*>(ws + L.blk_runs);
+    a.blk_grps = reinterpret_cast<uint32_t*>(ws + L.blk_grps);
+    a.runs = reinterpret_cast<RunEntry*>(ws + L.runs);
+    a.groups = reinterpret_cast<uint32_t*>(ws + L.groups);
+    a.groups_end = reinterpret_cast<uint32_t*>(ws + L.groups_end);
     a.status = reinterpret_cast<uint64_t*>(ws + L.status);
     a.excl = reinterpret_cast<uint32_t*>(ws + L.excl);
     a.plan_blocks = plan_blocks_for(S_bound);
-    a.max_entries = static_cast<uint32_t>(L.max_entries);
+    a.max_runs = static_cast<uint32_t>(L.max_runs);
+    a.max_groups = static_cast<uint32_t>(L.max_groups);
+    CUtensorMap map;
+    a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::G::kRows) ? 1 : 0;
     if (d_headflags != nullptr &&
         cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), st) != cudaSuccess)
         return MDX_ERR_CUDA;
     // Look-back words start from zero every call: the workspace's layout moves
     // with n, S and m, so the epoch tag alone cannot tell a status word from
     // another call's data.
-    if (cudaMemsetAsync(a.status, 0, L.max_entries * M * sizeof(uint64_t), st) != cudaSuccess)
+    if (cudaMemsetAsync(a.status, 0, L.max_runs * M * sizeof(uint64_t), st) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    if (cudaMemsetAsync(a.groups_end, 0xff, L.max_groups * sizeof(uint32_t), st) != cudaSuccess)
         return MDX_ERR_CUDA;
     seg_plan_spans<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
     seg_plan_emit<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
-    main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d);
+    main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d, map);
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
 }
 
@@ -362,7 +382,7 @@ template <class V>
 mdx_status dispatch_segm(const void* in, void* out, uint64_t n, mdx_discr dc, const uint64_t* offs,
                          uint64_t S, uint64_t Sb, const int32_t* fl, uint32_t* sz, uint32_t* hf,
                          unsigned char* ws, const SegLayout& L, cudaStream_t st) {
-    if (dc.kind == MDX_DISCR_MASK)
+    if (use_mask(dc))
         return dispatch_segm_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, offs, S, Sb, fl, sz, hf,
                                   ws, L, st);
     return dispatch_segm_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, offs, S, Sb, fl, sz, hf, ws,

@@ -37,6 +37,7 @@
 #include <cuda.h>  // CUtensorMap (type only; maps are encoded by the host)
 
 #include "mdx_device.cuh"
+#include "mdx_tile.cuh"
 
 namespace mdx {
 
@@ -405,79 +406,23 @@ __global__ void __launch_bounds__(THREADS) plain_scatter_kernel(PlainArgs a, D d
     }
 }
 
-// Per-thread class counters in 4-bit lanes: one u32 holds 8 classes, two
-// hold 16.  A lane never reaches 16: with 16 elements per thread only the
-// first 15 are counted in the lanes and the 16th is added when the counts are
-// published.
-template <int M>
-struct NibbleCounts {
-    static_assert(M <= 16, "nibble counters cover at most 16 classes");
-    static constexpr int NW = (M + 7) / 8;
-    uint32_t w[NW];
-    __device__ __forceinline__ void init() {
-#pragma unroll
-        for (int q = 0; q < NW; q++) w[q] = 0;
-    }
-    __device__ __forceinline__ uint32_t get(uint32_t c) const {
-        if constexpr (NW == 1) {
-            return (w[0] >> (c << 2)) & 15u;
-        } else {
-            return (((c < 8u) ? w[0] : w[1]) >> ((c & 7u) << 2)) & 15u;
-        }
-    }
-    __device__ __forceinline__ void inc(uint32_t c) {
-        if constexpr (NW == 1) {
-            w[0] += 1u << (c << 2);
-        } else {
-            const uint32_t one = 1u << ((c & 7u) << 2);
-            if (c < 8u) w[0] += one; else w[1] += one;
-        }
-    }
-};
-
-template <class V>
-__device__ __forceinline__ void unpack16_to(const uint4& r, V* e);
-template <>
-__device__ __forceinline__ void unpack16_to<uint32_t>(const uint4& r, uint32_t* e) {
-    e[0] = r.x; e[1] = r.y; e[2] = r.z; e[3] = r.w;
-}
-template <>
-__device__ __forceinline__ void unpack16_to<uint64_t>(const uint4& r, uint64_t* e) {
-    e[0] = static_cast<uint64_t>(r.x) | (static_cast<uint64_t>(r.y) << 32);
-    e[1] = static_cast<uint64_t>(r.z) | (static_cast<uint64_t>(r.w) << 32);
-}
-
 template <class V, int THREADS, int STAGES, int M>
 struct ScatterTmaSmem {
-    static constexpr int kItems = 64 / static_cast<int>(sizeof(V));  // 64 bytes per thread
-    static constexpr int kTile = THREADS * kItems;
-    static constexpr int kRows = kTile * static_cast<int>(sizeof(V)) / 128;  // 128-byte rows
-    static constexpr uint32_t kAU = 16 / sizeof(V);                 // elements per 16 bytes
-    // every class run gets kAU slots of slack for its 16-byte phase
-    static constexpr int kStageElems = kTile + static_cast<int>(kAU) * M;
+    using G = TileGeom<V, THREADS, M>;
+    static constexpr int kItems = G::kItems;
+    static constexpr int kTile = G::kTile;
+    static constexpr int kRows = G::kRows;
     static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
-    static constexpr size_t kStageBytes = static_cast<size_t>(kStageElems) * sizeof(V);
-    static constexpr size_t kCntBytes = static_cast<size_t>(M) * THREADS * 2;  // u16 counts
     // +1024: the ring is re-aligned to 1024 bytes (128-byte swizzle atoms)
-    static constexpr size_t kBytes = 1024 + kRingBytes + kStageBytes + kCntBytes;
+    static constexpr size_t kBytes = 1024 + kRingBytes + G::kStageBytes + G::kCntBytes;
 };
 
-// Scatter kernel for m <= 16.  Same contract as plain_scatter_kernel; faster
-// per element:
-//  * tiles arrive by tensor TMA (one 2-D box of 128-byte rows per tile) with
-//    the 128-byte swizzle, so the four 16-byte shared loads with which a thread
-//    takes its 64 contiguous bytes are free of bank conflicts;
-//  * a thread ranks its own consecutive elements with 4-bit counters in a
-//    register (local rank = count of its earlier same-class elements); a block
-//    scan over the [class][thread] count matrix in shared memory then gives
-//    every thread its exclusive class prefix (stable: thread order = input
-//    order), with the tile's class-run start folded in;
-//  * every class run is placed in the stage at the same 16-byte phase as its
-//    destination, so its aligned interior leaves by one bulk store
-//    (cp.async.bulk shared->global) and only the < 16-byte head and tail of a
-//    run are written by threads.  The stage is rewritten only after the bulk
-//    stores of the previous tile have read it (they have the whole next pass 1
-//    and row scan to do so).
+// Scatter kernel for m <= 16.  Same contract as plain_scatter_kernel; tiles
+// arrive by tensor TMA (one 2-D box of 128-byte rows per tile, 128-byte
+// swizzle, STAGES-deep mbarrier ring) and go through tile_scatter
+// (mdx_tile.cuh): thread-local nibble ranks, a block scan over the
+// [class][thread] count matrix, a shared-memory stage at the destination's
+// 16-byte phase and bulk stores of every class run.
 template <class V, class D, int M, int THREADS, int STAGES>
 __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 64 registers
     plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
@@ -485,29 +430,20 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     constexpr int ITEMS = L::kItems;
     constexpr int TILE = L::kTile;
     constexpr int ROWS = L::kRows;
-    constexpr uint32_t AU = L::kAU;
-    constexpr int W = THREADS / 32;
-    constexpr int PER = THREADS / 32;  // count-matrix entries per lane in a row scan
-    constexpr int LR = (ITEMS + 7) / 8;
-    static_assert(M <= 16 && M >= 2, "class bound");
-    static_assert(M <= W * 2, "each warp scans at most two rows");
-    static_assert(ITEMS == 16 || ITEMS == 8, "64 bytes of 4- or 8-byte elements");
-    static_assert(PER == 8, "row scan loads 8 entries per lane");
+    constexpr uint32_t AU = L::G::kAU;
     static_assert(ROWS <= 256, "TMA box height");
-    static_assert(L::kStageElems < 65536, "stage slots are kept in 16 bits");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
     unsigned char* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
     V* ring = reinterpret_cast<V*>(base);
     V* stage = reinterpret_cast<V*>(base + L::kRingBytes);
-    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(base + L::kRingBytes + L::kStageBytes);
+    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(base + L::kRingBytes + L::G::kStageBytes);
 
     __shared__ __align__(8) uint64_t bars[STAGES];
-    __shared__ uint32_t cursor[2][M];  // ping-pong by tile parity
-    __shared__ uint32_t run_start[M], run_cnt[M], run_dst[M], rowtot[M];
+    __shared__ TileShared<M> sh;
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const uint32_t G = a.num_chunks, k = blockIdx.x;
     uint32_t t0, t1;
     chunk_tiles(k, a.num_tiles, G, t0, t1);
@@ -520,7 +456,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     const bool tma_ok = a.use_tma != 0;
 
     if (tid < M)
-        cursor[0][tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
+        sh.cursor[0][tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
     if (tid == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
@@ -528,7 +464,8 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     }
     __syncthreads();
 
-    // i-th tile in processing order is tile t1-1-i (the chunk is walked backwards).
+    // i-th tile in processing order is tile t1-1-i (the chunk is walked
+    // backwards, so the tiles the counting kernel read last are still in L2).
     auto issue = [&](uint32_t i) {
         const uint32_t tile = t1 - 1u - i;
         uint64_t* bar = &bars[i % STAGES];
@@ -542,27 +479,16 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     if (tid == 0)
         for (uint32_t i = 0; i < STAGES && i < cnt; i++) issue(i);
 
-    const uint32_t e0 = tid * ITEMS;  // this thread's first tile-local element
-    uint16_t* my_cnt = cnt_sm + tid;  // column of this thread: my_cnt[c * THREADS]
+    const uint32_t e0 = tid * ITEMS;
     for (uint32_t i = 0; i < cnt; i++) {
         const uint32_t tile = t1 - 1u - i;
         const uint64_t ts = static_cast<uint64_t>(tile) * TILE;
         const uint32_t valid = static_cast<uint32_t>(min(static_cast<uint64_t>(TILE), a.n - ts));
         const bool full = valid == TILE;
         const bool ok = mbar_wait_bounded(&bars[i % STAGES], (i / STAGES) & 1u);
-
-        // ---- pass 1: take 64 contiguous bytes, classify, local ranks
         V v[ITEMS];
         if (tma_ok && full) {
-            const unsigned char* tb =
-                reinterpret_cast<const unsigned char*>(ring + (i % STAGES) * TILE);
-            const uint32_t row = static_cast<uint32_t>(tid) >> 1;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const uint32_t chunk = ((static_cast<uint32_t>(tid) & 1u) * 4u + q) ^ (row & 7u);
-                const uint4 r = *reinterpret_cast<const uint4*>(tb + row * 128u + chunk * 16u);
-                unpack16_to<V>(r, &v[q * AU]);
-            }
+            take_swizzled<V, ITEMS>(ring + (i % STAGES) * TILE, v);
         } else if (full) {
 #pragma unroll
             for (int j = 0; j < ITEMS; j++) v[j] = in[ts + e0 + j];
@@ -570,156 +496,18 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
 #pragma unroll
             for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
         }
-        NibbleCounts<M> nc;
-        nc.init();
-        uint32_t lr[LR];
-#pragma unroll
-        for (int q = 0; q < LR; q++) lr[q] = 0;
-        uint32_t last_c = M;  // class of element 15 (not in the nibbles)
-        if (full) {
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++) {
-                const uint32_t c = d(v[j]);
-                lr[j >> 3] += nc.get(c) << (4 * (j & 7));
-                if (j < 15) nc.inc(c); else last_c = c;
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++) {
-                if (e0 + j < valid) {
-                    const uint32_t c = d(v[j]);
-                    lr[j >> 3] += nc.get(c) << (4 * (j & 7));
-                    if (j < 15) nc.inc(c); else last_c = c;
-                }
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < M; c++) my_cnt[c * THREADS] = static_cast<uint16_t>(nc.get(c));
-        if (last_c < static_cast<uint32_t>(M)) my_cnt[last_c * THREADS] += 1;
-        if (__syncthreads_or(!ok)) {  // (A)
+        const bool done = tile_scatter<V, D, M, THREADS, false>(
+            d, v, 0u, valid, full, stage, cnt_sm, sh, i & 1u, out, out_phase, ok, [&] {
+                // the ring slot is consumed (values are in registers): refill it
+                if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
+            });
+        if (!done) {
             if (tid == 0) {
                 atomicOr(a.error, kErrTimeout);
                 for (uint32_t q = i; q < cnt && q < i + STAGES; q++)
                     (void)mbar_wait_bounded(&bars[q % STAGES], (q / STAGES) & 1u);
             }
-            if (tid < M) bulk_wait_all();
-            return;
-        }
-        // The ring slot is consumed (values are in registers): refill it now.
-        if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
-
-        // ---- row scans of the [class][thread] count matrix: warp w owns
-        // rows w and w + W; the prefixes stay in registers until the class
-        // runs are known
-        uint32_t pre[2][PER];
-        uint32_t rtot[2] = {0u, 0u};
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int c = warp + h * W;
-            if (c < M) {
-                const uint4 xw = *reinterpret_cast<const uint4*>(cnt_sm + c * THREADS + lane * PER);
-                const uint32_t x[8] = {xw.x & 0xffffu, xw.x >> 16, xw.y & 0xffffu, xw.y >> 16,
-                                       xw.z & 0xffffu, xw.z >> 16, xw.w & 0xffffu, xw.w >> 16};
-                uint32_t tot = 0;
-#pragma unroll
-                for (int q = 0; q < 8; q++) tot += x[q];
-                const uint32_t incl = warp_incl_scan(tot);
-                uint32_t run = incl - tot;
-#pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    pre[h][q] = run;
-                    run += x[q];
-                }
-                rtot[h] = __shfl_sync(0xffffffffu, incl, 31);
-                if (lane == 31) rowtot[c] = incl;
-            }
-        }
-        __syncthreads();  // (B)
-
-        // ---- class runs (every warp, lanes = classes): destination of run c
-        // (chunk walked backwards) and its stage slot, at the destination's
-        // 16-byte phase within kAU slots of slack per run
-        {
-            const uint32_t par = i & 1u;
-            const uint32_t c = static_cast<uint32_t>(lane);
-            const uint32_t cc = c < static_cast<uint32_t>(M) ? rowtot[c] : 0u;
-            const uint32_t dst = c < static_cast<uint32_t>(M) ? cursor[par][c] - cc : 0u;
-            const uint32_t room = cc + (c < static_cast<uint32_t>(M) ? AU : 0u);
-            const uint32_t q0 = warp_incl_scan(room) - room;
-            const uint32_t st = q0 + (((out_phase + dst) - q0) & (AU - 1u));
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int row = warp + h * W;
-                if (row < M) {
-                    // slots < kStageElems < 2^16: pairs of u16 prefixes per word
-                    const uint32_t add = __shfl_sync(0xffffffffu, st, row);
-                    const uint32_t add2 = add | (add << 16);
-                    *reinterpret_cast<uint4*>(cnt_sm + row * THREADS + lane * PER) =
-                        make_uint4((pre[h][0] | (pre[h][1] << 16)) + add2,
-                                   (pre[h][2] | (pre[h][3] << 16)) + add2,
-                                   (pre[h][4] | (pre[h][5] << 16)) + add2,
-                                   (pre[h][6] | (pre[h][7] << 16)) + add2);
-                }
-            }
-            if (warp == 0 && c < static_cast<uint32_t>(M)) {
-                cursor[par ^ 1u][c] = dst;
-                run_start[c] = st;
-                run_cnt[c] = cc;
-                run_dst[c] = dst;
-            }
-            (void)rtot;
-        }
-        // the stage is about to be rewritten: the bulk stores of the previous
-        // tile must have finished reading it
-        if (tid < M) bulk_wait_read<0>();
-        __syncthreads();  // (C)
-
-        // ---- pass 2: scatter into the class-sorted stage
-        V* stg = stage;
-        if (full) {
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++) {
-                const uint32_t c = d(v[j]);
-                const uint32_t slot = my_cnt[c * THREADS] + ((lr[j >> 3] >> (4 * (j & 7))) & 15u);
-                stg[slot] = v[j];
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < ITEMS; j++) {
-                if (e0 + j < valid) {
-                    const uint32_t c = d(v[j]);
-                    const uint32_t slot =
-                        my_cnt[c * THREADS] + ((lr[j >> 3] >> (4 * (j & 7))) & 15u);
-                    stg[slot] = v[j];
-                }
-            }
-        }
-        fence_proxy_async_smem();
-        __syncthreads();  // (D)
-
-        // ---- write-out: bulk store of each run's aligned interior, threads
-        // store the unaligned head and tail elements
-        if (tid < M) {
-            const uint32_t s = run_start[tid], cc = run_cnt[tid];
-            uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
-            if (head > cc) head = cc;
-            const uint32_t body = ((cc - head) / AU) * AU;
-            if (body > 0)
-                bulk_store_s2g(out + run_dst[tid] + head, stg + s + head, body * sizeof(V));
-            bulk_commit();
-        } else if (tid >= 32 && tid < 32 + M * 2 * static_cast<int>(AU)) {
-            const uint32_t c = (tid - 32) / (2 * AU), q = (tid - 32) % (2 * AU);
-            const uint32_t s = run_start[c], cc = run_cnt[c];
-            uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
-            if (head > cc) head = cc;
-            const uint32_t body = ((cc - head) / AU) * AU;
-            uint32_t off = 0xffffffffu;
-            if (q < AU) {
-                if (q < head) off = q;
-            } else if (head + body + (q - AU) < cc) {
-                off = head + body + (q - AU);
-            }
-            if (off != 0xffffffffu) out[run_dst[c] + off] = stg[s + off];
+            break;
         }
     }
     if (tid < M) bulk_wait_all();

@@ -5,33 +5,39 @@
 // per-element reductions, class offsets, indices, permute, sizes -- with nine
 // N-sized temporaries, four of them N*m tuples) by three launches:
 //
-//   seg_plan_spans  per segment: its length; segments longer than one window
-//                   (P elements) are "large" and get one work entry per
-//                   window they touch.  Block-local scan of the entry counts;
-//                   the last CTA scans the block totals and records the
-//                   number of entries, the largest span (the lag below), a new
-//                   epoch for the look-back words, and resets the ticket.
-//   seg_plan_emit   writes the work entries {segment, piece [p0, p1), last
-//                   entry of the segment} in element order.
-//   seg_main        one persistent launch.  CTAs take tickets in order:
-//                     * small-segment groups first: each segment of length
-//                       <= P is partitioned on its own by one warp (count
-//                       pass, then rank pass with __match_any_sync + __popc
-//                       ranks and running class counts), single HBM read;
-//                     * then, for every large-segment window entry j, a
-//                       count item C(j) (class counts of the piece, published
+//   seg_plan_spans  per segment: its length.  Segments longer than one tile
+//                   (P elements) are "large" and are cut into runs of up to
+//                   RUN_TILES tiles; the other ("small") segments are grouped
+//                   by the tile their first element falls in (a group spans
+//                   at most 2P elements).  Block-local scans of the run and
+//                   group counts; the last CTA scans the block totals and
+//                   records the counts, the largest number of runs of one
+//                   segment (the lag below) and a new look-back epoch, and
+//                   resets the persistent kernel's ticket.
+//   seg_plan_emit   writes the run entries {segment, [p0, p1), last run of
+//                   the segment} and the group heads, in element order.
+//   seg_main        one persistent launch.  CTAs take tickets in order (each
+//                   CTA fetches its next ticket while it works on the current
+//                   one):
+//                     * small-segment groups: the group's range is read into
+//                       shared memory once, warps partition one segment each
+//                       (count pass, then __match_any_sync + __popc ranks with
+//                       running class counts) into a shared output image, and
+//                       the CTA writes the range back with 16-byte stores --
+//                       one HBM read and one write per element;
+//                     * then, per run j of a large segment, a count item C(j)
+//                       (class counts of the run with 16-byte loads, published
 //                       to epoch-tagged per-class status words; decoupled
-//                       look-back over the segment's earlier entries gives the
-//                       piece's exclusive prefix, the segment's last entry
-//                       gives its class totals) and a scatter item S(j)
-//                       (re-reads the piece, ranks it CTA-wide, writes it
-//                       through a shared-memory stage).  S(j) is issued D
-//                       tickets after C(j), D = the longest span, so S(j)
-//                       only waits on earlier tickets (no deadlock) and finds
-//                       its piece still in L2 (D * P elements of lag).
+//                       look-back over the segment's earlier runs gives the
+//                       run's exclusive prefix, the last run gives the
+//                       segment's class totals) and a scatter item S(j) (the
+//                       run's tiles through a TMA ring and tile_scatter).
+//                       S(j) is issued D tickets after C(j), D = the most runs
+//                       of one segment, so it waits only on earlier tickets (no
+//                       deadlock) and re-reads its run from L2.
 //
 // Every wait is bounded (kWaitLimitNs); a wait that runs out latches
-// kErrTimeout and publishes what it has so that no other CTA waits forever.
+// kErrTimeout and publishes what it has so no other CTA waits forever.
 //
 // Output per segment equals seqMdiscr (SeqMdiscr.h:10-57) applied to the
 // segment, which is exactly what MdiscrSegmTest.cu:8-41 validates; sizes are
@@ -39,10 +45,16 @@
 // (MdiscrSegmKernels.cu.h:89-114 writes the latter into new_sizes).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include "mdx_device.cuh"
-#include "mdx_plain.cuh"  // NibbleCounts, unpack16_to
+#include "mdx_plain.cuh"  // PackedCounts
+#include "mdx_tile.cuh"
 
 namespace mdx {
+
+constexpr int kRunTiles = 8;     // tiles per run of a large segment
+constexpr int kGroupBatch = 8;   // small-segment groups per work item (pipelined)
 
 // status word: [63:34] epoch (30 bits), [33:32] state, [31:0] count
 constexpr uint64_t kStAgg = 1ull;
@@ -58,21 +70,22 @@ struct SegHeader {      // lives at the start of the segmented workspace
     uint32_t ticket;    // persistent-kernel ticket counter (reset by the planner)
     uint32_t error;     // latched error bits
     uint32_t epoch;     // look-back epoch of the current call (1 .. 2^30-1)
-    uint32_t num_lw;    // large-window entries this call
-    uint32_t lag;       // longest span of a large segment, in windows
+    uint32_t num_runs;  // large-segment runs this call
+    uint32_t lag;       // most runs of one segment (max over the planner's blocks)
     uint32_t plan_done; // planner CTA ticket
     uint64_t num_segs;  // S (written by the flags converter for the head-flag form)
     uint32_t lag_cur;   // lag of the current call (snapshot taken by the planner)
     uint32_t flags_ticket;  // tile ticket of the flags converter
     uint32_t flags_done;    // finished tiles of the flags converter
     uint32_t flags_epoch;   // look-back epoch of the flags converter
-    uint32_t pad[4];
+    uint32_t num_groups;    // small-segment groups this call
+    uint32_t pad[3];
 };
 
-struct LwEntry {        // one window piece of a large segment
+struct RunEntry {       // a run of up to kRunTiles tiles of one large segment
     uint32_t seg;       // segment index
-    uint32_t p0, p1;    // element range of the piece
-    uint32_t jlast;     // entry index of the segment's last piece
+    uint32_t p0, p1;    // element range of the run
+    uint32_t jlast;     // entry index of the segment's last run
 };
 
 struct SegArgs {
@@ -86,14 +99,20 @@ struct SegArgs {
     const int32_t* in_flags;   // head-flag input (validated by the planner) or null
     uint32_t m;
     SegHeader* hdr;
-    uint32_t* span_loc;        // [S] block-local exclusive entry offsets
-    uint32_t* blk_tot;         // [plan blocks] entry totals, then offsets
-    LwEntry* lw;               // [max entries]
-    uint64_t* status;          // [max entries][M]
-    uint32_t* excl;            // [max entries][M] exclusive prefix of each piece
+    uint32_t* run_loc;         // [S] block-local exclusive run offsets
+    uint32_t* grp_loc;         // [S] block-local exclusive group-head offsets
+    uint32_t* blk_runs;        // [plan blocks] run totals, then offsets
+    uint32_t* blk_grps;        // [plan blocks] group totals, then offsets
+    RunEntry* runs;            // [max_runs]
+    uint32_t* groups;          // [max_groups] first segment of each group
+    uint32_t* groups_end;      // [max_groups] one past its last segment (0xffffffff: none
+                               // marked, the group runs to S; reset every call)
+    uint64_t* status;          // [max_runs][M]
+    uint32_t* excl;            // [max_runs][M] exclusive prefix of each run
     uint32_t plan_blocks;
-    uint32_t max_entries;      // capacity of lw / status / excl (2 per window: enough
-                               // for segments that tile [0, n); malformed ones are cut)
+    uint32_t max_runs;         // capacity (enough for segments that tile [0, n))
+    uint32_t max_groups;
+    int use_tma;               // the tensor map passed to seg_main is valid
 };
 
 constexpr uint64_t kSegsOnDevice = ~0ull;
@@ -106,123 +125,174 @@ __device__ __forceinline__ uint64_t seg_count(const SegArgs& a) {
 // Block b of the planner owns segments [b*R, min((b+1)*R, S)), R = ceil(S/G).
 template <int P, int THREADS>
 __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
-    __shared__ uint32_t warp_tot[THREADS / 32];
-    __shared__ uint32_t carry_sh;
+    constexpr int W = THREADS / 32;
+    __shared__ uint32_t warp_runs[W], warp_grps[W];
     __shared__ int am_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t S = seg_count(a);
     const uint64_t G = gridDim.x;
     const uint64_t R = (S + G - 1) / G;
     const uint64_t s0 = blockIdx.x * R, s1 = min(s0 + R, S);
-    uint32_t carry = 0, maxspan = 0;
+    uint32_t carry_r = 0, carry_g = 0, maxruns = 0;
     for (uint64_t base = s0; base < s1; base += THREADS) {
         const uint64_t s = base + tid;
-        uint32_t span = 0;
+        uint32_t runs = 0, head = 0;
         if (s < s1) {
             const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
             if (a1 < a0 || a1 > a.n || (s == 0 && a0 != 0) || (s + 1 == S && a1 != a.n)) {
                 atomicOr(&a.hdr->error, kErrSegments);
             } else if (a1 - a0 > static_cast<uint64_t>(P)) {
-                span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
+                const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
+                runs = (span + kRunTiles - 1) / kRunTiles;
+            } else {
+                head = (s == 0 || a.offsets[s - 1] / (P / 2) != a0 / (P / 2)) ? 1u : 0u;
             }
-            if (a.in_flags != nullptr && a1 > a0 &&
+            if (a.in_flags != nullptr && a1 > a0 && a1 <= a.n &&
                 static_cast<uint64_t>(a.in_flags[a0]) != a1 - a0)
                 atomicOr(&a.hdr->error, kErrSegments);
         }
-        maxspan = max(maxspan, span);
-        const uint32_t incl = warp_incl_scan(span);
-        if (lane == 31) warp_tot[warp] = incl;
-        __syncthreads();
-        uint32_t wpre = 0, btot = 0;
-        for (int w = 0; w < THREADS / 32; w++) {
-            const uint32_t x = warp_tot[w];
-            wpre += (w < warp) ? x : 0u;
-            btot += x;
+        maxruns = max(maxruns, runs);
+        const uint32_t ir = warp_incl_scan(runs);
+        const uint32_t ig = warp_incl_scan(head);
+        if (lane == 31) {
+            warp_runs[warp] = ir;
+            warp_grps[warp] = ig;
         }
-        if (s < s1) a.span_loc[s] = carry + wpre + incl - span;
-        carry += btot;
+        __syncthreads();
+        uint32_t pr = 0, pg = 0, tr = 0, tg = 0;
+        for (int w = 0; w < W; w++) {
+            const uint32_t xr = warp_runs[w], xg = warp_grps[w];
+            pr += (w < warp) ? xr : 0u;
+            pg += (w < warp) ? xg : 0u;
+            tr += xr;
+            tg += xg;
+        }
+        if (s < s1) {
+            a.run_loc[s] = carry_r + pr + ir - runs;
+            a.grp_loc[s] = carry_g + pg + ig - head;
+        }
+        carry_r += tr;
+        carry_g += tg;
         __syncthreads();
     }
-    for (int d = 16; d > 0; d >>= 1) maxspan = max(maxspan, __shfl_xor_sync(0xffffffffu, maxspan, d));
-    if (lane == 0 && maxspan > 0) atomicMax(&a.hdr->lag, maxspan);
-    if (tid == 0) a.blk_tot[blockIdx.x] = carry;
+    for (int d = 16; d > 0; d >>= 1) maxruns = max(maxruns, __shfl_xor_sync(0xffffffffu, maxruns, d));
+    if (lane == 0 && maxruns > 0) atomicMax(&a.hdr->lag, maxruns);
+    if (tid == 0) {
+        a.blk_runs[blockIdx.x] = carry_r;
+        a.blk_grps[blockIdx.x] = carry_g;
+    }
     __threadfence();
     __syncthreads();
     if (tid == 0) am_last = (atomicAdd(&a.hdr->plan_done, 1u) == gridDim.x - 1);
     __syncthreads();
     if (!am_last) return;
     __threadfence();
-    // last CTA: exclusive scan of the block totals (in place)
-    if (warp == 0) {
+    // last CTA: exclusive scans of the block totals (in place)
+    if (warp < 2) {
+        uint32_t* arr = warp == 0 ? a.blk_runs : a.blk_grps;
         uint32_t run = 0;
         for (uint32_t b0 = 0; b0 < gridDim.x; b0 += 32) {
             const uint32_t b = b0 + lane;
-            const uint32_t x = b < gridDim.x ? __ldcg(&a.blk_tot[b]) : 0u;
+            const uint32_t x = b < gridDim.x ? __ldcg(&arr[b]) : 0u;
             const uint32_t incl = warp_incl_scan(x);
-            if (b < gridDim.x) a.blk_tot[b] = run + incl - x;
+            if (b < gridDim.x) arr[b] = run + incl - x;
             run += __shfl_sync(0xffffffffu, incl, 31);
         }
         if (lane == 0) {
-            carry_sh = run;
-            a.hdr->num_lw = run <= a.max_entries ? run : 0u;  // over capacity: malformed
-            a.hdr->lag_cur = a.hdr->lag;  // every block's atomicMax happened before its ticket
-            a.hdr->lag = 0u;
-            uint32_t e = a.hdr->epoch + 1u;
-            if (e >= (1u << 30) || e == 0u) e = 1u;
-            a.hdr->epoch = e;
-            a.hdr->ticket = 0u;
-            a.hdr->plan_done = 0u;
-            // head-flag converter state for its next call
-            a.hdr->flags_ticket = 0u;
-            a.hdr->flags_done = 0u;
-            uint32_t fe = a.hdr->flags_epoch + 1u;
-            if (fe >= (1u << 30)) fe = 1u;
-            a.hdr->flags_epoch = fe;
+            if (warp == 0) {
+                a.hdr->num_runs = run <= a.max_runs ? run : 0u;  // over capacity: malformed
+                a.hdr->lag_cur = a.hdr->lag;  // every block's atomicMax preceded its ticket
+                a.hdr->lag = 0u;
+            } else {
+                a.hdr->num_groups = run <= a.max_groups ? run : 0u;
+            }
         }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t e = a.hdr->epoch + 1u;
+        if (e >= (1u << 30) || e == 0u) e = 1u;
+        a.hdr->epoch = e;
+        a.hdr->ticket = 0u;
+        a.hdr->plan_done = 0u;
+        // head-flag converter state for its next call
+        a.hdr->flags_ticket = 0u;
+        a.hdr->flags_done = 0u;
+        uint32_t fe = a.hdr->flags_epoch + 1u;
+        if (fe >= (1u << 30)) fe = 1u;
+        a.hdr->flags_epoch = fe;
     }
 }
 
 template <int P, int THREADS>
 __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
-    __shared__ uint32_t list_seg[THREADS], list_pos[THREADS], list_span[THREADS];
+    __shared__ uint32_t list_seg[THREADS], list_pos[THREADS], list_runs[THREADS];
     __shared__ uint32_t list_n;
     const int tid = threadIdx.x;
     const uint64_t S = seg_count(a);
     const uint64_t G = gridDim.x;
     const uint64_t R = (S + G - 1) / G;
     const uint64_t s0 = blockIdx.x * R, s1 = min(s0 + R, S);
-    const uint32_t boff = a.blk_tot[blockIdx.x];
+    const uint32_t roff = a.blk_runs[blockIdx.x], goff = a.blk_grps[blockIdx.x];
+    const uint32_t num_runs = a.hdr->num_runs, num_groups = a.hdr->num_groups;
     for (uint64_t base = s0; base < s1; base += THREADS) {
         if (tid == 0) list_n = 0;
         __syncthreads();
         const uint64_t s = base + tid;
         if (s < s1) {
             const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
-            if (a1 >= a0 && a1 <= a.n && a1 - a0 > static_cast<uint64_t>(P)) {
-                const uint32_t q = atomicAdd(&list_n, 1u);
-                list_seg[q] = static_cast<uint32_t>(s);
-                list_pos[q] = boff + a.span_loc[s];
-                list_span[q] = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
+            if (a1 >= a0 && a1 <= a.n) {
+                if (a1 - a0 > static_cast<uint64_t>(P)) {
+                    const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
+                    const uint32_t nr = (span + kRunTiles - 1) / kRunTiles;
+                    const uint32_t pos = roff + a.run_loc[s];
+                    if (nr <= 16) {  // this thread emits the runs itself
+                        if (static_cast<uint64_t>(pos) + nr <= num_runs) {
+                            const uint64_t w0 = a0 / P;
+                            for (uint32_t r = 0; r < nr; r++) {
+                                const uint64_t wa = w0 + static_cast<uint64_t>(r) * kRunTiles;
+                                RunEntry e;
+                                e.seg = static_cast<uint32_t>(s);
+                                e.p0 = static_cast<uint32_t>(max(a0, wa * P));
+                                e.p1 = static_cast<uint32_t>(min(a1, (wa + kRunTiles) * P));
+                                e.jlast = pos + nr - 1u;
+                                a.runs[pos + r] = e;
+                            }
+                        }
+                    } else {  // long segments: the whole block emits them below
+                        const uint32_t q = atomicAdd(&list_n, 1u);
+                        list_seg[q] = static_cast<uint32_t>(s);
+                        list_pos[q] = pos;
+                        list_runs[q] = nr;
+                    }
+                } else if (s == 0 || a.offsets[s - 1] / (P / 2) != a0 / (P / 2)) {
+                    const uint32_t g = goff + a.grp_loc[s];
+                    if (g < num_groups) a.groups[g] = static_cast<uint32_t>(s);
+                }
             }
+            // the group before segment s ends at s at the latest when s starts
+            // a group, is large or is malformed
+            const bool small_ok = (a1 >= a0 && a1 <= a.n && a1 - a0 <= static_cast<uint64_t>(P));
+            const bool is_head = small_ok && (s == 0 || a.offsets[s - 1] / (P / 2) != a0 / (P / 2));
+            const uint32_t before = goff + a.grp_loc[s];  // groups starting before s
+            if ((is_head || !small_ok) && before >= 1u && before - 1u < num_groups)
+                atomicMin(&a.groups_end[before - 1u], static_cast<uint32_t>(s));
         }
         __syncthreads();
         const uint32_t cnt = list_n;
-        for (uint32_t q = 0; q < cnt; q++) {  // the block emits each large segment's entries
-            const uint32_t seg = list_seg[q], pos = list_pos[q], span = list_span[q];
+        for (uint32_t q = 0; q < cnt; q++) {  // the block emits each large segment's runs
+            const uint32_t seg = list_seg[q], pos = list_pos[q], nr = list_runs[q];
+            if (static_cast<uint64_t>(pos) + nr > num_runs) continue;  // malformed offsets
             const uint64_t a0 = a.offsets[seg], a1 = a.offsets[seg + 1];
             const uint64_t w0 = a0 / P;
-            if (static_cast<uint64_t>(pos) + span > a.max_entries) {  // malformed offsets
-                if (tid == 0) atomicOr(&a.hdr->error, kErrSegments);
-                continue;
-            }
-            for (uint32_t k = tid; k < span; k += THREADS) {
-                const uint64_t w = w0 + k;
-                LwEntry e;
+            for (uint32_t r = tid; r < nr; r += THREADS) {
+                const uint64_t wa = w0 + static_cast<uint64_t>(r) * kRunTiles;
+                RunEntry e;
                 e.seg = seg;
-                e.p0 = static_cast<uint32_t>(max(a0, w * P));
-                e.p1 = static_cast<uint32_t>(min(a1, (w + 1) * P));
-                e.jlast = pos + span - 1u;
-                a.lw[pos + k] = e;
+                e.p0 = static_cast<uint32_t>(max(a0, wa * P));
+                e.p1 = static_cast<uint32_t>(min(a1, (wa + kRunTiles) * P));
+                e.jlast = pos + nr - 1u;
+                a.runs[pos + r] = e;
             }
         }
         __syncthreads();
@@ -230,15 +300,20 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
 }
 
 // --------------------------------------------------------------- main kernel --
-template <class V, int M, int THREADS>
+template <class V, int M, int THREADS, int STAGES>
 struct SegSmem {
-    static constexpr int kItems = 64 / static_cast<int>(sizeof(V));
-    static constexpr int kTile = THREADS * kItems;  // == P
-    static constexpr uint32_t kAU = 16 / sizeof(V);
-    static constexpr int kStageElems = kTile + static_cast<int>(kAU) * M;
-    static constexpr size_t kStageBytes = static_cast<size_t>(kStageElems) * sizeof(V);
-    static constexpr size_t kCntBytes = static_cast<size_t>(M) * THREADS * 2;
-    static constexpr size_t kBytes = kStageBytes + kCntBytes + 64;
+    using G = TileGeom<V, THREADS, M>;
+    static constexpr int kTile = G::kTile;  // == P
+    static constexpr uint32_t kAU = G::kAU;
+    // small groups (segments starting in one half-tile window, each <= P):
+    // two input buffers (one being filled by TMA) and an output image, each
+    // for a range of <= P/2 + P elements plus 16-byte alignment slack
+    static constexpr int kGroupElems = kTile / 2 + kTile + 2 * static_cast<int>(kAU);
+    static constexpr size_t kGroupBytes = 3ull * kGroupElems * sizeof(V);
+    // runs: TMA ring + tile stage + count matrix
+    static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
+    static constexpr size_t kRunBytes = kRingBytes + G::kStageBytes + G::kCntBytes;
+    static constexpr size_t kBytes = 1024 + (kGroupBytes > kRunBytes ? kGroupBytes : kRunBytes);
 };
 
 // Bounded spin on a status word until it carries this epoch with state >=
@@ -255,90 +330,113 @@ __device__ __forceinline__ bool wait_status(const uint64_t* p, uint32_t epoch, u
     }
 }
 
-// One warp partitions one segment of length L <= P (two passes over it: the
-// second finds it in L1/L2).  Lanes 0..M-1 also write the segment's sizes.
+// Per-lane class counters in 16-bit fields (M <= 16: (M+1)/2 words), wide
+// enough for a whole segment's totals after a warp scan (<= 2P < 2^16).
+template <int M>
+struct HalfCounts {
+    static constexpr int NW = (M + 1) / 2;
+    uint32_t w[NW];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int q = 0; q < NW; q++) w[q] = 0;
+    }
+    __device__ __forceinline__ uint32_t get(uint32_t c) const {
+        uint32_t x = w[0];
+#pragma unroll
+        for (int q = 1; q < NW; q++) x = (c >> 1) == static_cast<uint32_t>(q) ? w[q] : x;
+        return (x >> ((c & 1u) << 4)) & 0xffffu;
+    }
+    __device__ __forceinline__ void inc(uint32_t c) {
+        const uint32_t one = 1u << ((c & 1u) << 4);
+#pragma unroll
+        for (int q = 0; q < NW; q++) w[q] += (c >> 1) == static_cast<uint32_t>(q) ? one : 0u;
+    }
+};
+
+// One warp partitions one segment held in shared memory (element e at
+// src[e], 0 <= e < L <= 2P) into the shared output image dst[0 .. L) and
+// writes the segment's sizes.  Lane l owns the contiguous elements
+// [l*k, (l+1)*k) with k odd (so the 32 lanes read 32 different banks):
+// pass 1 counts them, a warp scan of the counters gives every lane its
+// per-class prefix (stable: lane order = input order) and the segment's
+// class offsets, pass 2 places them.
 template <class V, class D, int M>
-__device__ void seg_small_warp(const SegArgs& a, const D& d, uint64_t s, uint64_t a0, uint64_t L,
-                               uint32_t* hist /* per-warp [M] */) {
-    const int lane = threadIdx.x & 31;
-    const V* in = static_cast<const V*>(a.in) + a0;
-    V* out = static_cast<V*>(a.out) + a0;
-    const uint32_t lt = lanemask_lt();
-    for (int c = lane; c < M; c += 32) hist[c] = 0;
-    __syncwarp();
-    // pass 1: class counts
-    for (uint64_t e0 = 0; e0 < L; e0 += 32) {
-        const uint64_t e = e0 + lane;
-        const bool live = e < L;
-        const uint32_t c = live ? d(in[e]) : static_cast<uint32_t>(M);
-        const uint32_t peers = __match_any_sync(0xffffffffu, c);
-        if (live && (peers >> lane) == 1u) hist[c] += __popc(peers);
-        __syncwarp();
+__device__ void seg_small_warp(const SegArgs& a, const D& d, uint64_t s, uint64_t a0, uint32_t L,
+                               const V* src, V* dst) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t k = (L + 31u) >> 5;
+    k |= 1u;  // odd stride
+    const uint32_t b = min(lane * k, L), e1 = min(b + k, L);
+    HalfCounts<M> cnt;
+    cnt.zero();
+    for (uint32_t e = b; e < e1; e++) cnt.inc(d(src[e]));
+    // warp inclusive scan of the packed counters
+    HalfCounts<M> incl = cnt;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+#pragma unroll
+        for (int q = 0; q < HalfCounts<M>::NW; q++) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl.w[q], dd);
+            if (lane >= static_cast<uint32_t>(dd)) incl.w[q] += y;
+        }
     }
-    // class offsets (exclusive scan over classes); lanes own classes lane, lane+32
-    uint32_t off0 = 0, off1 = 0, tot0 = 0, tot1 = 0;
-    {
-        tot0 = lane < M ? hist[lane] : 0u;
-        tot1 = lane + 32 < M ? hist[lane + 32] : 0u;
-        const uint32_t i0 = warp_incl_scan(tot0);
-        const uint32_t all0 = __shfl_sync(0xffffffffu, i0, 31);
-        const uint32_t i1 = warp_incl_scan(tot1);
-        off0 = i0 - tot0;
-        off1 = all0 + i1 - tot1;
+    // segment totals (lane 31's inclusive) -> class offsets
+    HalfCounts<M> tot;
+#pragma unroll
+    for (int q = 0; q < HalfCounts<M>::NW; q++) tot.w[q] = __shfl_sync(0xffffffffu, incl.w[q], 31);
+    HalfCounts<M> base;  // class offset + this lane's exclusive prefix, per class
+    base.zero();
+    uint32_t off = 0;
+#pragma unroll
+    for (int c = 0; c < M; c++) {
+        const uint32_t t = tot.get(c);
+        const uint32_t mine = incl.get(c) - cnt.get(c) + off;
+        base.w[c >> 1] |= mine << ((c & 1) << 4);
+        if (static_cast<uint32_t>(c) == lane) {
+            if (a.seg_sizes != nullptr && static_cast<uint32_t>(c) < a.m) a.seg_sizes[s * a.m + c] = t;
+            if (a.headflags != nullptr && t > 0) a.headflags[a0 + off] = t;
+        }
+        off += t;
     }
-    __syncwarp();
-    if (lane < M) hist[lane] = off0;            // running destination per class
-    if (lane + 32 < M) hist[lane + 32] = off1;
-    if (a.seg_sizes != nullptr) {
-        if (lane < M && static_cast<uint32_t>(lane) < a.m) a.seg_sizes[s * a.m + lane] = tot0;
-        if (lane + 32 < M && static_cast<uint32_t>(lane + 32) < a.m)
-            a.seg_sizes[s * a.m + lane + 32] = tot1;
-    }
-    if (a.headflags != nullptr) {
-        if (lane < M && tot0 > 0) a.headflags[a0 + off0] = tot0;
-        if (lane + 32 < M && tot1 > 0) a.headflags[a0 + off1] = tot1;
-    }
-    __syncwarp();
-    // pass 2: ranks in input order, scatter into the segment's output
-    for (uint64_t e0 = 0; e0 < L; e0 += 32) {
-        const uint64_t e = e0 + lane;
-        const bool live = e < L;
-        V v = V();
-        if (live) v = in[e];
-        const uint32_t c = live ? d(v) : static_cast<uint32_t>(M);
-        const uint32_t peers = __match_any_sync(0xffffffffu, c);
-        const uint32_t before = live ? hist[c] : 0u;
-        const uint32_t r = __popc(peers & lt);
-        if (live) out[before + r] = v;
-        __syncwarp();
-        if (live && (peers >> lane) == 1u) hist[c] = before + r + 1u;
-        __syncwarp();
+    for (uint32_t e = b; e < e1; e++) {
+        const V v = src[e];
+        const uint32_t c = d(v);
+        dst[base.get(c)] = v;
+        base.inc(c);
     }
 }
 
-template <class V, class D, int M, int THREADS>
-__global__ void __launch_bounds__(THREADS) seg_main(SegArgs a, D d) {
-    using L = SegSmem<V, M, THREADS>;
-    constexpr int ITEMS = L::kItems;
+template <class V, class D, int M, int THREADS, int STAGES>
+__global__ void __launch_bounds__(THREADS, 3)
+    seg_main(SegArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
+    using L = SegSmem<V, M, THREADS, STAGES>;
+    using TG = typename L::G;
+    constexpr int ITEMS = TG::kItems;
     constexpr int P = L::kTile;
+    constexpr int ROWS = TG::kRows;
     constexpr uint32_t AU = L::kAU;
     constexpr int W = THREADS / 32;
-    constexpr int PER = THREADS / 32;
-    constexpr uint32_t K = 32;  // segments per small-segment group
     static_assert(M <= 16 && M >= 2, "class bound");
-    static_assert(M <= 2 * W, "each warp scans at most two rows");
-    static_assert(PER == 8, "row scans load 8 entries per lane");
-    static_assert(L::kStageElems < 65536, "16-bit stage slots");
+    static_assert(ROWS <= 256, "TMA box height");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    V* stage = reinterpret_cast<V*>(smem_raw);
-    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(smem_raw + L::kStageBytes);
+    const uint32_t raw = smem_addr(smem_raw);
+    unsigned char* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    // small groups
+    V* g_in0 = reinterpret_cast<V*>(base);
+    V* g_out = g_in0 + 2 * L::kGroupElems;
+    // runs (aliases the group buffers)
+    V* ring = reinterpret_cast<V*>(base);
+    V* stage = reinterpret_cast<V*>(base + L::kRingBytes);
+    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(base + L::kRingBytes + TG::kStageBytes);
 
-    __shared__ uint32_t ticket_sh, next_seg_sh;
-    __shared__ uint32_t hist[W][M];
+    __shared__ __align__(8) uint64_t bars[STAGES];
+    __shared__ __align__(8) uint64_t gbars[2];
+    __shared__ TileShared<M> sh;
+    __shared__ uint32_t ticket_sh[2];
+    __shared__ uint32_t gi_h[2], gi_he[2], gi_next[2];  // group pipeline slots
+    __shared__ uint64_t gi_r0[2], gi_r1[2], gi_as[2], gi_tail[2];
     __shared__ uint32_t red[W][M];
-    __shared__ uint32_t run_start[M], run_cnt[M], run_dst[M], rowtot[M];
-    __shared__ uint32_t piece_base[M];  // class offset in segment + piece's exclusive prefix
     __shared__ int fail_sh;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -346,44 +444,129 @@ __global__ void __launch_bounds__(THREADS) seg_main(SegArgs a, D d) {
     V* out = static_cast<V*>(a.out);
     const uint32_t out_phase =
         static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
+    const bool in_vec = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
+    const bool out_vec = (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
+    const bool tma_ok = a.use_tma != 0;
     const uint64_t S = seg_count(a);
     const uint32_t epoch = a.hdr->epoch;
-    const uint32_t num_lw = a.hdr->num_lw;
-    const uint32_t lag = min(max(a.hdr->lag_cur, 1u), max(num_lw, 1u));
-    const uint32_t small_items = static_cast<uint32_t>((S + K - 1) / K);
-    const uint32_t total = small_items + 2u * num_lw;
-    uint16_t* my_cnt = cnt_sm + tid;
-    const uint32_t e0 = tid * ITEMS;
+    const uint32_t num_runs = a.hdr->num_runs;
+    const uint32_t num_groups = a.hdr->num_groups;
+    // S(j) trails C(j) by the most runs of one segment (so it only waits on
+    // earlier tickets) plus half a grid of slack (so those are mostly done)
+    const uint32_t lag = min(max(a.hdr->lag_cur, 1u) + gridDim.x / 2u, max(num_runs, 1u));
+    const uint32_t num_batches = (num_groups + kGroupBatch - 1) / kGroupBatch;
+    const uint32_t total = num_batches + 2u * num_runs;
+    uint32_t ring_uses = 0;   // mbarrier phase bookkeeping across items
+    uint32_t group_uses = 0;
 
-    for (;;) {
-        if (tid == 0) ticket_sh = atomicAdd(&a.hdr->ticket, 1u);
+    if (tid == 0) {
+#pragma unroll
+        for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+        mbar_init(&gbars[0], 1);
+        mbar_init(&gbars[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    // A ticket is taken only when the CTA is ready to work on it: a ticket held
+    // while its CTA waits on another item would delay every item that waits on
+    // it in turn.
+    for (uint32_t it = 0;; it++) {
+        if (tid == 0) ticket_sh[it & 1u] = atomicAdd(&a.hdr->ticket, 1u);
         __syncthreads();
-        const uint32_t t = ticket_sh;
+        const uint32_t t = ticket_sh[it & 1u];
         if (t >= total) break;
 
-        if (t < small_items) {
-            // ---------------- small segments: one warp per segment ----------
-            if (tid == 0) next_seg_sh = 0;
-            __syncthreads();
-            const uint64_t g0 = static_cast<uint64_t>(t) * K;
-            for (;;) {
-                uint32_t q = 0;
-                if (lane == 0) q = atomicAdd(&next_seg_sh, 1u);
-                q = __shfl_sync(0xffffffffu, q, 0);
-                if (q >= K) break;
-                const uint64_t s = g0 + q;
-                if (s >= S) break;
-                const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
-                if (a1 < a0 || a1 > a.n) continue;          // malformed: flagged by the planner
-                if (a1 - a0 > static_cast<uint64_t>(P)) continue;  // large: window items
-                seg_small_warp<V, D, M>(a, d, s, a0, a1 - a0, hist[warp]);
+        if (t < num_batches) {
+            // ---------------- a batch of small-segment groups ----------------
+            // group i of the batch: segments [h, he), elements [r0, r1); its
+            // range is fetched by one bulk copy while the previous group is
+            // partitioned
+            const uint32_t g0 = t * kGroupBatch;
+            const uint32_t gcnt = min(static_cast<uint32_t>(kGroupBatch), num_groups - g0);
+            auto issue_group = [&](uint32_t i) {  // thread 0 only
+                const uint32_t slot = (group_uses + i) & 1u;
+                const uint32_t h = a.groups[g0 + i];
+                const uint32_t he = static_cast<uint32_t>(min(static_cast<uint64_t>(a.groups_end[g0 + i]), S));
+                const uint64_t r0 = a.offsets[h], r1 = a.offsets[he];
+                const uint64_t as = r0 & ~static_cast<uint64_t>(AU - 1u);
+                uint64_t ve = min((r1 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u),
+                                  a.n & ~static_cast<uint64_t>(AU - 1u));
+                if (!in_vec || ve < as) ve = as;
+                gi_h[slot] = h;
+                gi_he[slot] = he;
+                gi_next[slot] = h;
+                gi_r0[slot] = r0;
+                gi_r1[slot] = r1;
+                gi_as[slot] = as;
+                gi_tail[slot] = max(ve, r0);
+                V* dst = g_in0 + slot * L::kGroupElems;
+                const uint32_t bytes = static_cast<uint32_t>((ve - as) * sizeof(V));
+                if (bytes > 0) {
+                    mbar_arrive_expect_tx(&gbars[slot], bytes);
+                    bulk_load_g2s(dst, in + as, bytes, &gbars[slot]);
+                } else {
+                    mbar_arrive(&gbars[slot]);
+                }
+            };
+            if (tid == 0) issue_group(0);
+            bool failed = false;
+            for (uint32_t i = 0; i < gcnt; i++) {
+                const uint32_t use = group_uses + i;
+                const uint32_t slot = use & 1u;
+                const bool ok = mbar_wait_bounded(&gbars[slot], (use >> 1) & 1u);
+                __syncthreads();  // slot info visible
+                V* gin = g_in0 + slot * L::kGroupElems;
+                const uint64_t as = gi_as[slot], r0 = gi_r0[slot], r1 = gi_r1[slot];
+                for (uint64_t e = gi_tail[slot] + tid; e < r1; e += THREADS) gin[e - as] = in[e];
+                if (__syncthreads_or(!ok)) {
+                    failed = true;
+                    if (tid == 0) {  // only this group's copy can be in flight
+                        atomicOr(&a.hdr->error, kErrTimeout);
+                        (void)mbar_wait_bounded(&gbars[slot], (use >> 1) & 1u);
+                    }
+                    break;
+                }
+                if (tid == 0 && i + 1 < gcnt) issue_group(i + 1);  // the other buffer is free
+                const uint32_t he = gi_he[slot];
+                for (;;) {
+                    uint32_t s = 0;
+                    if (lane == 0) s = atomicAdd(&gi_next[slot], 1u);
+                    s = __shfl_sync(0xffffffffu, s, 0);
+                    if (s >= he) break;
+                    const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
+                    seg_small_warp<V, D, M>(a, d, s, a0, static_cast<uint32_t>(a1 - a0),
+                                            gin + (a0 - as), g_out + (a0 - as));
+                }
+                __syncthreads();
+                // write the range back from the output image
+                if (out_vec && out_phase == 0u) {
+                    const uint64_t vs = (r0 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u);
+                    const uint64_t ve = r1 & ~static_cast<uint64_t>(AU - 1u);
+                    if (vs < ve) {
+                        const uint4* srcv = reinterpret_cast<const uint4*>(g_out + (vs - as));
+                        uint4* dstv = reinterpret_cast<uint4*>(out + vs);
+                        const uint32_t nv = static_cast<uint32_t>((ve - vs) / AU);
+                        for (uint32_t q = tid; q < nv; q += THREADS) dstv[q] = srcv[q];
+                        for (uint64_t e = r0 + tid; e < vs; e += THREADS) out[e] = g_out[e - as];
+                        for (uint64_t e = ve + tid; e < r1; e += THREADS) out[e] = g_out[e - as];
+                    } else {
+                        for (uint64_t e = r0 + tid; e < r1; e += THREADS) out[e] = g_out[e - as];
+                    }
+                } else {
+                    for (uint64_t e = r0 + tid; e < r1; e += THREADS) out[e] = g_out[e - as];
+                }
+                // generic-proxy accesses of these buffers precede the next TMA writes
+                fence_proxy_async_smem();
             }
+            group_uses += gcnt;
             __syncthreads();
+            if (failed) break;
             continue;
         }
 
-        // ---------------- large-segment window items ----------------
-        const uint32_t u = t - small_items;
+        // ---------------- runs of large segments ----------------
+        const uint32_t u = t - num_batches;
         uint32_t j;
         bool is_count;
         if (u < lag) {
@@ -391,78 +574,78 @@ __global__ void __launch_bounds__(THREADS) seg_main(SegArgs a, D d) {
             is_count = true;
         } else {
             const uint32_t v = u - lag;
-            const uint32_t pairs = num_lw - lag;
+            const uint32_t pairs = num_runs - lag;
             if (v < 2u * pairs) {
                 is_count = (v & 1u) != 0u;
                 j = is_count ? lag + (v >> 1) : (v >> 1);
             } else {
                 is_count = false;
                 j = pairs + (v - 2u * pairs);
-                if (lag >= num_lw) j = num_lw - 1u - j;  // all counts first: walk back for L2 reuse
+                if (lag >= num_runs) j = num_runs - 1u - j;  // all counts first: walk back (L2)
             }
         }
-        const LwEntry ent = a.lw[j];
-        const uint32_t wbase = (ent.p0 / P) * P;
-        const uint32_t lo = ent.p0 - wbase, hi = ent.p1 - wbase;
-        const bool first_piece = (ent.p0 == static_cast<uint32_t>(a.offsets[ent.seg]));
-        const bool last_piece = (j == ent.jlast);
-
-        // the piece's elements, blocked: thread t holds tile-local e0 .. e0+ITEMS-1
-        V v[ITEMS];
-        const bool whole = (e0 >= lo) && (e0 + ITEMS <= hi);
-        if (whole) {
-            const uint4* vp = reinterpret_cast<const uint4*>(in + wbase + e0);
-            const bool al = ((reinterpret_cast<uintptr_t>(in) & 15u) == 0);
-            if (al) {
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const uint4 r = __ldg(vp + q);
-                    unpack16_to<V>(r, &v[q * AU]);
-                }
-            } else {
-#pragma unroll
-                for (int q = 0; q < ITEMS; q++) v[q] = in[wbase + e0 + q];
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < ITEMS; q++)
-                v[q] = (e0 + q >= lo && e0 + q < hi) ? in[wbase + e0 + q] : V();
-        }
+        const RunEntry ent = a.runs[j];
+        const uint64_t seg_start = a.offsets[ent.seg];
+        const bool first_run = (ent.p0 == static_cast<uint32_t>(seg_start));
+        const bool last_run = (j == ent.jlast);
 
         if (is_count) {
-            // ---------------- C(j): class counts of the piece + look-back ----
-            NibbleCounts<M> nc;
-            nc.init();
-            uint32_t last_c = M;
+            // ---------------- C(j): class counts of the run + look-back ----
+            PackedCounts<M> pc;
+            pc.init();
+            const uint64_t p0 = ent.p0, p1 = ent.p1;
+            const uint64_t vs = in_vec ? ((p0 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u)) : p1;
+            const uint64_t ve = in_vec ? max(vs, p1 & ~static_cast<uint64_t>(AU - 1u)) : p1;
+            for (uint64_t e = p0 + tid; e < min(vs, p1); e += THREADS) pc.add(d(in[e]));
+            for (uint64_t e = ve + tid; e < p1 && vs < p1; e += THREADS) pc.add(d(in[e]));
+            {
+                const uint4* vp = reinterpret_cast<const uint4*>(in + vs);
+                const uint32_t nv = static_cast<uint32_t>((ve - vs) / AU);
+                int since_flush = 0;
+                constexpr int UNROLL = 4;
+                for (uint32_t q = tid; q < nv; q += THREADS * UNROLL) {
+                    uint4 r[UNROLL];
 #pragma unroll
-            for (int q = 0; q < ITEMS; q++) {
-                if (e0 + q >= lo && e0 + q < hi) {
-                    const uint32_t c = d(v[q]);
-                    if (q < 15) nc.inc(c); else last_c = c;
+                    for (int uu = 0; uu < UNROLL; uu++)
+                        if (q + uu * THREADS < nv) r[uu] = __ldg(vp + q + uu * THREADS);
+#pragma unroll
+                    for (int uu = 0; uu < UNROLL; uu++)
+                        if (q + uu * THREADS < nv) {
+                            V e[AU];
+                            unpack16_to<V>(r[uu], e);
+#pragma unroll
+                            for (uint32_t z = 0; z < AU; z++) pc.add(d(e[z]));
+                        }
+                    if (++since_flush == 14) {  // <= 14 * 16 + 2 * 3 edge elements < 256
+                        pc.flush();
+                        since_flush = 0;
+                    }
                 }
             }
+            pc.flush();
 #pragma unroll
             for (int c = 0; c < M; c++) {
-                const uint32_t x = warp_sum(nc.get(c) + (static_cast<uint32_t>(c) == last_c ? 1u : 0u));
+                const uint32_t x = warp_sum(pc.acc[c]);
                 if (lane == 0) red[warp][c] = x;
             }
             __syncthreads();
             if (warp == 0) {
                 const uint32_t c = lane;
+                const bool cls = c < static_cast<uint32_t>(M);
                 uint32_t agg = 0;
-                if (c < static_cast<uint32_t>(M))
+                if (cls)
                     for (int w = 0; w < W; w++) agg += red[w][c];
                 uint64_t* st = a.status + static_cast<uint64_t>(j) * M;
                 uint32_t prefix = 0;
                 bool ok = true;
-                if (c < static_cast<uint32_t>(M)) {
-                    if (first_piece) {
+                if (cls) {
+                    if (first_run) {
                         a.excl[static_cast<uint64_t>(j) * M + c] = 0u;
                         __threadfence();
                         st_release_u64(st + c, st_pack(epoch, kStInc, agg));
                     } else {
                         st_release_u64(st + c, st_pack(epoch, kStAgg, agg));
-                        // decoupled look-back over this segment's earlier pieces
+                        // decoupled look-back over this segment's earlier runs
                         for (uint32_t jj = j - 1u;; jj--) {
                             uint64_t w;
                             if (!wait_status(a.status + static_cast<uint64_t>(jj) * M + c, epoch,
@@ -479,14 +662,15 @@ __global__ void __launch_bounds__(THREADS) seg_main(SegArgs a, D d) {
                     }
                 }
                 if (__any_sync(0xffffffffu, !ok) && lane == 0) atomicOr(&a.hdr->error, kErrTimeout);
-                if (last_piece) {
+                if (last_run) {
                     // segment totals -> sizes (tuple and head-flag forms)
-                    const uint32_t tot = (c < static_cast<uint32_t>(M)) ? prefix + agg : 0u;
+                    const uint32_t tot = cls ? prefix + agg : 0u;
                     const uint32_t incl = warp_incl_scan(tot);
-                    const uint64_t a0 = a.offsets[ent.seg];
-                    if (c < static_cast<uint32_t>(M)) {
-                        if (a.seg_sizes != nullptr && c < a.m) a.seg_sizes[static_cast<uint64_t>(ent.seg) * a.m + c] = tot;
-                        if (a.headflags != nullptr && tot > 0) a.headflags[a0 + incl - tot] = tot;
+                    if (cls) {
+                        if (a.seg_sizes != nullptr && c < a.m)
+                            a.seg_sizes[static_cast<uint64_t>(ent.seg) * a.m + c] = tot;
+                        if (a.headflags != nullptr && tot > 0)
+                            a.headflags[seg_start + incl - tot] = tot;
                     }
                 }
             }
@@ -494,8 +678,7 @@ __global__ void __launch_bounds__(THREADS) seg_main(SegArgs a, D d) {
             continue;
         }
 
-        // ---------------- S(j): scatter the piece ----------------
-        // totals of the segment (its last entry) and this piece's prefix
+        // ---------------- S(j): scatter the run ----------------
         if (warp == 0) {
             const uint32_t c = lane;
             bool ok = true;
@@ -510,121 +693,70 @@ __global__ void __launch_bounds__(THREADS) seg_main(SegArgs a, D d) {
             }
             const uint32_t incl = warp_incl_scan(tot);
             if (c < static_cast<uint32_t>(M))
-                piece_base[c] = static_cast<uint32_t>(a.offsets[ent.seg]) + (incl - tot) + pre;
+                sh.cursor[0][c] = static_cast<uint32_t>(seg_start) + (incl - tot) + pre;
             const bool bad = __any_sync(0xffffffffu, !ok);
             if (lane == 0) {
                 fail_sh = bad ? 1 : 0;
                 if (bad) atomicOr(&a.hdr->error, kErrTimeout);
             }
         }
-        // local ranks of the piece's elements (as in plain_scatter_tma_kernel)
-        NibbleCounts<M> nc;
-        nc.init();
-        uint32_t lr[(ITEMS + 7) / 8];
-#pragma unroll
-        for (int q = 0; q < (ITEMS + 7) / 8; q++) lr[q] = 0;
-        uint32_t last_c = M;
-#pragma unroll
-        for (int q = 0; q < ITEMS; q++) {
-            if (e0 + q >= lo && e0 + q < hi) {
-                const uint32_t c = d(v[q]);
-                lr[q >> 3] += nc.get(c) << (4 * (q & 7));
-                if (q < 15) nc.inc(c); else last_c = c;
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < M; c++) my_cnt[c * THREADS] = static_cast<uint16_t>(nc.get(c));
-        if (last_c < static_cast<uint32_t>(M)) my_cnt[last_c * THREADS] += 1;
         __syncthreads();
-        if (fail_sh) {
-            __syncthreads();
-            continue;
-        }
-        uint32_t pre_r[2][PER];
+        if (fail_sh) continue;  // uniform: nothing was issued
+        const uint32_t wf = ent.p0 / P, wl = (ent.p1 - 1u) / P;
+        const uint32_t ntiles = wl - wf + 1u;
+        auto issue = [&](uint32_t i) {  // tile wf+i into ring slot (ring_uses+i) % STAGES
+            const uint32_t w = wf + i;
+            const uint32_t slot = (ring_uses + i) % STAGES;
+            const bool whole = static_cast<uint64_t>(w) * P >= ent.p0 &&
+                               static_cast<uint64_t>(w + 1) * P <= ent.p1;
+            if (tma_ok && whole) {
+                mbar_arrive_expect_tx(&bars[slot], P * sizeof(V));
+                tma_load_2d(ring + slot * P, &tmap, 0, static_cast<int32_t>(w * ROWS), &bars[slot]);
+            } else {
+                mbar_arrive(&bars[slot]);
+            }
+        };
+        if (tid == 0)
+            for (uint32_t i = 0; i < STAGES && i < ntiles; i++) issue(i);
+        const uint32_t e0 = tid * ITEMS;
+        bool failed = false;
+        for (uint32_t i = 0; i < ntiles; i++) {
+            const uint32_t w = wf + i;
+            const uint64_t ts = static_cast<uint64_t>(w) * P;
+            const uint32_t lo = static_cast<uint32_t>(max(static_cast<uint64_t>(ent.p0), ts) - ts);
+            const uint32_t hi = static_cast<uint32_t>(min(static_cast<uint64_t>(ent.p1), ts + P) - ts);
+            const bool full = lo == 0u && hi == static_cast<uint32_t>(P);
+            const uint32_t use = ring_uses + i;
+            const bool ok = mbar_wait_bounded(&bars[use % STAGES], (use / STAGES) & 1u);
+            V v[ITEMS];
+            if (tma_ok && full) {
+                take_swizzled<V, ITEMS>(ring + (use % STAGES) * P, v);
+            } else {
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int c = warp + h * W;
-            if (c < M) {
-                const uint4 xw = *reinterpret_cast<const uint4*>(cnt_sm + c * THREADS + lane * PER);
-                const uint32_t x[8] = {xw.x & 0xffffu, xw.x >> 16, xw.y & 0xffffu, xw.y >> 16,
-                                       xw.z & 0xffffu, xw.z >> 16, xw.w & 0xffffu, xw.w >> 16};
-                uint32_t tot = 0;
-#pragma unroll
-                for (int q = 0; q < 8; q++) tot += x[q];
-                const uint32_t incl = warp_incl_scan(tot);
-                uint32_t run = incl - tot;
-#pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    pre_r[h][q] = run;
-                    run += x[q];
+                for (int q = 0; q < ITEMS; q++)
+                    v[q] = (e0 + q >= lo && e0 + q < hi) ? in[ts + e0 + q] : V();
+            }
+            const bool done = tile_scatter<V, D, M, THREADS, true>(
+                d, v, lo, hi, full, stage, cnt_sm, sh, i & 1u, out, out_phase, ok, [&] {
+                    if (tid == 0 && i + STAGES < ntiles) issue(i + STAGES);
+                });
+            if (!done) {
+                failed = true;
+                if (tid == 0) {
+                    atomicOr(&a.hdr->error, kErrTimeout);
+                    for (uint32_t q = i; q < ntiles && q < i + STAGES; q++)
+                        (void)mbar_wait_bounded(&bars[(ring_uses + q) % STAGES],
+                                                ((ring_uses + q) / STAGES) & 1u);
                 }
-                if (lane == 31) rowtot[c] = incl;
+                break;
             }
         }
+        ring_uses += ntiles;
+        // the ring and the stage alias the group buffers: the bulk stores must
+        // have read the stage before a group item may overwrite it
+        if (tid < M) bulk_wait_read<0>();
         __syncthreads();
-        {
-            const uint32_t c = static_cast<uint32_t>(lane);
-            const uint32_t cc = c < static_cast<uint32_t>(M) ? rowtot[c] : 0u;
-            // the piece's class-c elements precede nothing else of the piece in
-            // the output: its class-c run starts at piece_base[c]
-            const uint32_t dst = c < static_cast<uint32_t>(M) ? piece_base[c] : 0u;
-            const uint32_t room = cc + (c < static_cast<uint32_t>(M) ? AU : 0u);
-            const uint32_t q0 = warp_incl_scan(room) - room;
-            const uint32_t st = q0 + (((out_phase + dst) - q0) & (AU - 1u));
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int row = warp + h * W;
-                if (row < M) {
-                    const uint32_t add = __shfl_sync(0xffffffffu, st, row);
-                    const uint32_t add2 = add | (add << 16);
-                    *reinterpret_cast<uint4*>(cnt_sm + row * THREADS + lane * PER) =
-                        make_uint4((pre_r[h][0] | (pre_r[h][1] << 16)) + add2,
-                                   (pre_r[h][2] | (pre_r[h][3] << 16)) + add2,
-                                   (pre_r[h][4] | (pre_r[h][5] << 16)) + add2,
-                                   (pre_r[h][6] | (pre_r[h][7] << 16)) + add2);
-                }
-            }
-            if (warp == 0 && c < static_cast<uint32_t>(M)) {
-                run_start[c] = st;
-                run_cnt[c] = cc;
-                run_dst[c] = dst;
-            }
-        }
-        if (tid < M) bulk_wait_read<0>();  // the stage's previous bulk stores
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < ITEMS; q++) {
-            if (e0 + q >= lo && e0 + q < hi) {
-                const uint32_t c = d(v[q]);
-                const uint32_t slot = my_cnt[c * THREADS] + ((lr[q >> 3] >> (4 * (q & 7))) & 15u);
-                stage[slot] = v[q];
-            }
-        }
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (tid < M) {
-            const uint32_t s = run_start[tid], cc = run_cnt[tid];
-            uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
-            if (head > cc) head = cc;
-            const uint32_t body = ((cc - head) / AU) * AU;
-            if (body > 0)
-                bulk_store_s2g(out + run_dst[tid] + head, stage + s + head, body * sizeof(V));
-            bulk_commit();
-        } else if (tid >= 32 && tid < 32 + M * 2 * static_cast<int>(AU)) {
-            const uint32_t c = (tid - 32) / (2 * AU), q = (tid - 32) % (2 * AU);
-            const uint32_t s = run_start[c], cc = run_cnt[c];
-            uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
-            if (head > cc) head = cc;
-            const uint32_t body = ((cc - head) / AU) * AU;
-            uint32_t off = 0xffffffffu;
-            if (q < AU) {
-                if (q < head) off = q;
-            } else if (head + body + (q - AU) < cc) {
-                off = head + body + (q - AU);
-            }
-            if (off != 0xffffffffu) out[run_dst[c] + off] = stage[s + off];
-        }
-        __syncthreads();
+        if (failed) break;
     }
     if (tid < M) bulk_wait_all();
 }

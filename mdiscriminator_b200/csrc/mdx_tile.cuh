@@ -1,0 +1,265 @@
+// mdx_tile.cuh -- the per-tile rank / stage / write-out step shared by the
+// plain scatter kernel and the segmented scatter items (m <= 16).
+//
+// A tile is THREADS * ITEMS elements (64 contiguous bytes per thread).  For
+// the elements of tile-local range [lo, hi):
+//  * pass 1: each thread ranks its own consecutive elements with 4-bit
+//    counters in a register (local rank = number of its earlier elements of
+//    the same class; the 16th element is kept aside so no lane can reach 16)
+//    and publishes its per-class counts to a [class][thread] u16 matrix;
+//  * row scans: warp w scans rows w and w + W of the matrix (exclusive prefix
+//    over threads = stable order); every warp derives the tile's class runs
+//    (lanes = classes) and folds each run's stage slot into its rows;
+//  * pass 2: element -> stage slot = row prefix + local rank;
+//  * write-out: each class run sits in the stage at the same 16-byte phase as
+//    its destination, so its aligned interior leaves by one bulk store
+//    (cp.async.bulk shared -> global) and threads store the < 16-byte head and
+//    tail.  Before the stage is rewritten the previous bulk stores must have
+//    read it (cp.async.bulk.wait_group.read).
+#pragma once
+
+#include "mdx_device.cuh"
+
+namespace mdx {
+
+// Per-thread class counters in 4-bit lanes: one u32 holds 8 classes, two
+// hold 16.
+template <int M>
+struct NibbleCounts {
+    static_assert(M <= 16, "nibble counters cover at most 16 classes");
+    static constexpr int NW = (M + 7) / 8;
+    uint32_t w[NW];
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int q = 0; q < NW; q++) w[q] = 0;
+    }
+    __device__ __forceinline__ uint32_t get(uint32_t c) const {
+        if constexpr (NW == 1) {
+            return (w[0] >> (c << 2)) & 15u;
+        } else {
+            return (((c < 8u) ? w[0] : w[1]) >> ((c & 7u) << 2)) & 15u;
+        }
+    }
+    __device__ __forceinline__ void inc(uint32_t c) {
+        if constexpr (NW == 1) {
+            w[0] += 1u << (c << 2);
+        } else {
+            const uint32_t one = 1u << ((c & 7u) << 2);
+            if (c < 8u) w[0] += one; else w[1] += one;
+        }
+    }
+};
+
+template <class V>
+__device__ __forceinline__ void unpack16_to(const uint4& r, V* e);
+template <>
+__device__ __forceinline__ void unpack16_to<uint32_t>(const uint4& r, uint32_t* e) {
+    e[0] = r.x; e[1] = r.y; e[2] = r.z; e[3] = r.w;
+}
+template <>
+__device__ __forceinline__ void unpack16_to<uint64_t>(const uint4& r, uint64_t* e) {
+    e[0] = static_cast<uint64_t>(r.x) | (static_cast<uint64_t>(r.y) << 32);
+    e[1] = static_cast<uint64_t>(r.z) | (static_cast<uint64_t>(r.w) << 32);
+}
+
+template <class V, int THREADS, int M>
+struct TileGeom {
+    static constexpr int kItems = 64 / static_cast<int>(sizeof(V));  // 64 bytes per thread
+    static constexpr int kTile = THREADS * kItems;
+    static constexpr int kRows = kTile * static_cast<int>(sizeof(V)) / 128;  // 128-byte rows
+    static constexpr uint32_t kAU = 16 / sizeof(V);                 // elements per 16 bytes
+    // every class run gets kAU slots of slack for its 16-byte phase
+    static constexpr int kStageElems = kTile + static_cast<int>(kAU) * M;
+    static constexpr size_t kStageBytes = static_cast<size_t>(kStageElems) * sizeof(V);
+    static constexpr size_t kCntBytes = static_cast<size_t>(M) * THREADS * 2;  // u16 counts
+    static_assert(kStageElems < 65536, "stage slots are kept in 16 bits");
+};
+
+// Shared-memory state of the tile step.
+template <int M>
+struct TileShared {
+    uint32_t cursor[2][M];  // ping-pong by tile parity
+    uint32_t run_start[M], run_cnt[M], run_dst[M], rowtot[M];
+};
+
+// Take a thread's 64 bytes of a tile that TMA placed in shared memory with
+// the 128-byte swizzle (16-byte chunk q of 128-byte row r sits at chunk
+// q ^ (r & 7)).
+template <class V, int ITEMS>
+__device__ __forceinline__ void take_swizzled(const V* tile, V (&v)[ITEMS]) {
+    constexpr uint32_t AU = 16 / sizeof(V);
+    const unsigned char* tb = reinterpret_cast<const unsigned char*>(tile);
+    const uint32_t row = threadIdx.x >> 1;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint32_t chunk = ((threadIdx.x & 1u) * 4u + q) ^ (row & 7u);
+        const uint4 r = *reinterpret_cast<const uint4*>(tb + row * 128u + chunk * 16u);
+        unpack16_to<V>(r, &v[q * AU]);
+    }
+}
+
+// One tile: see the file comment.  `full` means lo == 0 and hi == TILE (no
+// bounds checks).  FORWARD: run c of this tile starts at cursor[par][c] and
+// the cursor advances; otherwise it ends there and the cursor moves back.
+// `after_counts` runs right after the first barrier (the input ring slot is
+// consumed by then).  Returns false, having written nothing, when `ok` is
+// false on any thread.
+template <class V, class D, int M, int THREADS, bool FORWARD, class AfterCounts>
+__device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeof(V)], uint32_t lo,
+                                             uint32_t hi, bool full, V* stage, uint16_t* cnt_sm,
+                                             TileShared<M>& sh, uint32_t par, V* out,
+                                             uint32_t out_phase, bool ok,
+                                             AfterCounts after_counts) {
+    using G = TileGeom<V, THREADS, M>;
+    constexpr int ITEMS = G::kItems;
+    constexpr uint32_t AU = G::kAU;
+    constexpr int W = THREADS / 32;
+    constexpr int PER = THREADS / 32;
+    constexpr int LR = (ITEMS + 7) / 8;
+    static_assert(M <= 16 && M >= 2, "class bound");
+    static_assert(M <= 2 * W, "each warp scans at most two rows");
+    static_assert(ITEMS == 16 || ITEMS == 8, "64 bytes of 4- or 8-byte elements");
+    static_assert(PER == 8, "row scans load 8 entries per lane");
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t e0 = tid * ITEMS;
+    uint16_t* my_cnt = cnt_sm + tid;  // this thread's column: my_cnt[c * THREADS]
+
+    // ---- pass 1
+    NibbleCounts<M> nc;
+    nc.init();
+    uint32_t lr[LR];
+#pragma unroll
+    for (int q = 0; q < LR; q++) lr[q] = 0;
+    uint32_t last_c = M;  // class of element 15 (kept out of the nibbles)
+    if (full) {
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const uint32_t c = d(v[j]);
+            lr[j >> 3] += nc.get(c) << (4 * (j & 7));
+            if (j < 15) nc.inc(c); else last_c = c;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            if (e0 + j >= lo && e0 + j < hi) {
+                const uint32_t c = d(v[j]);
+                lr[j >> 3] += nc.get(c) << (4 * (j & 7));
+                if (j < 15) nc.inc(c); else last_c = c;
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < M; c++) my_cnt[c * THREADS] = static_cast<uint16_t>(nc.get(c));
+    if (last_c < static_cast<uint32_t>(M)) my_cnt[last_c * THREADS] += 1;
+    if (__syncthreads_or(!ok)) return false;  // (A)
+    after_counts();
+
+    // ---- row scans: warp w owns rows w and w + W
+    uint32_t pre[2][PER];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int c = warp + h * W;
+        if (c < M) {
+            const uint4 xw = *reinterpret_cast<const uint4*>(cnt_sm + c * THREADS + lane * PER);
+            const uint32_t x[8] = {xw.x & 0xffffu, xw.x >> 16, xw.y & 0xffffu, xw.y >> 16,
+                                   xw.z & 0xffffu, xw.z >> 16, xw.w & 0xffffu, xw.w >> 16};
+            uint32_t tot = 0;
+#pragma unroll
+            for (int q = 0; q < 8; q++) tot += x[q];
+            const uint32_t incl = warp_incl_scan(tot);
+            uint32_t run = incl - tot;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                pre[h][q] = run;
+                run += x[q];
+            }
+            if (lane == 31) sh.rowtot[c] = incl;
+        }
+    }
+    __syncthreads();  // (B)
+
+    // ---- class runs (every warp, lanes = classes): destination of run c and
+    // its stage slot, at the destination's 16-byte phase within kAU slots of
+    // slack per run
+    {
+        const uint32_t c = static_cast<uint32_t>(lane);
+        const bool cls = c < static_cast<uint32_t>(M);
+        const uint32_t cc = cls ? sh.rowtot[c] : 0u;
+        const uint32_t cur = cls ? sh.cursor[par][c] : 0u;
+        const uint32_t dst = FORWARD ? cur : cur - cc;
+        const uint32_t room = cc + (cls ? AU : 0u);
+        const uint32_t q0 = warp_incl_scan(room) - room;
+        const uint32_t st = q0 + (((out_phase + dst) - q0) & (AU - 1u));
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int row = warp + h * W;
+            if (row < M) {
+                // slots < kStageElems < 2^16: pairs of u16 prefixes per word
+                const uint32_t add = __shfl_sync(0xffffffffu, st, row);
+                const uint32_t add2 = add | (add << 16);
+                *reinterpret_cast<uint4*>(cnt_sm + row * THREADS + lane * PER) =
+                    make_uint4((pre[h][0] | (pre[h][1] << 16)) + add2,
+                               (pre[h][2] | (pre[h][3] << 16)) + add2,
+                               (pre[h][4] | (pre[h][5] << 16)) + add2,
+                               (pre[h][6] | (pre[h][7] << 16)) + add2);
+            }
+        }
+        if (warp == 0 && cls) {
+            sh.cursor[par ^ 1u][c] = FORWARD ? cur + cc : dst;
+            sh.run_start[c] = st;
+            sh.run_cnt[c] = cc;
+            sh.run_dst[c] = dst;
+        }
+    }
+    // the stage is about to be rewritten: the previous tile's bulk stores
+    // must have finished reading it
+    if (tid < M) bulk_wait_read<0>();
+    __syncthreads();  // (C)
+
+    // ---- pass 2: scatter into the class-sorted stage
+    if (full) {
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            const uint32_t c = d(v[j]);
+            stage[my_cnt[c * THREADS] + ((lr[j >> 3] >> (4 * (j & 7))) & 15u)] = v[j];
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < ITEMS; j++) {
+            if (e0 + j >= lo && e0 + j < hi) {
+                const uint32_t c = d(v[j]);
+                stage[my_cnt[c * THREADS] + ((lr[j >> 3] >> (4 * (j & 7))) & 15u)] = v[j];
+            }
+        }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();  // (D)
+
+    // ---- write-out: bulk store of each run's aligned interior; threads store
+    // the unaligned head and tail elements
+    if (tid < M) {
+        const uint32_t s = sh.run_start[tid], cc = sh.run_cnt[tid];
+        uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
+        if (head > cc) head = cc;
+        const uint32_t body = ((cc - head) / AU) * AU;
+        if (body > 0) bulk_store_s2g(out + sh.run_dst[tid] + head, stage + s + head, body * sizeof(V));
+        bulk_commit();
+    } else if (tid >= 32 && tid < 32 + M * 2 * static_cast<int>(AU)) {
+        const uint32_t c = (tid - 32) / (2 * AU), q = (tid - 32) % (2 * AU);
+        const uint32_t s = sh.run_start[c], cc = sh.run_cnt[c];
+        uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
+        if (head > cc) head = cc;
+        const uint32_t body = ((cc - head) / AU) * AU;
+        uint32_t off = 0xffffffffu;
+        if (q < AU) {
+            if (q < head) off = q;
+        } else if (head + body + (q - AU) < cc) {
+            off = head + body + (q - AU);
+        }
+        if (off != 0xffffffffu) out[sh.run_dst[c] + off] = stage[s + off];
+    }
+    return true;
+}
+
+}  // namespace mdx
