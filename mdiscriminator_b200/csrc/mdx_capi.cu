@@ -25,10 +25,15 @@ constexpr int kStages = 2;
 constexpr size_t kHeaderBytes = 256;  // done, error, ... (see WsHeader)
 constexpr size_t kAlign = 256;
 
-struct WsHeader {  // first bytes of every workspace
-    uint32_t done;
-    uint32_t error;
+struct WsHeader {  // first bytes of every workspace (the segmented header extends it)
+    uint32_t seg_ticket;  // segmented kernel's ticket (SegHeader::ticket)
+    uint32_t error;       // latched error bits, shared by every entry point
 };
+// The plain path's chunk ticket has a slot of its own, outside the 64-byte
+// segmented header: one workspace may serve plain and segmented calls in turn,
+// and each path leaves its own counters as the next call of that path expects.
+constexpr size_t kPlainDoneOffset = 192;
+static_assert(sizeof(SegHeader) <= kPlainDoneOffset, "plain ticket outside the segmented header");
 
 template <class V>
 struct ElemCfg;
@@ -215,7 +220,7 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.class_tot = reinterpret_cast<uint32_t*>(ws + L.class_tot);
     a.sizes = d_sizes;
     a.headflags = d_headflags;
-    a.done = &reinterpret_cast<WsHeader*>(ws)->done;
+    a.done = reinterpret_cast<uint32_t*>(ws + kPlainDoneOffset);
     a.error = &reinterpret_cast<WsHeader*>(ws)->error;
     a.m = m;
     a.use_tma = 0;

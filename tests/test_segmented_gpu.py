@@ -195,3 +195,23 @@ def test_full_size_100k_lognormal_segments(cuda_ready):
     assert torch.equal(out, d.to(torch.int32)[order])
     counts = torch.bincount(key, minlength=len(lengths) * 4).view(-1, 4)
     assert torch.equal(seg_sizes.to(torch.int64), counts)
+
+
+def test_one_workspace_serves_plain_and_segmented_calls(cuda_ready):
+    """Plain and segmented calls alternate on the cached workspace: each path
+    keeps its own counters, so neither leaves state the other misreads."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    lengths = lognormal_lengths(300, 71)
+    offs = offsets_from_lengths(lengths)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 72)
+    d = torch.from_numpy(x).cuda()
+    do = torch.from_numpy(offs.view(np.int64)).cuda()
+    eo, es = oracle.partition(x, 8)
+    so, ss = oracle.partition_segmented(x, offs, 4)
+    for _ in range(2):
+        out, seg_sizes = mdx.partition_segmented(d, do, ("mod", 4))
+        assert np.array_equal(out.cpu().numpy(), so) and np.array_equal(seg_sizes.cpu().numpy(), ss)
+        out, sizes = mdx.partition(d, ("mod", 8))
+        assert np.array_equal(out.cpu().numpy(), eo) and np.array_equal(sizes.cpu().numpy(), es)
+    assert mdx.workspace(0).error() == mdx.MDX_OK
