@@ -147,6 +147,32 @@ mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segmen
                            void* d_out, int32_t* d_new_sizes, mdx_elem elem, mdx_discr discr,
                            void* d_ws, size_t ws_bytes, mdx_stream_t stream);
 
+/*
+ * mdx_partition for callers that cannot allocate device memory (no
+ * counterpart in the reference): code running inside a device allocator or
+ * memory-pool callback, a plugin whose host forbids device allocations after
+ * start-up, or a loop that cannot afford cudaMalloc's device-wide
+ * synchronisation, and that has no workspace to hand in.  Same arguments and
+ * results as mdx_partition minus the workspace: the scratch is a fixed
+ * 525,312-byte array inside the library, present on every GPU that loads it
+ * until the process exits.
+ *   - m <= 16 at any n < 2^32; m > 16 returns MDX_ERR_WORKSPACE (the request
+ *     needs more scratch than the array holds) before anything is launched.
+ *   - The first call on a device does a one-time set-up for that device
+ *     (looks up the array's device address, sets kernel attributes): make it
+ *     before any stream capture.
+ *   - All calls share the array; each call clears what must start at zero on
+ *     its stream.  Calls that may overlap on the GPU race: keep them in one
+ *     stream or order them.
+ *   - A device-side wait that runs out (a tile copy that never lands within a
+ *     second) is not reported by this entry point; use mdx_partition with a
+ *     workspace and mdx_workspace_error where that report is needed.
+ * Allocates nothing: no cudaMalloc, no cudaFree, no allocating library call.
+ */
+mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                 mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                                 mdx_stream_t stream);
+
 /* Human-readable text of a status. */
 const char* mdx_strerror(mdx_status s);
 
