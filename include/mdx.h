@@ -148,6 +148,31 @@ mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segmen
                            void* d_ws, size_t ws_bytes, mdx_stream_t stream);
 
 /*
+ * CUDA-graph capture and replay (SURVEY's mdx_graph_*; the reference launches
+ * every kernel from the host each call, cuda_code/MdiscrSegmHost.cu.h:70-158).
+ * mdx_graph_partition / mdx_graph_partition_segmented record one call with
+ * the given arguments into a CUDA graph (captured on a private stream of the
+ * current device; nothing runs yet); mdx_graph_launch replays it on `stream`
+ * (the pointers are fixed, their contents may change between replays; replays
+ * sharing a workspace must not overlap); mdx_graph_destroy frees it.
+ */
+typedef struct mdx_graph_st* mdx_graph;
+
+mdx_status mdx_graph_partition(mdx_graph* graph, const void* d_in, void* d_out, uint64_t n,
+                               mdx_elem elem, mdx_discr discr, uint32_t* d_sizes,
+                               uint32_t* d_headflags, void* d_ws, size_t ws_bytes);
+
+mdx_status mdx_graph_partition_segmented(mdx_graph* graph, const void* d_in, void* d_out,
+                                         uint64_t n, mdx_elem elem, mdx_discr discr,
+                                         const uint64_t* d_offsets, uint64_t num_segments,
+                                         uint32_t* d_seg_sizes, uint32_t* d_headflags,
+                                         void* d_ws, size_t ws_bytes);
+
+mdx_status mdx_graph_launch(mdx_graph graph, mdx_stream_t stream);
+
+mdx_status mdx_graph_destroy(mdx_graph graph);
+
+/*
  * mdx_partition for callers that cannot allocate device memory (no
  * counterpart in the reference): code running inside a device allocator or
  * memory-pool callback, a plugin whose host forbids device allocations after

@@ -1,0 +1,180 @@
+// mdx/mdiscr.cuh -- header-only drop-in for the reference's host templates.
+//
+// A program written against the reference keeps its functors and calls; it
+// swaps the include and compiles with nvcc for sm_100a (-I<repo>/include):
+//
+//   #include "MdiscrHost_optimized_clean.cu.h"   ->   #include "mdx/mdiscr.cuh"
+//   mdiscr<Mod8>(n, 1 << 16, d_in, d_out)          (same call)
+//   mdiscrSegm<Mod4>(n, in, segment_sizes, out, new_sizes)   (same call)
+//
+// Signatures (reference):
+//   template<class DISCR> typename DISCR::TupleType
+//   mdiscr(const unsigned int n, const unsigned int num_hwd_thds,
+//          typename DISCR::InType* d_in, typename DISCR::InType* d_out)
+//     -- cuda_code/MdiscrHost_optimized_clean.cu.h:9-15
+//   template<class DISCR> void
+//   mdiscrSegm(unsigned int n, typename DISCR::InType* in, int* segment_sizes,
+//              typename DISCR::InType* out, int* new_sizes)
+//     -- cuda_code/MdiscrSegmHost.cu.h:36-42
+//
+// DISCR follows the reference's functor concept (HelpersCommon.h:587-596):
+// InType (4 or 8 bytes), TupleType with `cardinal` (m) and operator[], and a
+// static `apply(InType) -> unsigned` callable on the device (__host__
+// __device__).  Any such functor runs through the same sm_100a kernels as the
+// C ABI: m <= 64 for mdiscr, m <= 16 for mdiscrSegm.
+//
+// Differences from the reference: no per-call cudaMalloc (a workspace per
+// device is allocated on first use and grown when a call needs more; it is
+// kept until exit); errors print and exit like the reference's gpuErrchk
+// (HelpersHost.cu.h:11-19) unless MDX_NO_EXIT is defined, which makes them
+// throw std::runtime_error; `num_hwd_thds` is accepted and ignored.  Calls are
+// synchronous on the legacy default stream, as the reference's are.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <stdexcept>
+#include <type_traits>
+
+#include "../mdx.h"
+#include "../../mdiscriminator_b200/csrc/mdx_host.cuh"
+
+namespace mdx {
+namespace detail {
+
+inline const char* status_text(mdx_status s) {
+    switch (s) {
+        case MDX_OK: return "ok";
+        case MDX_ERR_INVALID: return "invalid argument";
+        case MDX_ERR_WORKSPACE: return "workspace too small or misaligned";
+        case MDX_ERR_CUDA: return "CUDA runtime error";
+        case MDX_ERR_TIMEOUT: return "device-side bounded wait timed out";
+        case MDX_ERR_UNSUPPORTED: return "unsupported request";
+        case MDX_ERR_SEGMENTS: return "malformed segment description";
+    }
+    return "unknown status";
+}
+
+inline void check(mdx_status s, const char* file, int line) {
+    if (s == MDX_OK) return;
+#ifdef MDX_NO_EXIT
+    (void)file;
+    (void)line;
+    throw std::runtime_error(status_text(s));
+#else
+    std::fprintf(stderr, "mdx error (%d): %s (%s, line %d)\n", static_cast<int>(s), status_text(s),
+                 file, line);
+    std::exit(static_cast<int>(s));
+#endif
+}
+
+// One zero-initialised workspace per device, grown on demand.
+inline unsigned char* workspace(size_t need) {
+    static std::mutex mu;
+    static void* ptr[64] = {};
+    static size_t bytes[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (bytes[dev] < need) {
+        if (ptr[dev] != nullptr) cudaFree(ptr[dev]);  // waits for work still using it
+        ptr[dev] = nullptr;
+        bytes[dev] = 0;
+        if (cudaMalloc(&ptr[dev], need) != cudaSuccess) return nullptr;
+        if (cudaMemset(ptr[dev], 0, need) != cudaSuccess) return nullptr;
+        bytes[dev] = need;
+    }
+    return static_cast<unsigned char*>(ptr[dev]);
+}
+
+// Latched device error of a workspace (and clear it), after a synchronise.
+inline mdx_status take_error(unsigned char* ws) {
+    if (cudaDeviceSynchronize() != cudaSuccess) return MDX_ERR_CUDA;
+    uint32_t err = 0;
+    if (cudaMemcpy(&err, ws + 4, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MDX_ERR_CUDA;
+    if (err == 0) return MDX_OK;
+    cudaMemset(ws + 4, 0, 4);
+    return (err & kErrTimeout) ? MDX_ERR_TIMEOUT : MDX_ERR_SEGMENTS;
+}
+
+template <unsigned m>
+constexpr int class_bound_of() {
+    return m <= 2 ? 2 : m <= 4 ? 4 : m <= 8 ? 8 : m <= 16 ? 16 : m <= 32 ? 32 : 64;
+}
+
+template <class T>
+using elem_of = typename std::conditional<sizeof(T) == 4, uint32_t, uint64_t>::type;
+
+template <class T>
+constexpr mdx_elem elem_kind() {
+    return sizeof(T) == 4 ? MDX_ELEM_U32 : MDX_ELEM_REC8;
+}
+
+}  // namespace detail
+
+template <class DISCR>
+typename DISCR::TupleType mdiscr(const unsigned int num_elems, const unsigned int num_hwd_thds,
+                                 typename DISCR::InType* d_in, typename DISCR::InType* d_out) {
+    using In = typename DISCR::InType;
+    static_assert(sizeof(In) == 4 || sizeof(In) == 8, "4-byte values or 8-byte records");
+    constexpr unsigned m = DISCR::TupleType::cardinal;
+    static_assert(m >= 1 && m <= 64, "1 <= m <= 64");
+    constexpr int M = detail::class_bound_of<m>();
+    using V = detail::elem_of<In>;
+    (void)num_hwd_thds;
+    typename DISCR::TupleType result;
+    for (unsigned c = 0; c < m; c++) result[c] = 0;
+    if (num_elems == 0) return result;
+    const host::PlainLayout L = host::plain_layout(num_elems, detail::elem_kind<In>(), m);
+    unsigned char* ws = detail::workspace(L.total);
+    if (ws == nullptr) detail::check(MDX_ERR_CUDA, __FILE__, __LINE__);
+    detail::check(host::check_io(d_in, d_out, num_elems, detail::elem_kind<In>()), __FILE__,
+                  __LINE__);
+    detail::check(host::run_plain<V, DiscrStatic<DISCR, M>, M>(
+                      d_in, d_out, num_elems, DiscrStatic<DISCR, M>{}, m, nullptr, nullptr, ws, L,
+                      nullptr, nullptr),
+                  __FILE__, __LINE__);
+    detail::check(detail::take_error(ws), __FILE__, __LINE__);
+    uint32_t h[64];
+    if (cudaMemcpy(h, ws + L.class_tot, m * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        detail::check(MDX_ERR_CUDA, __FILE__, __LINE__);
+    for (unsigned c = 0; c < m; c++) result[c] = h[c];
+    return result;
+}
+
+template <class DISCR>
+void mdiscrSegm(const unsigned int num_elems, typename DISCR::InType* in_array, int* segment_sizes,
+                typename DISCR::InType* out_array, int* new_sizes) {
+    using In = typename DISCR::InType;
+    static_assert(sizeof(In) == 4 || sizeof(In) == 8, "4-byte values or 8-byte records");
+    constexpr unsigned m = DISCR::TupleType::cardinal;
+    static_assert(m >= 1 && m <= 16, "the segmented path takes 1 <= m <= 16");
+    constexpr int M = detail::class_bound_of<m>();
+    using V = detail::elem_of<In>;
+    if (num_elems == 0) return;
+    const mdx_elem e = detail::elem_kind<In>();
+    detail::check(host::check_io(in_array, out_array, num_elems, e), __FILE__, __LINE__);
+    const host::SegLayout L = host::seg_layout(num_elems, num_elems, e, m, true);
+    unsigned char* ws = detail::workspace(L.total);
+    if (ws == nullptr) detail::check(MDX_ERR_CUDA, __FILE__, __LINE__);
+    detail::check(host::launch_flags_to_offsets(segment_sizes, num_elems, ws, L, nullptr), __FILE__,
+                  __LINE__);
+    const uint64_t* offs = reinterpret_cast<const uint64_t*>(ws + L.offsets);
+    detail::check(host::run_segm<V, DiscrStatic<DISCR, M>, M>(
+                      in_array, out_array, num_elems, DiscrStatic<DISCR, M>{}, m, offs,
+                      kSegsOnDevice, num_elems, segment_sizes, nullptr,
+                      reinterpret_cast<uint32_t*>(new_sizes), ws, L, nullptr),
+                  __FILE__, __LINE__);
+    detail::check(detail::take_error(ws), __FILE__, __LINE__);
+}
+
+}  // namespace mdx
+
+#ifndef MDX_NO_GLOBAL_TEMPLATES
+// The reference declares these templates at global scope.
+using mdx::mdiscr;
+using mdx::mdiscrSegm;
+#endif

@@ -95,6 +95,16 @@ def lib() -> ctypes.CDLL:
             L.mdx_partition_segmented.restype = st
             L.mdx_mdiscr_segm.argtypes = [u32, vp, vp, vp, vp, ctypes.c_int, Discr, vp, sz, vp]
             L.mdx_mdiscr_segm.restype = st
+            L.mdx_graph_partition.argtypes = [ctypes.POINTER(vp), vp, vp, u64, ctypes.c_int, Discr,
+                                              vp, vp, vp, sz]
+            L.mdx_graph_partition.restype = st
+            L.mdx_graph_partition_segmented.argtypes = [ctypes.POINTER(vp), vp, vp, u64, ctypes.c_int,
+                                                        Discr, vp, u64, vp, vp, vp, sz]
+            L.mdx_graph_partition_segmented.restype = st
+            L.mdx_graph_launch.argtypes = [vp, vp]
+            L.mdx_graph_launch.restype = st
+            L.mdx_graph_destroy.argtypes = [vp]
+            L.mdx_graph_destroy.restype = st
             L.mdx_strerror.argtypes = [st]
             L.mdx_strerror.restype = ctypes.c_char_p
             L.mdx_version.argtypes = []
@@ -343,3 +353,65 @@ def mdiscr_segm(d_in, d_segment_sizes, discr, d_out=None, d_new_sizes=None,
                                ctypes.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(stream))
     _check(st, "mdx_mdiscr_segm")
     return d_out, d_new_sizes
+
+
+# ------------------------------------------------------------- CUDA graphs --
+class Graph:
+    """One captured partition call (mdx_graph_*): replay with :meth:`launch`.
+
+    The captured pointers are fixed; their contents may change between
+    replays.  Keeps the tensors it was captured with alive."""
+
+    def __init__(self, handle, keep):
+        self._h = handle
+        self._keep = keep
+
+    def launch(self, stream=None):
+        _check(lib().mdx_graph_launch(self._h, _stream_ptr(stream)), "mdx_graph_launch")
+
+    def close(self):
+        if self._h:
+            lib().mdx_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def capture_partition(d_in, discr, out, sizes, headflags=None, ws: Optional[Workspace] = None):
+    """Capture mdx_partition(d_in -> out, sizes[, headflags]) into a Graph."""
+    _require_cuda(d_in, out, sizes, headflags)
+    dc = make_discr(discr)
+    n = d_in.numel()
+    elem = _elem_of(d_in)
+    ws = ws or new_workspace(workspace_size(n, elem, dc.m), d_in.device)
+    h = ctypes.c_void_p()
+    st = lib().mdx_graph_partition(ctypes.byref(h), ctypes.c_void_p(d_in.data_ptr()),
+                                   ctypes.c_void_p(out.data_ptr()), n, elem, dc,
+                                   ctypes.c_void_p(sizes.data_ptr()),
+                                   ctypes.c_void_p(headflags.data_ptr() if headflags is not None else 0),
+                                   ctypes.c_void_p(ws.ptr), ws.nbytes)
+    _check(st, "mdx_graph_partition")
+    return Graph(h, (d_in, out, sizes, headflags, ws))
+
+
+def capture_partition_segmented(d_in, d_offsets, discr, out, seg_sizes, headflags=None,
+                                ws: Optional[Workspace] = None):
+    """Capture mdx_partition_segmented into a Graph."""
+    _require_cuda(d_in, d_offsets, out, seg_sizes, headflags)
+    dc = make_discr(discr)
+    n = d_in.numel()
+    S = d_offsets.numel() - 1
+    elem = _elem_of(d_in)
+    ws = ws or new_workspace(segmented_workspace_size(n, S, elem, dc.m), d_in.device)
+    h = ctypes.c_void_p()
+    st = lib().mdx_graph_partition_segmented(
+        ctypes.byref(h), ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(out.data_ptr()), n, elem,
+        dc, ctypes.c_void_p(d_offsets.data_ptr()), S, ctypes.c_void_p(seg_sizes.data_ptr()),
+        ctypes.c_void_p(headflags.data_ptr() if headflags is not None else 0),
+        ctypes.c_void_p(ws.ptr), ws.nbytes)
+    _check(st, "mdx_graph_partition_segmented")
+    return Graph(h, (d_in, d_offsets, out, seg_sizes, headflags, ws))

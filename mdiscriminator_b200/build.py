@@ -56,5 +56,24 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+CPP_TEST_SRC = os.path.join(os.path.dirname(HERE), "tests", "cpp", "template_dropin.cu")
+CPP_TEST_BIN = os.path.join(os.path.dirname(HERE), "tests", "cpp", "template_dropin")
+
+
+def build_cpp_test(force: bool = False) -> str:
+    """Compile the program that uses the header-only templates (include/mdx/mdiscr.cuh)."""
+    inputs = [CPP_TEST_SRC, os.path.join(os.path.dirname(HERE), "include", "mdx", "mdiscr.cuh")]
+    newest = max([os.path.getmtime(p) for p in inputs] + [_newest_input_mtime()])
+    if not force and os.path.exists(CPP_TEST_BIN) and os.path.getmtime(CPP_TEST_BIN) >= newest:
+        return CPP_TEST_BIN
+    cmd = [nvcc(), *ARCH, "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(HERE), "include"),
+           "-o", CPP_TEST_BIN + ".tmp", CPP_TEST_SRC]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
+    os.replace(CPP_TEST_BIN + ".tmp", CPP_TEST_BIN)
+    return CPP_TEST_BIN
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

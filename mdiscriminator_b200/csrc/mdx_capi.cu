@@ -5,411 +5,11 @@
 // is a run-time parameter of the functor).
 #include <cuda_runtime.h>
 
-#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched from the runtime)
+#include "mdx_host.cuh"
 
-#include <cstdio>
-#include <cstring>
-#include <mutex>
-
-#include "../../include/mdx.h"
-#include "mdx_plain.cuh"
-#include "mdx_segm.cuh"
-#include "mdx_tile.cuh"
-
-namespace mdx {
-namespace {
-
-constexpr int kThreads = 256;
-constexpr uint32_t kMaxChunks = 4096;
-constexpr int kStages = 2;
-constexpr size_t kHeaderBytes = 256;  // done, error, ... (see WsHeader)
-constexpr size_t kAlign = 256;
-
-struct WsHeader {  // first bytes of every workspace (the segmented header extends it)
-    uint32_t seg_ticket;  // segmented kernel's ticket (SegHeader::ticket)
-    uint32_t error;       // latched error bits, shared by every entry point
-};
-// The plain path's chunk ticket has a slot of its own, outside the 64-byte
-// segmented header: one workspace may serve plain and segmented calls in turn,
-// and each path leaves its own counters as the next call of that path expects.
-constexpr size_t kPlainDoneOffset = 192;
-static_assert(sizeof(SegHeader) <= kPlainDoneOffset, "plain ticket outside the segmented header");
-
-template <class V>
-struct ElemCfg;
-template <>
-struct ElemCfg<uint32_t> {
-    static constexpr int kItems = 16;  // 4096-element tiles, 16 KB
-};
-template <>
-struct ElemCfg<uint64_t> {
-    static constexpr int kItems = 8;  // 2048-record tiles, 16 KB
-};
-
-inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
-inline uint32_t class_bound(uint32_t m) {
-    uint32_t b = 2;
-    while (b < m) b <<= 1;
-    return b;
-}
-
-inline size_t elem_bytes(mdx_elem e) { return e == MDX_ELEM_REC8 ? 8 : 4; }
-inline uint32_t tile_elems(mdx_elem e) {
-    return kThreads * (e == MDX_ELEM_REC8 ? ElemCfg<uint64_t>::kItems : ElemCfg<uint32_t>::kItems);
-}
-
-inline uint32_t num_tiles_of(uint64_t n, mdx_elem e) {
-    const uint64_t t = tile_elems(e);
-    return static_cast<uint32_t>((n + t - 1) / t);
-}
-
-inline uint32_t max_chunks_of(uint64_t n, mdx_elem e) {
-    const uint32_t nt = num_tiles_of(n, e);
-    return nt < kMaxChunks ? (nt == 0 ? 1u : nt) : kMaxChunks;
-}
-
-struct PlainLayout {
-    size_t class_base, class_tot, chunk_cnt, chunk_pre, total;
-};
-
-inline PlainLayout plain_layout(uint64_t n, mdx_elem e, uint32_t m) {
-    const uint32_t M = class_bound(m);
-    const size_t G = max_chunks_of(n, e);
-    PlainLayout L;
-    L.class_base = kHeaderBytes;
-    L.class_tot = L.class_base + kMaxClasses * 4;
-    L.chunk_cnt = align_up(L.class_tot + kMaxClasses * 4, kAlign);
-    L.chunk_pre = align_up(L.chunk_cnt + M * G * 4, kAlign);
-    L.total = align_up(L.chunk_pre + M * G * 4, kAlign);
-    return L;
-}
-
-inline bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
-
-mdx_status check_discr(mdx_discr d) {
-    if (d.m < 1 || d.m > MDX_MAX_CLASSES) return MDX_ERR_INVALID;
-    if (d.kind != MDX_DISCR_MOD && d.kind != MDX_DISCR_MASK) return MDX_ERR_INVALID;
-    if (d.kind == MDX_DISCR_MASK && !is_pow2(d.m)) return MDX_ERR_INVALID;
-    return MDX_OK;
-}
-
-mdx_status check_elem(mdx_elem e) {
-    return (e == MDX_ELEM_U32 || e == MDX_ELEM_REC8) ? MDX_OK : MDX_ERR_INVALID;
-}
-
-// Resident CTAs per SM of a kernel, cached per (device, kernel).
-struct OccEntry {
-    int device;
-    const void* fn;
-    int blocks;
-    int sms;
-};
-std::mutex g_occ_mu;
-OccEntry g_occ[256];
-int g_occ_n = 0;
-
-cudaError_t occupancy(const void* fn, size_t dyn_smem, int* blocks, int* sms) {
-    int dev = 0;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess) return err;
-    {
-        std::lock_guard<std::mutex> lk(g_occ_mu);
-        for (int i = 0; i < g_occ_n; i++)
-            if (g_occ[i].device == dev && g_occ[i].fn == fn) {
-                *blocks = g_occ[i].blocks;
-                *sms = g_occ[i].sms;
-                return cudaSuccess;
-            }
-    }
-    if (dyn_smem > 48 * 1024) {
-        err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(dyn_smem));
-        if (err != cudaSuccess) return err;
-    }
-    int b = 0, s = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, dyn_smem);
-    if (err != cudaSuccess) return err;
-    err = cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev);
-    if (err != cudaSuccess) return err;
-    if (b < 1) b = 1;
-    std::lock_guard<std::mutex> lk(g_occ_mu);
-    if (g_occ_n < 256) g_occ[g_occ_n++] = OccEntry{dev, fn, b, s};
-    *blocks = b;
-    *sms = s;
-    return cudaSuccess;
-}
-
-// cuTensorMapEncodeTiled, fetched through the runtime so the library needs no
-// direct libcuda link.
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn tensor_map_encoder() {
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
-                                             &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    return fn;
-}
-
-// The n elements viewed as rows of 128 bytes (n * sizeof(V) / 128 whole rows),
-// boxes of `box_rows` rows, 128-byte swizzle.  False if TMA cannot be used
-// (unaligned base, fewer rows than one box, encoder unavailable).
-bool make_row_map(CUtensorMap* map, const void* base, uint64_t n, size_t elem, uint32_t box_rows) {
-    std::memset(map, 0, sizeof(*map));
-    if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return false;
-    const uint64_t per_row = 128 / elem;
-    const uint64_t rows = n / per_row;
-    if (rows < box_rows) return false;
-    EncodeTiledFn enc = tensor_map_encoder();
-    if (enc == nullptr) return false;
-    const cuuint64_t dims[2] = {per_row, rows};
-    const cuuint64_t strides[1] = {128};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(per_row), box_rows};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUtensorMapDataType dt =
-        elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_UINT64;
-    return enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-template <class V, class D, int M>
-mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
-                     uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
-                     cudaStream_t stream, cudaEvent_t ev_mid) {
-    constexpr int ITEMS = ElemCfg<V>::kItems;
-    constexpr int TILE = kThreads * ITEMS;
-    auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
-    const void* scatter_fn;
-    size_t smem;
-    if constexpr (M <= 16) {
-        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
-        static_assert(SL::kTile == TILE, "both kernels use the same tiles");
-        scatter_fn = reinterpret_cast<const void*>(plain_scatter_tma_kernel<V, D, M, kThreads, kStages>);
-        smem = SL::kBytes;
-    } else {
-        scatter_fn = reinterpret_cast<const void*>(plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages>);
-        smem = plain_scatter_smem<V, TILE, kStages>();
-    }
-    int blocks = 0, sms = 0;
-    if (occupancy(scatter_fn, smem, &blocks, &sms) != cudaSuccess) return MDX_ERR_CUDA;
-    const uint32_t nt = static_cast<uint32_t>((n + TILE - 1) / TILE);
-    uint32_t G = static_cast<uint32_t>(blocks) * static_cast<uint32_t>(sms);
-    if (G > nt) G = nt;
-    if (G > kMaxChunks) G = kMaxChunks;
-
-    PlainArgs a;
-    a.in = d_in;
-    a.out = d_out;
-    a.n = n;
-    a.num_tiles = nt;
-    a.num_chunks = G;
-    a.chunk_cnt = reinterpret_cast<uint32_t*>(ws + L.chunk_cnt);
-    a.chunk_pre = reinterpret_cast<uint32_t*>(ws + L.chunk_pre);
-    a.class_base = reinterpret_cast<uint32_t*>(ws + L.class_base);
-    a.class_tot = reinterpret_cast<uint32_t*>(ws + L.class_tot);
-    a.sizes = d_sizes;
-    a.headflags = d_headflags;
-    a.done = reinterpret_cast<uint32_t*>(ws + kPlainDoneOffset);
-    a.error = &reinterpret_cast<WsHeader*>(ws)->error;
-    a.m = m;
-    a.use_tma = 0;
-    // head flags: all zero but for count_c at offset_c, which the last
-    // counting CTA writes
-    if (d_headflags != nullptr &&
-        cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    count<<<G, kThreads, 0, stream>>>(a, d);
-    if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
-    if constexpr (M <= 16) {
-        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
-        CUtensorMap map;
-        a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
-        plain_scatter_tma_kernel<V, D, M, kThreads, kStages><<<G, kThreads, smem, stream>>>(a, d, map);
-    } else {
-        plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages><<<G, kThreads, smem, stream>>>(a, d);
-    }
-    return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
-}
-
-template <class V, class D>
-mdx_status dispatch_plain_m(const void* in, void* out, uint64_t n, D d, uint32_t m, uint32_t* sz,
-                            uint32_t* hf, unsigned char* ws, const PlainLayout& L,
-                            cudaStream_t st, cudaEvent_t ev) {
-    switch (class_bound(m)) {
-        case 2: return run_plain<V, D, 2>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 4: return run_plain<V, D, 4>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 8: return run_plain<V, D, 8>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 16: return run_plain<V, D, 16>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 32: return run_plain<V, D, 32>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 64: return run_plain<V, D, 64>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        default: return MDX_ERR_INVALID;
-    }
-}
-
-// key % m == key & (m - 1) for unsigned keys when m is a power of two (Mod<4>
-// and Mod4 agree), so such MOD requests take the mask functor.
-inline bool use_mask(mdx_discr dc) { return dc.kind == MDX_DISCR_MASK || is_pow2(dc.m); }
-
-template <class V>
-mdx_status dispatch_plain(const void* in, void* out, uint64_t n, mdx_discr dc, uint32_t* sz,
-                          uint32_t* hf, unsigned char* ws, const PlainLayout& L, cudaStream_t st,
-                          cudaEvent_t ev) {
-    if (use_mask(dc))
-        return dispatch_plain_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, sz, hf, ws, L, st, ev);
-    return dispatch_plain_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, sz, hf, ws, L, st, ev);
-}
-
-// ------------------------------------------------------------- segmented --
-constexpr int kPlanThreads = 256;
-constexpr uint32_t kMaxPlanBlocks = 1024;
-constexpr int kFlagsTile = 4096;
-
-inline uint32_t window_elems(mdx_elem e) { return tile_elems(e); }
-
-struct SegLayout {
-    size_t run_loc, grp_loc, blk_runs, blk_grps, runs, groups, groups_end, status, excl, offsets,
-        flag_status, total;
-    uint64_t max_runs, max_groups;
-};
-
-// flags_form: room for n+1 offsets and the converter's tile status words.
-inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool flags_form) {
-    const uint32_t M = class_bound(m);
-    const uint64_t P = window_elems(e);
-    const uint64_t NW = (n + P - 1) / P;
-    SegLayout L;
-    L.max_runs = 2 * NW + 2;    // runs of segments that tile [0, n): far fewer
-    L.max_groups = 2 * NW + 2;  // at most one group per half tile (+ trailing empty segments)
-    L.run_loc = kHeaderBytes;
-    L.grp_loc = align_up(L.run_loc + 4 * (S + 1), kAlign);
-    L.blk_runs = align_up(L.grp_loc + 4 * (S + 1), kAlign);
-    L.blk_grps = align_up(L.blk_runs + 4 * kMaxPlanBlocks, kAlign);
-    L.runs = align_up(L.blk_grps + 4 * kMaxPlanBlocks, kAlign);
-    L.groups = align_up(L.runs + sizeof(RunEntry) * L.max_runs, kAlign);
-    L.groups_end = align_up(L.groups + 4 * L.max_groups, kAlign);
-    L.status = align_up(L.groups_end + 4 * L.max_groups, kAlign);
-    L.excl = align_up(L.status + 8ull * M * L.max_runs, kAlign);
-    L.offsets = align_up(L.excl + 4ull * M * L.max_runs, kAlign);
-    L.flag_status = L.offsets;
-    L.total = L.offsets;
-    if (flags_form) {
-        L.flag_status = align_up(L.offsets + 8 * (n + 1), kAlign);
-        L.total = align_up(L.flag_status + 8 * ((n + kFlagsTile - 1) / kFlagsTile + 1), kAlign);
-    }
-    return L;
-}
-
-inline uint32_t plan_blocks_for(uint64_t S_bound) {
-    uint64_t g = (S_bound + 511) / 512;
-    if (g < 1) g = 1;
-    if (g > kMaxPlanBlocks) g = kMaxPlanBlocks;
-    return static_cast<uint32_t>(g);
-}
-
-template <class V, class D, int M>
-mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
-                    const uint64_t* d_offsets, uint64_t S, uint64_t S_bound, const int32_t* in_flags,
-                    uint32_t* d_seg_sizes, uint32_t* d_headflags, unsigned char* ws,
-                    const SegLayout& L, cudaStream_t st) {
-    using SL = SegSmem<V, M, kThreads, kStages>;
-    constexpr int P = SL::kTile;
-    auto main_fn = seg_main<V, D, M, kThreads, kStages>;
-    int blocks = 0, sms = 0;
-    if (occupancy(reinterpret_cast<const void*>(main_fn), SL::kBytes, &blocks, &sms) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    SegArgs a;
-    a.in = d_in;
-    a.out = d_out;
-    a.n = n;
-    a.offsets = d_offsets;
-    a.num_segs = S;
-    a.seg_sizes = d_seg_sizes;
-    a.headflags = d_headflags;
-    a.in_flags = in_flags;
-    a.m = m;
-    a.hdr = reinterpret_cast<SegHeader*>(ws);
-    a.run_loc = reinterpret_cast<uint32_t*>(ws + L.run_loc);
-    a.grp_loc = reinterpret_cast<uint32_t*>(ws + L.grp_loc);
-    a.blk_runs = reinterpret_cast<uint32_t*>(ws + L.blk_runs);
-    a.blk_grps = reinterpret_cast<uint32_t*>(ws + L.blk_grps);
-    a.runs = reinterpret_cast<RunEntry*>(ws + L.runs);
-    a.groups = reinterpret_cast<uint32_t*>(ws + L.groups);
-    a.groups_end = reinterpret_cast<uint32_t*>(ws + L.groups_end);
-    a.status = reinterpret_cast<uint64_t*>(ws + L.status);
-    a.excl = reinterpret_cast<uint32_t*>(ws + L.excl);
-    a.plan_blocks = plan_blocks_for(S_bound);
-    a.max_runs = static_cast<uint32_t>(L.max_runs);
-    a.max_groups = static_cast<uint32_t>(L.max_groups);
-    CUtensorMap map;
-    a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::G::kRows) ? 1 : 0;
-    if (d_headflags != nullptr &&
-        cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), st) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    // Look-back words start from zero every call: the workspace's layout moves
-    // with n, S and m, so the epoch tag alone cannot tell a status word from
-    // another call's data.
-    if (cudaMemsetAsync(a.status, 0, L.max_runs * M * sizeof(uint64_t), st) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    if (cudaMemsetAsync(a.groups_end, 0xff, L.max_groups * sizeof(uint32_t), st) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    seg_plan_spans<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
-    seg_plan_emit<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
-    main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d, map);
-    return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
-}
-
-template <class V, class D>
-mdx_status dispatch_segm_m(const void* in, void* out, uint64_t n, D d, uint32_t m,
-                           const uint64_t* offs, uint64_t S, uint64_t Sb, const int32_t* fl,
-                           uint32_t* sz, uint32_t* hf, unsigned char* ws, const SegLayout& L,
-                           cudaStream_t st) {
-    switch (class_bound(m)) {
-        case 2: return run_segm<V, D, 2>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
-        case 4: return run_segm<V, D, 4>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
-        case 8: return run_segm<V, D, 8>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
-        case 16: return run_segm<V, D, 16>(in, out, n, d, m, offs, S, Sb, fl, sz, hf, ws, L, st);
-        default: return MDX_ERR_UNSUPPORTED;
-    }
-}
-
-template <class V>
-mdx_status dispatch_segm(const void* in, void* out, uint64_t n, mdx_discr dc, const uint64_t* offs,
-                         uint64_t S, uint64_t Sb, const int32_t* fl, uint32_t* sz, uint32_t* hf,
-                         unsigned char* ws, const SegLayout& L, cudaStream_t st) {
-    if (use_mask(dc))
-        return dispatch_segm_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, offs, S, Sb, fl, sz, hf,
-                                  ws, L, st);
-    return dispatch_segm_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, offs, S, Sb, fl, sz, hf, ws,
-                              L, st);
-}
-
-mdx_status check_io(const void* d_in, void* d_out, uint64_t n, mdx_elem elem) {
-    if (n == 0) return MDX_OK;
-    if (d_in == nullptr || d_out == nullptr) return MDX_ERR_INVALID;
-    const size_t w = elem_bytes(elem);
-    const char* ib = static_cast<const char*>(d_in);
-    const char* ob = static_cast<const char*>(d_out);
-    if (ib < ob + n * w && ob < ib + n * w) return MDX_ERR_INVALID;
-    if (reinterpret_cast<uintptr_t>(d_in) % w || reinterpret_cast<uintptr_t>(d_out) % w)
-        return MDX_ERR_INVALID;
-    return MDX_OK;
-}
-
-}  // namespace
-}  // namespace mdx
 
 using namespace mdx;
+using namespace mdx::host;
 
 extern "C" {
 
@@ -555,24 +155,90 @@ mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segmen
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     unsigned char* ws = static_cast<unsigned char*>(d_ws);
     uint64_t* offs = reinterpret_cast<uint64_t*>(ws + L.offsets);
-    int blocks = 0, sms = 0;
-    auto conv = seg_flags_to_offsets<kThreads, kFlagsTile>;
-    if (occupancy(reinterpret_cast<const void*>(conv), 0, &blocks, &sms) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    const uint32_t tiles = static_cast<uint32_t>((n + kFlagsTile - 1) / kFlagsTile);
-    uint32_t G = static_cast<uint32_t>(blocks) * sms;
-    if (G > tiles) G = tiles;
-    if (cudaMemsetAsync(ws + L.flag_status, 0, sizeof(uint64_t) * (tiles + 1), st) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    conv<<<G, kThreads, 0, st>>>(d_segment_sizes, n, offs, reinterpret_cast<SegHeader*>(ws),
-                                 reinterpret_cast<uint64_t*>(ws + L.flag_status));
-    if (cudaGetLastError() != cudaSuccess) return MDX_ERR_CUDA;
+    if ((s = launch_flags_to_offsets(d_segment_sizes, n, ws, L, st)) != MDX_OK) return s;
     uint32_t* hf = reinterpret_cast<uint32_t*>(d_new_sizes);
     if (elem == MDX_ELEM_U32)
         return dispatch_segm<uint32_t>(d_in, d_out, n, discr, offs, kSegsOnDevice, n,
                                        d_segment_sizes, nullptr, hf, ws, L, st);
     return dispatch_segm<uint64_t>(d_in, d_out, n, discr, offs, kSegsOnDevice, n, d_segment_sizes,
                                    nullptr, hf, ws, L, st);
+}
+
+}  // extern "C"
+
+struct mdx_graph_st {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+};
+
+namespace {
+// Capture what `issue` launches on a private stream into a graph.  Relaxed
+// mode: a kernel family's first call may set attributes and query occupancy
+// while capturing.
+template <class F>
+mdx_status capture_graph(mdx_graph* out, F&& issue) {
+    if (out == nullptr) return MDX_ERR_INVALID;
+    *out = nullptr;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return MDX_ERR_CUDA;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaStreamDestroy(s);
+        return MDX_ERR_CUDA;
+    }
+    const mdx_status st = issue(s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(s, &g);
+    cudaStreamDestroy(s);
+    if (st != MDX_OK || end != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return st != MDX_OK ? st : MDX_ERR_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return MDX_ERR_CUDA;
+    }
+    *out = new mdx_graph_st{g, exec};
+    return MDX_OK;
+}
+}  // namespace
+
+extern "C" {
+
+mdx_status mdx_graph_partition(mdx_graph* graph, const void* d_in, void* d_out, uint64_t n,
+                               mdx_elem elem, mdx_discr discr, uint32_t* d_sizes,
+                               uint32_t* d_headflags, void* d_ws, size_t ws_bytes) {
+    return capture_graph(graph, [&](cudaStream_t s) {
+        return mdx_partition(d_in, d_out, n, elem, discr, d_sizes, d_headflags, d_ws, ws_bytes,
+                             reinterpret_cast<mdx_stream_t>(s));
+    });
+}
+
+mdx_status mdx_graph_partition_segmented(mdx_graph* graph, const void* d_in, void* d_out,
+                                         uint64_t n, mdx_elem elem, mdx_discr discr,
+                                         const uint64_t* d_offsets, uint64_t num_segments,
+                                         uint32_t* d_seg_sizes, uint32_t* d_headflags,
+                                         void* d_ws, size_t ws_bytes) {
+    return capture_graph(graph, [&](cudaStream_t s) {
+        return mdx_partition_segmented(d_in, d_out, n, elem, discr, d_offsets, num_segments,
+                                       d_seg_sizes, d_headflags, d_ws, ws_bytes,
+                                       reinterpret_cast<mdx_stream_t>(s));
+    });
+}
+
+mdx_status mdx_graph_launch(mdx_graph graph, mdx_stream_t stream) {
+    if (graph == nullptr) return MDX_ERR_INVALID;
+    return cudaGraphLaunch(graph->exec, reinterpret_cast<cudaStream_t>(stream)) == cudaSuccess
+               ? MDX_OK
+               : MDX_ERR_CUDA;
+}
+
+mdx_status mdx_graph_destroy(mdx_graph graph) {
+    if (graph == nullptr) return MDX_OK;
+    const bool ok = cudaGraphExecDestroy(graph->exec) == cudaSuccess &&
+                    cudaGraphDestroy(graph->graph) == cudaSuccess;
+    delete graph;
+    return ok ? MDX_OK : MDX_ERR_CUDA;
 }
 
 const char* mdx_strerror(mdx_status s) {

@@ -77,7 +77,9 @@ template <class DISCR, int M>
 struct DiscrStatic {
     template <class V>
     __host__ __device__ __forceinline__ uint32_t operator()(const V& v) const {
-        const uint32_t c = DISCR::apply(v);
+        static_assert(sizeof(typename DISCR::InType) == sizeof(V), "element size");
+        const uint32_t c =
+            DISCR::apply(*reinterpret_cast<const typename DISCR::InType*>(&v));
         return c < static_cast<uint32_t>(M) ? c : static_cast<uint32_t>(M - 1);
     }
 };

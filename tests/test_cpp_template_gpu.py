@@ -1,0 +1,19 @@
+"""The header-only C++ drop-in (include/mdx/mdiscr.cuh): a program written
+against the reference's template signatures, with its own functors (a mask,
+remainders, a non-remainder class function, 8-byte records), runs the plain
+and segmented paths and checks them against a CPU stable partition."""
+import subprocess
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_template_dropin_program(cuda_ready):
+    from mdiscriminator_b200 import build as mdx_build
+    exe = mdx_build.build_cpp_test()
+    res = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    print(res.stdout)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "INVALID" not in res.stdout
+    assert res.stdout.count("VALID") == 8
