@@ -134,6 +134,22 @@ mdx_status mdx_partition_segmented(const void* d_in, void* d_out, uint64_t n, md
                                    mdx_stream_t stream);
 
 /*
+ * Segmented partition in which every segment has its own class count:
+ * segment s uses class = key % d_seg_m[s], 1 <= d_seg_m[s] <= m_max <= 16
+ * (no reference counterpart: mdiscrSegm fixes one DISCR per call,
+ * MdiscrSegmHost.cu.h:36-42).  It lets independent requests with different m
+ * share one batched launch.  Rows of d_seg_sizes are m_max wide (classes at
+ * or above a segment's m count 0).  Workspace: mdx_segmented_workspace_size
+ * with m = m_max.  A d_seg_m entry outside [1, m_max] latches
+ * MDX_ERR_SEGMENTS (the kernel clamps it).
+ */
+mdx_status mdx_partition_segmented_multi(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                         const uint32_t* d_seg_m, uint32_t m_max,
+                                         const uint64_t* d_offsets, uint64_t num_segments,
+                                         uint32_t* d_seg_sizes, uint32_t* d_headflags,
+                                         void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+/*
  * Reference-shaped segmented form with head-flag segment sizes in and out:
  *   template<class DISCR> void mdiscrSegm(n, in, int* segment_sizes, out, int* new_sizes)
  *     (cuda_code/MdiscrSegmHost.cu.h:36-42)
@@ -197,6 +213,46 @@ mdx_status mdx_graph_destroy(mdx_graph graph);
 mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
                                  mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
                                  mdx_stream_t stream);
+
+/*
+ * Serving loop (continuous batching; no reference counterpart -- the
+ * reference has one synchronous call per array).  Requests are u32 arrays
+ * with their own m (class = value % m, 1 <= m <= m_max <= 16); their buffers
+ * are device memory or page-locked host memory (pageable memory is refused
+ * with MDX_ERR_INVALID).  The server owns budget_bytes of device memory (an
+ * input and an output ring), admits requests in FIFO order as ring space
+ * allows, coalesces consecutive admitted requests into batched segmented
+ * launches on up to num_streams streams at once (new requests are admitted
+ * and launched while earlier batches run), and records every request's
+ * latency from submit to completion.
+ */
+typedef struct mdx_server_st* mdx_server;
+
+typedef struct {
+    uint64_t budget_bytes;        /* device memory for request data (both rings) */
+    uint32_t num_streams;         /* batches in flight at once (0: 2) */
+    uint32_t max_batch_requests;  /* requests per batched launch (0: 1024, <= 65535) */
+    uint64_t max_batch_elems;     /* elements per batched launch (0: ring size) */
+    uint32_t m_max;               /* largest m a request may use (0: 16, <= 16) */
+} mdx_server_config;
+
+typedef struct {
+    uint64_t submitted, completed, batches, elements;
+    uint64_t waiting, inflight_batches;
+    double p50_s, p99_s, mean_s;  /* latency of completed requests, submit to completion */
+    double window_s;              /* from the last reset to the last completion */
+} mdx_server_stats;
+
+mdx_status mdx_server_create(mdx_server* server, const mdx_server_config* config);
+/* in: n values; out: n values; sizes: m class sizes.  Returns immediately. */
+mdx_status mdx_server_submit(mdx_server server, const uint32_t* in, uint32_t* out, uint32_t* sizes,
+                             uint64_t n, uint32_t m, uint64_t* ticket);
+/* Block until the request is done; its latency in seconds. */
+mdx_status mdx_server_wait(mdx_server server, uint64_t ticket, double* latency_s);
+mdx_status mdx_server_get_stats(mdx_server server, mdx_server_stats* stats);
+mdx_status mdx_server_reset_stats(mdx_server server);
+/* Finishes the work already submitted, then frees everything. */
+mdx_status mdx_server_destroy(mdx_server server);
 
 /* Human-readable text of a status. */
 const char* mdx_strerror(mdx_status s);

@@ -93,6 +93,9 @@ def lib() -> ctypes.CDLL:
             L.mdx_partition_segmented.argtypes = [vp, vp, u64, ctypes.c_int, Discr, vp, u64, vp,
                                                   vp, vp, sz, vp]
             L.mdx_partition_segmented.restype = st
+            L.mdx_partition_segmented_multi.argtypes = [vp, vp, u64, ctypes.c_int, vp, u32, vp, u64,
+                                                        vp, vp, vp, sz, vp]
+            L.mdx_partition_segmented_multi.restype = st
             L.mdx_mdiscr_segm.argtypes = [u32, vp, vp, vp, vp, ctypes.c_int, Discr, vp, sz, vp]
             L.mdx_mdiscr_segm.restype = st
             L.mdx_graph_partition.argtypes = [ctypes.POINTER(vp), vp, vp, u64, ctypes.c_int, Discr,
@@ -327,6 +330,37 @@ def partition_segmented(d_in, d_offsets, discr, out=None, seg_sizes=None, headfl
     return (out, seg_sizes, hf) if hf is not None else (out, seg_sizes)
 
 
+def partition_segmented_multi(d_in, d_offsets, d_seg_m, m_max: int, out=None, seg_sizes=None,
+                              headflags=False, ws: Optional[Workspace] = None, stream=None):
+    """Segmented partition with a class count per segment (class = key % m_s);
+    ``d_seg_m`` is a CUDA u32/i32 tensor of S entries in [1, m_max], m_max <= 16.
+    Returns ``(out, seg_sizes[S, m_max])`` [, head flags]."""
+    torch = _torch()
+    _require_cuda(d_in, d_offsets, d_seg_m)
+    n = d_in.numel()
+    S = d_offsets.numel() - 1
+    elem = _elem_of(d_in)
+    if out is None:
+        out = torch.empty_like(d_in)
+    if seg_sizes is None:
+        seg_sizes = torch.empty((S, m_max), dtype=torch.uint32, device=d_in.device)
+    hf = None
+    if headflags is True:
+        hf = torch.empty(n, dtype=torch.uint32, device=d_in.device)
+    elif headflags is not False and headflags is not None:
+        hf = headflags
+    need = segmented_workspace_size(n, S, elem, m_max)
+    ws = ws or workspace(need, d_in.device, stream)
+    st = lib().mdx_partition_segmented_multi(
+        ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(out.data_ptr()), n, elem,
+        ctypes.c_void_p(d_seg_m.data_ptr()), m_max, ctypes.c_void_p(d_offsets.data_ptr()), S,
+        ctypes.c_void_p(seg_sizes.data_ptr()),
+        ctypes.c_void_p(hf.data_ptr() if hf is not None else 0), ctypes.c_void_p(ws.ptr),
+        ws.nbytes, _stream_ptr(stream))
+    _check(st, "mdx_partition_segmented_multi")
+    return (out, seg_sizes, hf) if hf is not None else (out, seg_sizes)
+
+
 def mdiscr_segm(d_in, d_segment_sizes, discr, d_out=None, d_new_sizes=None,
                 ws: Optional[Workspace] = None, stream=None):
     """Reference-shaped ``mdiscrSegm``: head-flag segment sizes in (i32, the
@@ -415,3 +449,98 @@ def capture_partition_segmented(d_in, d_offsets, discr, out, seg_sizes, headflag
         ctypes.c_void_p(ws.ptr), ws.nbytes)
     _check(st, "mdx_graph_partition_segmented")
     return Graph(h, (d_in, d_offsets, out, seg_sizes, headflags, ws))
+
+
+# ------------------------------------------------------------ serving loop --
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_uint64), ("num_streams", ctypes.c_uint32),
+                ("max_batch_requests", ctypes.c_uint32), ("max_batch_elems", ctypes.c_uint64),
+                ("m_max", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("batches", ctypes.c_uint64), ("elements", ctypes.c_uint64),
+                ("waiting", ctypes.c_uint64), ("inflight_batches", ctypes.c_uint64),
+                ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("mean_s", ctypes.c_double),
+                ("window_s", ctypes.c_double)]
+
+
+def _bind_server(L):
+    if getattr(L, "_server_bound", False):
+        return L
+    vp = ctypes.c_void_p
+    L.mdx_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ServerConfig)]
+    L.mdx_server_create.restype = ctypes.c_int
+    L.mdx_server_submit.argtypes = [vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32,
+                                    ctypes.POINTER(ctypes.c_uint64)]
+    L.mdx_server_submit.restype = ctypes.c_int
+    L.mdx_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
+    L.mdx_server_wait.restype = ctypes.c_int
+    L.mdx_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.mdx_server_get_stats.restype = ctypes.c_int
+    L.mdx_server_reset_stats.argtypes = [vp]
+    L.mdx_server_reset_stats.restype = ctypes.c_int
+    L.mdx_server_destroy.argtypes = [vp]
+    L.mdx_server_destroy.restype = ctypes.c_int
+    L._server_bound = True
+    return L
+
+
+class Server:
+    """Continuous-batching partition server (mdx_server_*): u32 requests with
+    their own m, in device or page-locked host tensors; FIFO admission into a
+    device pool of ``budget_bytes``; consecutive admitted requests share one
+    batched segmented launch; up to ``num_streams`` batches run at once."""
+
+    def __init__(self, budget_bytes: int, num_streams: int = 2, max_batch_requests: int = 1024,
+                 max_batch_elems: int = 0, m_max: int = 16):
+        L = _bind_server(lib())
+        cfg = ServerConfig(budget_bytes, num_streams, max_batch_requests, max_batch_elems, m_max)
+        h = ctypes.c_void_p()
+        _check(L.mdx_server_create(ctypes.byref(h), ctypes.byref(cfg)), "mdx_server_create")
+        self._h = h
+        self._L = L
+        self._keep = {}
+
+    def submit(self, d_in, d_out, sizes, m: int) -> int:
+        """Queue one request; the tensors must stay alive until wait()."""
+        for x in (d_in, d_out, sizes):
+            if not x.is_contiguous() or x.element_size() != 4:
+                raise ValueError("requests are contiguous 4-byte arrays")
+        if d_out.numel() < d_in.numel() or sizes.numel() < m:
+            raise ValueError("output needs n entries and sizes m entries")
+        t = ctypes.c_uint64()
+        _check(self._L.mdx_server_submit(self._h, ctypes.c_void_p(d_in.data_ptr()),
+                                         ctypes.c_void_p(d_out.data_ptr()),
+                                         ctypes.c_void_p(sizes.data_ptr()), d_in.numel(), m,
+                                         ctypes.byref(t)), "mdx_server_submit")
+        self._keep[t.value] = (d_in, d_out, sizes)
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        lat = ctypes.c_double()
+        st = self._L.mdx_server_wait(self._h, ticket, ctypes.byref(lat))
+        self._keep.pop(ticket, None)
+        _check(st, "mdx_server_wait")
+        return lat.value
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(self._L.mdx_server_get_stats(self._h, ctypes.byref(s)), "mdx_server_get_stats")
+        return {name: getattr(s, name) for name, _ in ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        _check(self._L.mdx_server_reset_stats(self._h), "mdx_server_reset_stats")
+
+    def close(self) -> None:
+        if self._h:
+            self._L.mdx_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -139,6 +139,36 @@ mdx_status mdx_partition_segmented(const void* d_in, void* d_out, uint64_t n, md
                                    nullptr, d_seg_sizes, d_headflags, ws, L, st);
 }
 
+mdx_status mdx_partition_segmented_multi(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                         const uint32_t* d_seg_m, uint32_t m_max,
+                                         const uint64_t* d_offsets, uint64_t num_segments,
+                                         uint32_t* d_seg_sizes, uint32_t* d_headflags,
+                                         void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
+    mdx_status s = check_elem(elem);
+    if (s != MDX_OK) return s;
+    if (m_max < 1 || m_max > 16) return m_max > 16 ? MDX_ERR_UNSUPPORTED : MDX_ERR_INVALID;
+    if (n > MDX_MAX_ELEMS || num_segments > MDX_MAX_ELEMS) return MDX_ERR_INVALID;
+    if ((s = check_io(d_in, d_out, n, elem)) != MDX_OK) return s;
+    if (num_segments == 0) return n == 0 ? MDX_OK : MDX_ERR_SEGMENTS;
+    if (d_offsets == nullptr || d_seg_m == nullptr) return MDX_ERR_INVALID;
+    const SegLayout L = seg_layout(n, num_segments, elem, m_max, false);
+    if (d_ws == nullptr || ws_bytes < L.total) return MDX_ERR_WORKSPACE;
+    if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    unsigned char* ws = static_cast<unsigned char*>(d_ws);
+    const DiscrMod d = DiscrMod::make(m_max);  // replaced per segment by key % m_s
+    auto go = [&](auto tag) -> mdx_status {
+        using V = decltype(tag);
+        switch (class_bound(m_max)) {
+            case 2: return run_segm<V, DiscrMod, 2>(d_in, d_out, n, d, m_max, d_offsets, num_segments, num_segments, nullptr, d_seg_sizes, d_headflags, ws, L, st, d_seg_m);
+            case 4: return run_segm<V, DiscrMod, 4>(d_in, d_out, n, d, m_max, d_offsets, num_segments, num_segments, nullptr, d_seg_sizes, d_headflags, ws, L, st, d_seg_m);
+            case 8: return run_segm<V, DiscrMod, 8>(d_in, d_out, n, d, m_max, d_offsets, num_segments, num_segments, nullptr, d_seg_sizes, d_headflags, ws, L, st, d_seg_m);
+            default: return run_segm<V, DiscrMod, 16>(d_in, d_out, n, d, m_max, d_offsets, num_segments, num_segments, nullptr, d_seg_sizes, d_headflags, ws, L, st, d_seg_m);
+        }
+    };
+    return elem == MDX_ELEM_U32 ? go(uint32_t{}) : go(uint64_t{});
+}
+
 mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segment_sizes,
                            void* d_out, int32_t* d_new_sizes, mdx_elem elem, mdx_discr discr,
                            void* d_ws, size_t ws_bytes, mdx_stream_t stream) {

@@ -52,7 +52,7 @@ struct DiscrMask {
 struct DiscrMod {
     uint64_t c;
     uint32_t m;
-    static DiscrMod make(uint32_t m_) {
+    __host__ __device__ static DiscrMod make(uint32_t m_) {
         DiscrMod d;
         d.m = m_;
         d.c = ~0ull / m_ + 1ull;

@@ -330,7 +330,7 @@ template <class V, class D, int M>
 mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
                     const uint64_t* d_offsets, uint64_t S, uint64_t S_bound, const int32_t* in_flags,
                     uint32_t* d_seg_sizes, uint32_t* d_headflags, unsigned char* ws,
-                    const SegLayout& L, cudaStream_t st) {
+                    const SegLayout& L, cudaStream_t st, const uint32_t* d_seg_m = nullptr) {
     using SL = SegSmem<V, M, kThreads, kStages>;
     constexpr int P = SL::kTile;
     auto main_fn = seg_main<V, D, M, kThreads, kStages>;
@@ -360,6 +360,8 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.plan_blocks = plan_blocks_for(S_bound);
     a.max_runs = static_cast<uint32_t>(L.max_runs);
     a.max_groups = static_cast<uint32_t>(L.max_groups);
+    a.seg_m = d_seg_m;
+    a.m_bound = m;
     CUtensorMap map;
     a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::G::kRows) ? 1 : 0;
     if (d_headflags != nullptr &&

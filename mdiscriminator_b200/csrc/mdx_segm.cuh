@@ -47,6 +47,8 @@
 
 #include <cuda.h>  // CUtensorMap
 
+#include <type_traits>
+
 #include "mdx_device.cuh"
 #include "mdx_plain.cuh"  // PackedCounts
 #include "mdx_tile.cuh"
@@ -113,7 +115,23 @@ struct SegArgs {
     uint32_t max_runs;         // capacity (enough for segments that tile [0, n))
     uint32_t max_groups;
     int use_tma;               // the tensor map passed to seg_main is valid
+    const uint32_t* seg_m;     // per-segment class counts (remainder discriminator), or null:
+                               // every segment uses the launch's discriminator
+    uint32_t m_bound;          // classes of any segment are < m_bound (per-segment m clamped)
 };
+
+// The discriminator of segment s: the launch's, or -- when the call carries
+// per-segment class counts -- key % m_s (m_s clamped to [1, m_bound]).
+template <class D>
+__device__ __forceinline__ D seg_discr(const SegArgs& a, const D& d, uint64_t s) {
+    if constexpr (std::is_same<D, DiscrMod>::value) {
+        if (a.seg_m != nullptr) {
+            const uint32_t m = min(max(a.seg_m[s], 1u), a.m_bound);
+            return DiscrMod::make(m);
+        }
+    }
+    return d;
+}
 
 constexpr uint64_t kSegsOnDevice = ~0ull;
 
@@ -149,6 +167,8 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
             }
             if (a.in_flags != nullptr && a1 > a0 && a1 <= a.n &&
                 static_cast<uint64_t>(a.in_flags[a0]) != a1 - a0)
+                atomicOr(&a.hdr->error, kErrSegments);
+            if (a.seg_m != nullptr && (a.seg_m[s] < 1u || a.seg_m[s] > a.m_bound))
                 atomicOr(&a.hdr->error, kErrSegments);
         }
         maxruns = max(maxruns, runs);
@@ -535,7 +555,7 @@ __global__ void __launch_bounds__(THREADS, 3)
                     s = __shfl_sync(0xffffffffu, s, 0);
                     if (s >= he) break;
                     const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
-                    seg_small_warp<V, D, M>(a, d, s, a0, static_cast<uint32_t>(a1 - a0),
+                    seg_small_warp<V, D, M>(a, seg_discr(a, d, s), s, a0, static_cast<uint32_t>(a1 - a0),
                                             gin + (a0 - as), g_out + (a0 - as));
                 }
                 __syncthreads();
@@ -586,6 +606,7 @@ __global__ void __launch_bounds__(THREADS, 3)
         }
         const RunEntry ent = a.runs[j];
         const uint64_t seg_start = a.offsets[ent.seg];
+        const D dj = seg_discr(a, d, ent.seg);
         const bool first_run = (ent.p0 == static_cast<uint32_t>(seg_start));
         const bool last_run = (j == ent.jlast);
 
@@ -596,8 +617,8 @@ __global__ void __launch_bounds__(THREADS, 3)
             const uint64_t p0 = ent.p0, p1 = ent.p1;
             const uint64_t vs = in_vec ? ((p0 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u)) : p1;
             const uint64_t ve = in_vec ? max(vs, p1 & ~static_cast<uint64_t>(AU - 1u)) : p1;
-            for (uint64_t e = p0 + tid; e < min(vs, p1); e += THREADS) pc.add(d(in[e]));
-            for (uint64_t e = ve + tid; e < p1 && vs < p1; e += THREADS) pc.add(d(in[e]));
+            for (uint64_t e = p0 + tid; e < min(vs, p1); e += THREADS) pc.add(dj(in[e]));
+            for (uint64_t e = ve + tid; e < p1 && vs < p1; e += THREADS) pc.add(dj(in[e]));
             {
                 const uint4* vp = reinterpret_cast<const uint4*>(in + vs);
                 const uint32_t nv = static_cast<uint32_t>((ve - vs) / AU);
@@ -614,7 +635,7 @@ __global__ void __launch_bounds__(THREADS, 3)
                             V e[AU];
                             unpack16_to<V>(r[uu], e);
 #pragma unroll
-                            for (uint32_t z = 0; z < AU; z++) pc.add(d(e[z]));
+                            for (uint32_t z = 0; z < AU; z++) pc.add(dj(e[z]));
                         }
                     if (++since_flush == 14) {  // <= 14 * 16 + 2 * 3 edge elements < 256
                         pc.flush();
@@ -737,7 +758,7 @@ __global__ void __launch_bounds__(THREADS, 3)
                     v[q] = (e0 + q >= lo && e0 + q < hi) ? in[ts + e0 + q] : V();
             }
             const bool done = tile_scatter<V, D, M, THREADS, true>(
-                d, v, lo, hi, full, stage, cnt_sm, sh, i & 1u, out, out_phase, ok, [&] {
+                dj, v, lo, hi, full, stage, cnt_sm, sh, i & 1u, out, out_phase, ok, [&] {
                     if (tid == 0 && i + STAGES < ntiles) issue(i + STAGES);
                 });
             if (!done) {

@@ -1,0 +1,459 @@
+// mdx_server.cu -- serving loop: continuous batching of partition requests.
+//
+// A request is one u32 array of n elements with its own class count m
+// (class = value % m, 1 <= m <= m_max <= 16); its input, output and sizes live
+// either in device memory or in page-locked host memory (both are reachable
+// from kernels through unified addressing).  The server owns a device pool of
+// `budget_bytes`: an input ring and an output ring of equal size.
+//
+//  * Admission: a submitted request waits in FIFO order until its n elements
+//    fit in the rings; admitted requests hold consecutive ring slots, so any
+//    run of them is one contiguous array.
+//  * Scheduling: whenever admitted requests are waiting and one of the
+//    `num_streams` batch slots is free, the scheduler thread takes the longest
+//    contiguous run of them (up to max_batch_requests / max_batch_elems) and
+//    issues, on that slot's stream: a gather kernel copying every request's
+//    input into its ring slot, the per-segment-m segmented partition
+//    (mdx_partition_segmented_multi: one segment per request), a scatter
+//    kernel copying results and class sizes back to each request, and a host
+//    function stamping the completion time.  Requests that arrive while
+//    batches run are admitted as ring space frees and launched on another
+//    stream: their work overlaps the batches already on the device.
+//  * Completion: ring space is released in admission order when a batch
+//    finishes; waiters are woken; the latency of every request (submit to
+//    completion stamp) goes into the p50 / p99 statistics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/mdx.h"
+
+namespace mdx {
+namespace server {
+
+constexpr int kCopyThreads = 256;
+constexpr uint32_t kCopyChunk = 8192;  // elements per copy CTA
+
+struct CopyJob {            // one request in a batch
+    const uint32_t* src;    // gather: request input;  scatter: ring output
+    uint32_t* dst;          // gather: ring input;     scatter: request output
+    uint64_t n;
+    const uint32_t* sizes_src;  // scatter only: this segment's row of class sizes
+    uint32_t* sizes_dst;        // scatter only: the request's m sizes
+    uint32_t m;
+};
+
+// blockIdx.y = request, blockIdx.x = chunk of kCopyChunk elements.
+__global__ void __launch_bounds__(kCopyThreads) copy_jobs(const CopyJob* jobs) {
+    const CopyJob j = jobs[blockIdx.y];
+    const uint64_t a = static_cast<uint64_t>(blockIdx.x) * kCopyChunk;
+    if (blockIdx.x == 0 && j.sizes_dst != nullptr && threadIdx.x < j.m)
+        j.sizes_dst[threadIdx.x] = j.sizes_src[threadIdx.x];
+    if (a >= j.n) return;
+    const uint64_t b = min(a + kCopyChunk, j.n);
+    for (uint64_t e = a + threadIdx.x; e < b; e += kCopyThreads) j.dst[e] = j.src[e];
+}
+
+// The device-side address of a buffer, or null when kernels cannot reach it
+// (pageable host memory, unknown pointers).
+template <class T>
+T* device_view(T* p) {
+    if (p == nullptr) return nullptr;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (attr.type == cudaMemoryTypeUnregistered) return nullptr;
+    return static_cast<T*>(attr.devicePointer);
+}
+
+using Clock = std::chrono::steady_clock;
+inline double now_s() {
+    return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
+}
+
+struct Req {
+    uint64_t id;
+    uint64_t n;
+    uint32_t m;
+    const uint32_t* in;
+    uint32_t* out;
+    uint32_t* sizes;
+    uint64_t off = 0;  // ring slot
+    double t_submit = 0, t_done = 0;
+    bool done = false;
+};
+
+struct Batch;
+
+struct Slot {                   // one stream's worth of batch resources
+    cudaStream_t stream = nullptr;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    uint64_t* d_offsets = nullptr;  // [max_batch + 1]
+    uint32_t* d_seg_m = nullptr;    // [max_batch]
+    uint32_t* d_seg_sizes = nullptr;  // [max_batch * m_max]
+    CopyJob* d_jobs = nullptr;      // [2 * max_batch]: gather then scatter
+    uint64_t* h_offsets = nullptr;  // pinned staging
+    uint32_t* h_seg_m = nullptr;
+    CopyJob* h_jobs = nullptr;
+    bool busy = false;
+};
+
+struct Batch {
+    int slot;
+    std::vector<uint64_t> ids;
+    uint64_t ring_end;  // ring position after this batch's requests
+    bool done = false;
+    double t_done = 0;
+    struct Server* server;
+};
+
+struct Server {
+    mdx_server_config cfg{};
+    int device = 0;
+    uint32_t* d_in = nullptr;
+    uint32_t* d_out = nullptr;
+    uint64_t cap = 0;        // elements per ring
+    uint64_t head = 0;       // next allocation
+    std::deque<std::pair<uint64_t, uint64_t>> live;  // admitted allocations (off, n), in order
+    std::vector<Slot> slots;
+
+    std::mutex mu;
+    std::condition_variable cv_sched, cv_done;
+    std::deque<Req*> waiting;   // submitted, not admitted
+    std::deque<Req*> admitted;  // in the ring, not launched
+    std::unordered_map<uint64_t, Req*> reqs;  // every request not yet collected
+    std::deque<Batch*> inflight;  // launch order
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread sched;
+    mdx_status sticky = MDX_OK;   // first failure of a launch (reported by wait)
+
+    // statistics
+    uint64_t st_submitted = 0, st_completed = 0, st_batches = 0, st_elements = 0;
+    std::vector<double> latencies;
+    double st_t0 = 0, st_t_last = 0;
+
+    // ring: [off, off + n) for a new request, or false if it does not fit now.
+    // Live allocations are consecutive in admission order; when the head wraps
+    // to 0 the unused end [head, cap) is skipped until the tail passes it.
+    bool ring_alloc(uint64_t n, uint64_t* off) {
+        if (n == 0 || n > cap) return false;
+        if (live.empty()) {
+            head = 0;
+            *off = 0;
+        } else {
+            const uint64_t tail = live.front().first;
+            if (head > tail) {  // not wrapped: free [head, cap) and [0, tail)
+                if (head + n <= cap) *off = head;
+                else if (n <= tail) *off = 0;
+                else return false;
+            } else {  // wrapped: free [head, tail)
+                if (head + n <= tail) *off = head;
+                else return false;
+            }
+        }
+        head = *off + n;
+        live.emplace_back(*off, n);
+        return true;
+    }
+};
+
+void CUDART_CB batch_done_cb(void* p) {  // runs on the driver's thread: no CUDA calls
+    Batch* b = static_cast<Batch*>(p);
+    Server* s = b->server;
+    std::lock_guard<std::mutex> lk(s->mu);
+    b->done = true;
+    b->t_done = now_s();
+    s->cv_sched.notify_all();
+}
+
+// Admit waiting requests (FIFO) while they fit.  Caller holds the lock.
+void admit(Server* s) {
+    while (!s->waiting.empty()) {
+        Req* r = s->waiting.front();
+        uint64_t off = 0;
+        if (!s->ring_alloc(r->n, &off)) break;
+        r->off = off;
+        s->admitted.push_back(r);
+        s->waiting.pop_front();
+    }
+}
+
+// Retire finished batches in launch order.  Caller holds the lock.
+void retire(Server* s) {
+    while (!s->inflight.empty() && s->inflight.front()->done) {
+        Batch* b = s->inflight.front();
+        s->inflight.pop_front();
+        for (uint64_t id : b->ids) {
+            Req* r = s->reqs[id];
+            r->t_done = b->t_done;
+            r->done = true;
+            s->live.pop_front();
+            s->st_completed++;
+            s->st_elements += r->n;
+            s->latencies.push_back(r->t_done - r->t_submit);
+            s->st_t_last = r->t_done;
+        }
+        s->slots[b->slot].busy = false;
+        delete b;
+    }
+    s->cv_done.notify_all();
+}
+
+mdx_status launch_batch(Server* s, Slot& sl, const std::vector<Req*>& batch) {
+    const uint64_t base = batch.front()->off;
+    const uint32_t S = static_cast<uint32_t>(batch.size());
+    uint64_t acc = 0;
+    for (uint32_t i = 0; i < S; i++) {
+        Req* r = batch[i];
+        sl.h_offsets[i] = acc;
+        sl.h_seg_m[i] = r->m;
+        sl.h_jobs[i] = CopyJob{r->in, s->d_in + r->off, r->n, nullptr, nullptr, 0};
+        sl.h_jobs[S + i] = CopyJob{s->d_out + r->off, r->out, r->n,
+                                   sl.d_seg_sizes + static_cast<uint64_t>(i) * s->cfg.m_max,
+                                   r->sizes, r->m};
+        acc += r->n;
+    }
+    sl.h_offsets[S] = acc;
+    uint64_t max_n = 0;
+    for (Req* r : batch) max_n = std::max(max_n, r->n);
+    const uint32_t chunks = static_cast<uint32_t>((max_n + kCopyChunk - 1) / kCopyChunk);
+    cudaStream_t st = sl.stream;
+    if (cudaMemcpyAsync(sl.d_offsets, sl.h_offsets, sizeof(uint64_t) * (S + 1),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(sl.d_seg_m, sl.h_seg_m, sizeof(uint32_t) * S, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(sl.d_jobs, sl.h_jobs, sizeof(CopyJob) * 2 * S, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess)
+        return MDX_ERR_CUDA;
+    copy_jobs<<<dim3(std::max(chunks, 1u), S), kCopyThreads, 0, st>>>(sl.d_jobs);
+    mdx_status r = mdx_partition_segmented_multi(
+        s->d_in + base, s->d_out + base, acc, MDX_ELEM_U32, sl.d_seg_m, s->cfg.m_max,
+        sl.d_offsets, S, sl.d_seg_sizes, nullptr, sl.ws, sl.ws_bytes,
+        reinterpret_cast<mdx_stream_t>(st));
+    if (r != MDX_OK) return r;
+    copy_jobs<<<dim3(std::max(chunks, 1u), S), kCopyThreads, 0, st>>>(sl.d_jobs + S);
+    return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+}
+
+void scheduler(Server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        retire(s);
+        admit(s);
+        int free_slot = -1;
+        for (size_t k = 0; k < s->slots.size(); k++)
+            if (!s->slots[k].busy) { free_slot = static_cast<int>(k); break; }
+        if (s->stop && s->admitted.empty() && s->waiting.empty() && s->inflight.empty()) break;
+        if (free_slot < 0 || s->admitted.empty()) {
+            s->cv_sched.wait(lk);
+            continue;
+        }
+        // the longest contiguous run of admitted requests, within the caps
+        std::vector<Req*> batch;
+        uint64_t elems = 0, end = 0;
+        while (!s->admitted.empty() && batch.size() < s->cfg.max_batch_requests) {
+            Req* r = s->admitted.front();
+            if (!batch.empty() && (r->off != end || elems + r->n > s->cfg.max_batch_elems)) break;
+            batch.push_back(r);
+            elems += r->n;
+            end = r->off + r->n;
+            s->admitted.pop_front();
+        }
+        Slot& sl = s->slots[free_slot];
+        sl.busy = true;
+        Batch* b = new Batch{free_slot, {}, end, false, 0, s};
+        for (Req* r : batch) b->ids.push_back(r->id);
+        s->inflight.push_back(b);
+        s->st_batches++;
+        lk.unlock();
+        mdx_status st = launch_batch(s, sl, batch);
+        if (st == MDX_OK &&
+            cudaLaunchHostFunc(sl.stream, batch_done_cb, b) != cudaSuccess)
+            st = MDX_ERR_CUDA;
+        lk.lock();
+        if (st != MDX_OK) {  // nothing will complete this batch: finish it now
+            if (s->sticky == MDX_OK) s->sticky = st;
+            b->done = true;
+            b->t_done = now_s();
+        }
+    }
+}
+
+}  // namespace server
+}  // namespace mdx
+
+struct mdx_server_st {
+    mdx::server::Server s;
+};
+
+using namespace mdx::server;
+
+extern "C" {
+
+mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
+    if (out == nullptr || cfg_in == nullptr) return MDX_ERR_INVALID;
+    *out = nullptr;
+    mdx_server_config cfg = *cfg_in;
+    if (cfg.num_streams == 0) cfg.num_streams = 2;
+    if (cfg.max_batch_requests == 0) cfg.max_batch_requests = 1024;
+    if (cfg.max_batch_requests > 65535) cfg.max_batch_requests = 65535;
+    if (cfg.m_max == 0) cfg.m_max = 16;
+    if (cfg.m_max > 16 || cfg.budget_bytes < 8 * 4096) return MDX_ERR_INVALID;
+    auto* h = new mdx_server_st();
+    Server& s = h->s;
+    s.cfg = cfg;
+    s.cap = cfg.budget_bytes / 8;  // u32 input ring + u32 output ring
+    if (s.cap > MDX_MAX_ELEMS) s.cap = MDX_MAX_ELEMS;
+    if (cfg.max_batch_elems == 0 || cfg.max_batch_elems > s.cap) s.cfg.max_batch_elems = s.cap;
+    bool ok = cudaGetDevice(&s.device) == cudaSuccess &&
+              cudaMalloc(&s.d_in, s.cap * 4) == cudaSuccess &&
+              cudaMalloc(&s.d_out, s.cap * 4) == cudaSuccess;
+    const uint32_t B = s.cfg.max_batch_requests;
+    s.slots.resize(cfg.num_streams);
+    for (auto& sl : s.slots) {
+        if (!ok) break;
+        sl.ws_bytes = mdx_segmented_workspace_size(s.cfg.max_batch_elems, B, MDX_ELEM_U32, cfg.m_max);
+        ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaMalloc(&sl.ws, sl.ws_bytes) == cudaSuccess &&
+             mdx_workspace_init(sl.ws, sl.ws_bytes, reinterpret_cast<mdx_stream_t>(sl.stream)) == MDX_OK &&
+             cudaMalloc(&sl.d_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
+             cudaMalloc(&sl.d_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
+             cudaMalloc(&sl.d_seg_sizes, sizeof(uint32_t) * B * cfg.m_max) == cudaSuccess &&
+             cudaMalloc(&sl.d_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess &&
+             cudaMallocHost(&sl.h_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
+             cudaMallocHost(&sl.h_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
+             cudaMallocHost(&sl.h_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess;
+    }
+    if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
+        mdx_server_destroy(h);
+        return MDX_ERR_CUDA;
+    }
+    s.st_t0 = now_s();
+    s.sched = std::thread(scheduler, &s);
+    *out = h;
+    return MDX_OK;
+}
+
+mdx_status mdx_server_submit(mdx_server h, const uint32_t* in, uint32_t* out, uint32_t* sizes,
+                             uint64_t n, uint32_t m, uint64_t* ticket) {
+    if (h == nullptr || ticket == nullptr) return MDX_ERR_INVALID;
+    Server& s = h->s;
+    if (m < 1 || m > s.cfg.m_max || n == 0 || n > s.cap || n > s.cfg.max_batch_elems)
+        return MDX_ERR_INVALID;
+    // every buffer must be reachable from kernels: device memory, or
+    // page-locked host memory mapped into the device's address space
+    const uint32_t* d_in = device_view(in);
+    uint32_t* d_out = device_view(out);
+    uint32_t* d_sizes = device_view(sizes);
+    if (d_in == nullptr || d_out == nullptr || d_sizes == nullptr) return MDX_ERR_INVALID;
+    Req* r = new Req();
+    r->n = n;
+    r->m = m;
+    r->in = d_in;
+    r->out = d_out;
+    r->sizes = d_sizes;
+    {
+        std::lock_guard<std::mutex> lk(s.mu);
+        r->id = s.next_id++;
+        r->t_submit = now_s();
+        s.reqs[r->id] = r;
+        s.waiting.push_back(r);
+        s.st_submitted++;
+        *ticket = r->id;
+    }
+    s.cv_sched.notify_all();
+    return MDX_OK;
+}
+
+mdx_status mdx_server_wait(mdx_server h, uint64_t ticket, double* latency_s) {
+    if (h == nullptr) return MDX_ERR_INVALID;
+    Server& s = h->s;
+    std::unique_lock<std::mutex> lk(s.mu);
+    auto it = s.reqs.find(ticket);
+    if (it == s.reqs.end()) return MDX_ERR_INVALID;
+    Req* r = it->second;
+    s.cv_done.wait(lk, [&] { return r->done; });
+    if (latency_s) *latency_s = r->t_done - r->t_submit;
+    s.reqs.erase(it);
+    delete r;
+    return s.sticky;
+}
+
+mdx_status mdx_server_get_stats(mdx_server h, mdx_server_stats* out) {
+    if (h == nullptr || out == nullptr) return MDX_ERR_INVALID;
+    Server& s = h->s;
+    std::lock_guard<std::mutex> lk(s.mu);
+    out->submitted = s.st_submitted;
+    out->completed = s.st_completed;
+    out->batches = s.st_batches;
+    out->elements = s.st_elements;
+    out->waiting = s.waiting.size();
+    out->inflight_batches = s.inflight.size();
+    std::vector<double> v = s.latencies;
+    out->p50_s = out->p99_s = out->mean_s = 0;
+    if (!v.empty()) {
+        std::sort(v.begin(), v.end());
+        out->p50_s = v[(v.size() - 1) / 2];
+        out->p99_s = v[std::min(v.size() - 1, static_cast<size_t>(0.99 * (v.size() - 1) + 0.5))];
+        double sum = 0;
+        for (double x : v) sum += x;
+        out->mean_s = sum / v.size();
+    }
+    out->window_s = s.st_t_last > s.st_t0 ? s.st_t_last - s.st_t0 : 0.0;
+    return MDX_OK;
+}
+
+mdx_status mdx_server_reset_stats(mdx_server h) {
+    if (h == nullptr) return MDX_ERR_INVALID;
+    Server& s = h->s;
+    std::lock_guard<std::mutex> lk(s.mu);
+    s.st_submitted = s.st_completed = s.st_batches = s.st_elements = 0;
+    s.latencies.clear();
+    s.st_t0 = now_s();
+    s.st_t_last = s.st_t0;
+    return MDX_OK;
+}
+
+mdx_status mdx_server_destroy(mdx_server h) {
+    if (h == nullptr) return MDX_OK;
+    Server& s = h->s;
+    if (s.sched.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(s.mu);
+            s.stop = true;
+        }
+        s.cv_sched.notify_all();
+        s.sched.join();
+    }
+    for (auto& sl : s.slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        cudaFree(sl.ws);
+        cudaFree(sl.d_offsets);
+        cudaFree(sl.d_seg_m);
+        cudaFree(sl.d_seg_sizes);
+        cudaFree(sl.d_jobs);
+        cudaFreeHost(sl.h_offsets);
+        cudaFreeHost(sl.h_seg_m);
+        cudaFreeHost(sl.h_jobs);
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    cudaFree(s.d_in);
+    cudaFree(s.d_out);
+    for (auto& kv : s.reqs) delete kv.second;
+    delete h;
+    return MDX_OK;
+}
+
+}  // extern "C"

@@ -215,3 +215,28 @@ def test_one_workspace_serves_plain_and_segmented_calls(cuda_ready):
         out, sizes = mdx.partition(d, ("mod", 8))
         assert np.array_equal(out.cpu().numpy(), eo) and np.array_equal(sizes.cpu().numpy(), es)
     assert mdx.workspace(0).error() == mdx.MDX_OK
+
+
+@pytest.mark.parametrize("m_max", [4, 16])
+def test_per_segment_class_counts(cuda_ready, m_max):
+    """One launch, a class count per segment (class = v % m_s): each segment
+    equals the oracle run with its own m."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    rng = np.random.default_rng(90 + m_max)
+    lengths = lognormal_lengths(1200, 91 + m_max)
+    offs = offsets_from_lengths(lengths)
+    seg_m = rng.integers(1, m_max + 1, size=len(lengths)).astype(np.int32)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 92)
+    out, seg_sizes, hf = mdx.partition_segmented_multi(
+        torch.from_numpy(x).cuda(), torch.from_numpy(offs.view(np.int64)).cuda(),
+        torch.from_numpy(seg_m).cuda(), m_max, headflags=True)
+    torch.cuda.synchronize()
+    assert mdx.workspace(0).error() == mdx.MDX_OK
+    go, gs, gf = out.cpu().numpy(), seg_sizes.cpu().numpy(), hf.cpu().numpy()
+    for s in range(len(lengths)):
+        a, b = int(offs[s]), int(offs[s + 1])
+        eo, es, ef = oracle.partition(x[a:b], int(seg_m[s]), headflags=True)
+        assert np.array_equal(go[a:b], eo), f"segment {s}"
+        assert np.array_equal(gs[s, :seg_m[s]], es) and not gs[s, seg_m[s]:].any()
+        assert np.array_equal(gf[a:b], ef)
