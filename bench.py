@@ -224,6 +224,84 @@ def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segmen
     }
 
 
+def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), duration_s=1.0):
+    """Served partition requests: open-loop Poisson arrivals at each offered
+    load; lengths log-uniform over [2^10, 2^24], values uniform over [0, 2^31),
+    m uniform over {2, 4, 8, 16}, class = v mod m; a 16 GiB device budget for
+    the server's request pool; requests' data in device memory (views of a
+    resident array, outputs to distinct slices).  p50 / p99 latency (submit to
+    completion) and elements/s per load, against one plain partition per
+    request issued back to back on one stream."""
+    import math
+
+    import numpy as np
+    rng = np.random.default_rng(17)
+    src_n = 1 << 28
+    src = make_input(torch, src_n, 5, dev)
+    out_pool = torch.empty(1 << 30, dtype=torch.int32, device=dev)
+    sizes_pool = torch.empty((1 << 16, 16), dtype=torch.int32, device=dev)
+    res = []
+    srv = mdx.Server(budget_bytes=16 << 30, num_streams=4, max_batch_requests=1024,
+                     max_batch_elems=1 << 28)
+
+    def make_requests(k):
+        n = np.exp(rng.uniform(math.log(1 << 10), math.log(1 << 24), size=k)).astype(np.int64)
+        m = rng.choice([2, 4, 8, 16], size=k)
+        st = rng.integers(0, src_n - (1 << 24), size=k)
+        reqs, pos = [], 0
+        for i in range(k):
+            if pos + n[i] > out_pool.numel():
+                pos = 0
+            reqs.append((src[st[i]:st[i] + n[i]], out_pool[pos:pos + n[i]],
+                         sizes_pool[i % sizes_pool.shape[0]], int(m[i]), int(n[i])))
+            pos += int(n[i])
+        return reqs
+
+    # warm-up (set-up of every kernel family)
+    for d_in, d_out, sz, m, _ in make_requests(64):
+        srv.wait(srv.submit(d_in, d_out, sz, m))
+    for load in loads:
+        k = max(int(load * duration_s), 200)
+        reqs = make_requests(k)
+        arrivals = np.cumsum(rng.exponential(1.0 / load, size=k))
+        srv.reset_stats()
+        tickets = []
+        t0 = time.perf_counter()
+        for (d_in, d_out, sz, m, _), ta in zip(reqs, arrivals):
+            while time.perf_counter() - t0 < ta:
+                pass
+            tickets.append(srv.submit(d_in, d_out, sz, m))
+        t_sub = time.perf_counter() - t0
+        for t in tickets:
+            srv.wait(t)
+        st = srv.stats()
+        elems = sum(r[4] for r in reqs)
+        res.append({"offered_req_per_s": load, "achieved_submit_rate": k / t_sub,
+                    "requests": k, "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
+                    "gelem_per_s": elems / st["window_s"] / 1e9 if st["window_s"] > 0 else None,
+                    "batches": st["batches"], "mean_request_elems": elems / k})
+    srv.close()
+    # one plain launch per request, back to back, on the same request mix
+    reqs = make_requests(400)
+    ws = mdx.new_workspace(mdx.workspace_size(1 << 24, mdx.ELEM_U32, 16), dev)
+    sizes = torch.empty(16, dtype=torch.uint32, device=dev)
+    for d_in, d_out, _, m, _ in reqs[:10]:
+        mdx.partition(d_in, ("mod", m), out=d_out, sizes=sizes[:m], ws=ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for d_in, d_out, _, m, _ in reqs:
+        mdx.partition(d_in, ("mod", m), out=d_out, sizes=sizes[:m], ws=ws)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    plain = sum(r[4] for r in reqs) / t_plain / 1e9
+    return {"workload": "served requests: Poisson arrivals, n log-uniform [2^10, 2^24] int32, "
+                        "m uniform {2,4,8,16}, 16 GiB budget, device-resident request data",
+            "loads": res,
+            "per_request_plain": {"value": plain, "unit": "Gelem/s",
+                                  "sample": "400 requests of the same mix, one mdx_partition each, "
+                                            "back to back on one stream (host wall clock)"}}
+
+
 def cpu_baseline(n_sample: int, m: int, reps: int):
     """The reference's openmpMdiscr on a bounded sample (rank 0, N=1 only)."""
     import numpy as np
@@ -290,11 +368,13 @@ def main():
     ap.add_argument("--impl", default="mdx", choices=["mdx", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--m", type=int, default=M_DEFAULT)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--ref-sample", type=int, default=1 << 25)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched segmented measurement")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served-requests measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -366,26 +446,43 @@ def main():
     call_ms = [a.elapsed_time(c) for a, _, c in ev]
     value = world * n / step_s / 1e9
 
-    # end to end through the public API: pinned host in -> partition -> host out
-    h_in = torch.empty(n, dtype=torch.int32, pin_memory=True)
-    h_in.copy_(d_in)
-    h_out = torch.empty(n, dtype=torch.int32, pin_memory=True)
-    h_sizes = torch.empty(m, dtype=torch.uint32, pin_memory=True)
-    d_in2 = torch.empty_like(d_in)
-    for _ in range(2):
-        d_in2.copy_(h_in, non_blocking=True)
-        mdx.partition(d_in2, discr, out=d_out, sizes=sizes, ws=ws)
-        h_out.copy_(d_out, non_blocking=True)
-        h_sizes.copy_(sizes, non_blocking=True)
+    # end to end through the public API: every step copies its input from
+    # pinned host memory, partitions it and copies the result and the sizes
+    # back.  Two buffer sets on two streams, so one step's device-to-host
+    # copy overlaps the next step's host-to-device copy (PCIe is full duplex).
+    e2e_sets = []
+    for k in range(2):
+        h_in = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        h_in.copy_(d_in)
+        e2e_sets.append({
+            "h_in": h_in, "h_out": torch.empty(n, dtype=torch.int32, pin_memory=True),
+            "h_sizes": torch.empty(m, dtype=torch.uint32, pin_memory=True),
+            "d_in": torch.empty_like(d_in), "d_out": torch.empty_like(d_in),
+            "sizes": torch.empty(m, dtype=torch.uint32, device=dev),
+            "ws": mdx.new_workspace(mdx.workspace_size(n, mdx.ELEM_U32, m), dev),
+            "stream": torch.cuda.Stream(device=dev)})
+
+    def e2e_step(i):
+        b = e2e_sets[i % 2]
+        with torch.cuda.stream(b["stream"]):
+            b["d_in"].copy_(b["h_in"], non_blocking=True)
+            mdx.partition(b["d_in"], discr, out=b["d_out"], sizes=b["sizes"], ws=b["ws"],
+                          stream=b["stream"])
+            b["h_out"].copy_(b["d_out"], non_blocking=True)
+            b["h_sizes"].copy_(b["sizes"], non_blocking=True)
+
+    for i in range(2):
+        e2e_step(i)
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_steps):
-        d_in2.copy_(h_in, non_blocking=True)
-        mdx.partition(d_in2, discr, out=d_out, sizes=sizes, ws=ws)
-        h_out.copy_(d_out, non_blocking=True)
-        h_sizes.copy_(sizes, non_blocking=True)
+    for b in e2e_sets:
+        b["stream"].wait_event(e0)
+    for i in range(args.e2e_steps):
+        e2e_step(i)
+    for b in e2e_sets:
+        stream.wait_stream(b["stream"])
     e1.record(stream)
     barrier()
     e2e_s = e0.elapsed_time(e1) * 1e-3
@@ -395,7 +492,8 @@ def main():
         e2e_s = float(tt.item())
     e2e_value = world * n * args.e2e_steps / e2e_s / 1e9
     # sanity: the last result equals the device result of the same input
-    assert torch.equal(h_out.to(dev), d_out)
+    assert torch.equal(e2e_sets[(args.e2e_steps - 1) % 2]["h_out"].to(dev), d_out)
+    del e2e_sets
 
     if rank == 0:
         peak, peak_src = peaks()
@@ -426,6 +524,9 @@ def main():
         batched = None
         if world == 1 and not args.no_batched:
             batched = batched_measurement(torch, mdx, dev, peak)
+        served = None
+        if world == 1 and not args.no_served:
+            served = served_measurement(torch, mdx, dev, peak)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu, why = cpu_baseline(args.ref_sample, m, reps=3)
@@ -445,6 +546,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "batched": batched,
+            "served": served,
             "clocks": clk,
             "gpu_launches": 2 * args.steps,
         }

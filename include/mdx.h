@@ -254,6 +254,24 @@ mdx_status mdx_server_reset_stats(mdx_server server);
 /* Finishes the work already submitted, then frees everything. */
 mdx_status mdx_server_destroy(mdx_server server);
 
+/*
+ * Run-time knobs of the kernels (no reference counterpart; the reference fixes
+ * its block shapes at compile time with -D macros swept by cuda_code/run.py).
+ * Entries are kept per (element layout, class bound = smallest power of two
+ * >= m, ceil(log2 n)); mdx_set_tuning sets every n bucket in
+ * [log2_n_lo, log2_n_hi].  Zero fields keep the built-in default.
+ */
+typedef struct {
+    uint32_t plain_ctas_per_sm;  /* plain path: CTAs per SM of the chunk grid (0: as many as fit) */
+    uint32_t run_tiles;          /* segmented: tiles per run of a large segment (default 8) */
+    uint32_t group_batch;        /* segmented: small-segment groups per work item (default 8) */
+    uint32_t lag_slack_pct;      /* segmented: extra lag of scatter items, % of the grid (default 50) */
+} mdx_tuning;
+
+mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,
+                          const mdx_tuning* tuning);
+mdx_status mdx_get_tuning(mdx_elem elem, uint32_t m, uint64_t n, mdx_tuning* tuning);
+
 /* Human-readable text of a status. */
 const char* mdx_strerror(mdx_status s);
 

@@ -57,6 +57,45 @@ class Discr(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("m", ctypes.c_uint32)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("plain_ctas_per_sm", ctypes.c_uint32), ("run_tiles", ctypes.c_uint32),
+                ("group_batch", ctypes.c_uint32), ("lag_slack_pct", ctypes.c_uint32)]
+
+
+TUNING_PATH = os.path.join(HERE, "tuning.json")
+
+
+def set_tuning(elem: int, m: int, log2_n_lo: int, log2_n_hi: int, **knobs) -> None:
+    """Install run-time knobs for (element layout, class bound of m, n buckets)."""
+    t = Tuning(**{k: int(v) for k, v in knobs.items() if k in dict(Tuning._fields_)})
+    _check(lib().mdx_set_tuning(elem, m, log2_n_lo, log2_n_hi, ctypes.byref(t)), "mdx_set_tuning")
+
+
+def get_tuning(elem: int, m: int, n: int) -> dict:
+    t = Tuning()
+    _check(lib().mdx_get_tuning(elem, m, n, ctypes.byref(t)), "mdx_get_tuning")
+    return {name: getattr(t, name) for name, _ in Tuning._fields_}
+
+
+def load_tuning(path: str, missing_ok: bool = False) -> int:
+    """Install the autotuner's table (mdiscriminator_b200/autotune.py output)."""
+    import json
+    if not os.path.exists(path):
+        if missing_ok:
+            return 0
+        raise FileNotFoundError(path)
+    with open(path) as f:
+        table = json.load(f)
+    k = 0
+    for e in table.get("entries", []):
+        elem = ELEM_REC8 if e["elem"] == "rec8" else ELEM_U32
+        lo, hi = e["log2_n"]
+        set_tuning(elem, e["m"], lo, hi, **{x: e[x] for x in ("plain_ctas_per_sm", "run_tiles",
+                                                             "group_batch", "lag_slack_pct") if x in e})
+        k += 1
+    return k
+
+
 _lib = None
 _lib_lock = threading.Lock()
 
@@ -108,11 +147,16 @@ def lib() -> ctypes.CDLL:
             L.mdx_graph_launch.restype = st
             L.mdx_graph_destroy.argtypes = [vp]
             L.mdx_graph_destroy.restype = st
+            L.mdx_set_tuning.argtypes = [ctypes.c_int, u32, u32, u32, ctypes.POINTER(Tuning)]
+            L.mdx_set_tuning.restype = st
+            L.mdx_get_tuning.argtypes = [ctypes.c_int, u32, u64, ctypes.POINTER(Tuning)]
+            L.mdx_get_tuning.restype = st
             L.mdx_strerror.argtypes = [st]
             L.mdx_strerror.restype = ctypes.c_char_p
             L.mdx_version.argtypes = []
             L.mdx_version.restype = ctypes.c_char_p
             _lib = L
+            load_tuning(TUNING_PATH, missing_ok=True)
     return _lib
 
 

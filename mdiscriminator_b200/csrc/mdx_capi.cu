@@ -271,6 +271,35 @@ mdx_status mdx_graph_destroy(mdx_graph graph) {
     return ok ? MDX_OK : MDX_ERR_CUDA;
 }
 
+mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,
+                          const mdx_tuning* t) {
+    if (check_elem(elem) != MDX_OK || t == nullptr || m < 1 || m > MDX_MAX_CLASSES ||
+        log2_n_lo > log2_n_hi || log2_n_hi > 33)
+        return MDX_ERR_INVALID;
+    if (t->run_tiles > 64 || t->group_batch > 1024 || t->lag_slack_pct > 400) return MDX_ERR_INVALID;
+    TuningTable& tt = tuning_table();
+    std::lock_guard<std::mutex> lk(tt.mu);
+    for (uint32_t b = log2_n_lo; b <= log2_n_hi; b++) {
+        Tuning& x = tt.t[elem == MDX_ELEM_REC8 ? 1 : 0][bound_index(class_bound(m))][b];
+        x.plain_ctas_per_sm = t->plain_ctas_per_sm;
+        x.run_tiles = t->run_tiles ? t->run_tiles : kRunTiles;
+        x.group_batch = t->group_batch ? t->group_batch : kGroupBatch;
+        x.lag_slack_pct = t->lag_slack_pct ? t->lag_slack_pct : kLagSlackPct;
+    }
+    return MDX_OK;
+}
+
+mdx_status mdx_get_tuning(mdx_elem elem, uint32_t m, uint64_t n, mdx_tuning* t) {
+    if (check_elem(elem) != MDX_OK || t == nullptr || m < 1 || m > MDX_MAX_CLASSES)
+        return MDX_ERR_INVALID;
+    const Tuning x = tuning_for(elem, class_bound(m), n);
+    t->plain_ctas_per_sm = x.plain_ctas_per_sm;
+    t->run_tiles = x.run_tiles;
+    t->group_batch = x.group_batch;
+    t->lag_slack_pct = x.lag_slack_pct;
+    return MDX_OK;
+}
+
 const char* mdx_strerror(mdx_status s) {
     switch (s) {
         case MDX_OK: return "ok";

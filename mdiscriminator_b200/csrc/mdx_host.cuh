@@ -192,6 +192,39 @@ inline bool make_row_map(CUtensorMap* map, const void* base, uint64_t n, size_t 
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// ------------------------------------------------------------------ tuning --
+// Run-time knobs per (element width, class bound, log2 n), installed by
+// mdx_set_tuning (the package loads the autotuner's table at import).
+struct Tuning {
+    uint32_t plain_ctas_per_sm = 0;  // 0: as many as fit
+    uint32_t run_tiles = kRunTiles;
+    uint32_t group_batch = kGroupBatch;
+    uint32_t lag_slack_pct = kLagSlackPct;
+};
+struct TuningTable {
+    std::mutex mu;
+    Tuning t[2][7][34];  // [elem][log2 class bound - 1][ceil log2 n]
+};
+inline TuningTable& tuning_table() {
+    static TuningTable tt;
+    return tt;
+}
+inline uint32_t log2_ceil(uint64_t x) {
+    uint32_t b = 0;
+    while ((1ull << b) < x && b < 33) b++;
+    return b;
+}
+inline int bound_index(uint32_t M) {
+    int i = 0;
+    while ((2u << i) < M && i < 6) i++;
+    return i;
+}
+inline Tuning tuning_for(mdx_elem e, uint32_t M, uint64_t n) {
+    TuningTable& tt = tuning_table();
+    std::lock_guard<std::mutex> lk(tt.mu);
+    return tt.t[e == MDX_ELEM_REC8 ? 1 : 0][bound_index(M)][log2_ceil(n)];
+}
+
 template <class V, class D, int M>
 mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
                      uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
@@ -213,6 +246,9 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     int blocks = 0, sms = 0;
     if (occupancy(scatter_fn, smem, &blocks, &sms) != cudaSuccess) return MDX_ERR_CUDA;
     const uint32_t nt = static_cast<uint32_t>((n + TILE - 1) / TILE);
+    const Tuning tun = tuning_for(sizeof(V) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_U32, M, n);
+    if (tun.plain_ctas_per_sm > 0 && static_cast<int>(tun.plain_ctas_per_sm) < blocks)
+        blocks = static_cast<int>(tun.plain_ctas_per_sm);
     uint32_t G = static_cast<uint32_t>(blocks) * static_cast<uint32_t>(sms);
     if (G > nt) G = nt;
     if (G > kMaxChunks) G = kMaxChunks;
@@ -362,6 +398,12 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.max_groups = static_cast<uint32_t>(L.max_groups);
     a.seg_m = d_seg_m;
     a.m_bound = m;
+    {
+        const Tuning tun = tuning_for(sizeof(V) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_U32, M, n);
+        a.run_tiles = tun.run_tiles >= 1 ? tun.run_tiles : kRunTiles;
+        a.group_batch = tun.group_batch >= 1 ? tun.group_batch : kGroupBatch;
+        a.lag_slack_pct = tun.lag_slack_pct;
+    }
     CUtensorMap map;
     a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::G::kRows) ? 1 : 0;
     if (d_headflags != nullptr &&

@@ -55,8 +55,10 @@
 
 namespace mdx {
 
+// Defaults of the run-time knobs (the autotuner may choose others):
 constexpr int kRunTiles = 8;     // tiles per run of a large segment
 constexpr int kGroupBatch = 8;   // small-segment groups per work item (pipelined)
+constexpr int kLagSlackPct = 50; // extra lag of scatter items, in % of the grid
 
 // status word: [63:34] epoch (30 bits), [33:32] state, [31:0] count
 constexpr uint64_t kStAgg = 1ull;
@@ -84,7 +86,7 @@ struct SegHeader {      // lives at the start of the segmented workspace
     uint32_t pad[3];
 };
 
-struct RunEntry {       // a run of up to kRunTiles tiles of one large segment
+struct RunEntry {       // a run of up to run_tiles tiles of one large segment
     uint32_t seg;       // segment index
     uint32_t p0, p1;    // element range of the run
     uint32_t jlast;     // entry index of the segment's last run
@@ -118,6 +120,9 @@ struct SegArgs {
     const uint32_t* seg_m;     // per-segment class counts (remainder discriminator), or null:
                                // every segment uses the launch's discriminator
     uint32_t m_bound;          // classes of any segment are < m_bound (per-segment m clamped)
+    uint32_t run_tiles;        // tiles per run of a large segment
+    uint32_t group_batch;      // small-segment groups per work item
+    uint32_t lag_slack_pct;    // extra lag of scatter items, in % of the grid
 };
 
 // The discriminator of segment s: the launch's, or -- when the call carries
@@ -161,7 +166,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
                 atomicOr(&a.hdr->error, kErrSegments);
             } else if (a1 - a0 > static_cast<uint64_t>(P)) {
                 const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
-                runs = (span + kRunTiles - 1) / kRunTiles;
+                runs = (span + a.run_tiles - 1) / a.run_tiles;
             } else {
                 head = (s == 0 || a.offsets[s - 1] / (P / 2) != a0 / (P / 2)) ? 1u : 0u;
             }
@@ -264,17 +269,17 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
             if (a1 >= a0 && a1 <= a.n) {
                 if (a1 - a0 > static_cast<uint64_t>(P)) {
                     const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
-                    const uint32_t nr = (span + kRunTiles - 1) / kRunTiles;
+                    const uint32_t nr = (span + a.run_tiles - 1) / a.run_tiles;
                     const uint32_t pos = roff + a.run_loc[s];
                     if (nr <= 16) {  // this thread emits the runs itself
                         if (static_cast<uint64_t>(pos) + nr <= num_runs) {
                             const uint64_t w0 = a0 / P;
                             for (uint32_t r = 0; r < nr; r++) {
-                                const uint64_t wa = w0 + static_cast<uint64_t>(r) * kRunTiles;
+                                const uint64_t wa = w0 + static_cast<uint64_t>(r) * a.run_tiles;
                                 RunEntry e;
                                 e.seg = static_cast<uint32_t>(s);
                                 e.p0 = static_cast<uint32_t>(max(a0, wa * P));
-                                e.p1 = static_cast<uint32_t>(min(a1, (wa + kRunTiles) * P));
+                                e.p1 = static_cast<uint32_t>(min(a1, (wa + a.run_tiles) * P));
                                 e.jlast = pos + nr - 1u;
                                 a.runs[pos + r] = e;
                             }
@@ -306,11 +311,11 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
             const uint64_t a0 = a.offsets[seg], a1 = a.offsets[seg + 1];
             const uint64_t w0 = a0 / P;
             for (uint32_t r = tid; r < nr; r += THREADS) {
-                const uint64_t wa = w0 + static_cast<uint64_t>(r) * kRunTiles;
+                const uint64_t wa = w0 + static_cast<uint64_t>(r) * a.run_tiles;
                 RunEntry e;
                 e.seg = seg;
                 e.p0 = static_cast<uint32_t>(max(a0, wa * P));
-                e.p1 = static_cast<uint32_t>(min(a1, (wa + kRunTiles) * P));
+                e.p1 = static_cast<uint32_t>(min(a1, (wa + a.run_tiles) * P));
                 e.jlast = pos + nr - 1u;
                 a.runs[pos + r] = e;
             }
@@ -473,8 +478,9 @@ __global__ void __launch_bounds__(THREADS, 3)
     const uint32_t num_groups = a.hdr->num_groups;
     // S(j) trails C(j) by the most runs of one segment (so it only waits on
     // earlier tickets) plus half a grid of slack (so those are mostly done)
-    const uint32_t lag = min(max(a.hdr->lag_cur, 1u) + gridDim.x / 2u, max(num_runs, 1u));
-    const uint32_t num_batches = (num_groups + kGroupBatch - 1) / kGroupBatch;
+    const uint32_t lag =
+        min(max(a.hdr->lag_cur, 1u) + gridDim.x * a.lag_slack_pct / 100u, max(num_runs, 1u));
+    const uint32_t num_batches = (num_groups + a.group_batch - 1) / a.group_batch;
     const uint32_t total = num_batches + 2u * num_runs;
     uint32_t ring_uses = 0;   // mbarrier phase bookkeeping across items
     uint32_t group_uses = 0;
@@ -502,8 +508,8 @@ __global__ void __launch_bounds__(THREADS, 3)
             // group i of the batch: segments [h, he), elements [r0, r1); its
             // range is fetched by one bulk copy while the previous group is
             // partitioned
-            const uint32_t g0 = t * kGroupBatch;
-            const uint32_t gcnt = min(static_cast<uint32_t>(kGroupBatch), num_groups - g0);
+            const uint32_t g0 = t * a.group_batch;
+            const uint32_t gcnt = min(a.group_batch, num_groups - g0);
             auto issue_group = [&](uint32_t i) {  // thread 0 only
                 const uint32_t slot = (group_uses + i) & 1u;
                 const uint32_t h = a.groups[g0 + i];

@@ -1,0 +1,66 @@
+"""Run-time knobs (mdx_set_tuning / mdx_get_tuning): host-side table checks
+on the CPU, and bit-exact results under non-default knobs on the GPU."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import mdiscriminator_b200 as mdx
+import oracle
+from mdiscriminator_b200 import build as mdx_build
+
+
+def test_tuning_table_roundtrip_and_validation():
+    mdx_build.build()
+    mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12, run_tiles=4, group_batch=16, lag_slack_pct=25,
+                   plain_ctas_per_sm=2)
+    t = mdx.get_tuning(mdx.ELEM_U32, 7, 3000)  # m=7 -> class bound 8, log2 3000 -> 12
+    assert t == {"plain_ctas_per_sm": 2, "run_tiles": 4, "group_batch": 16, "lag_slack_pct": 25}
+    assert mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20)["run_tiles"] == 8  # other bucket: default
+    assert mdx.get_tuning(mdx.ELEM_REC8, 7, 3000)["run_tiles"] == 8    # other element layout
+    with pytest.raises(mdx.MdxError):
+        mdx.set_tuning(mdx.ELEM_U32, 4, 5, 3, run_tiles=8)   # empty range
+    with pytest.raises(mdx.MdxError):
+        mdx.set_tuning(mdx.ELEM_U32, 4, 0, 40, run_tiles=8)  # past the last bucket
+    with pytest.raises(mdx.MdxError):
+        mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, run_tiles=1000)
+    mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12)  # back to the defaults
+
+
+def test_committed_table_is_well_formed():
+    if not os.path.exists(mdx.TUNING_PATH):
+        pytest.skip("no tuning table committed")
+    with open(mdx.TUNING_PATH) as f:
+        table = json.load(f)
+    for e in table["entries"]:
+        assert e["elem"] in ("u32", "rec8") and 1 <= e["m"] <= 64
+        lo, hi = e["log2_n"]
+        assert 0 <= lo <= hi <= 33
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("knobs", [dict(run_tiles=1, group_batch=1, lag_slack_pct=1, plain_ctas_per_sm=1),
+                                   dict(run_tiles=16, group_batch=32, lag_slack_pct=200,
+                                        plain_ctas_per_sm=2)])
+def test_results_do_not_depend_on_knobs(cuda_ready, knobs):
+    torch = cuda_ready
+    rng = np.random.default_rng(4)
+    lengths = np.clip(np.rint(rng.lognormal(np.log(1024), 1.5, size=1500)), 1, 1 << 22).astype(np.int64)
+    offs = np.concatenate([[0], np.cumsum(lengths)]).astype(np.uint64)
+    n = int(offs[-1])
+    x = oracle.fill_uniform_u32(n, 9)
+    mdx.set_tuning(mdx.ELEM_U32, 4, 0, 33, **knobs)
+    try:
+        d = torch.from_numpy(x).cuda()
+        out, seg_sizes = mdx.partition_segmented(d, torch.from_numpy(offs.view(np.int64)).cuda(),
+                                                 ("mod", 4))
+        pout, psizes = mdx.partition(d, ("mod", 4))
+        torch.cuda.synchronize()
+        eo, es = oracle.partition_segmented(x, offs, 4)
+        assert np.array_equal(out.cpu().numpy(), eo) and np.array_equal(seg_sizes.cpu().numpy(), es)
+        po, ps = oracle.partition(x, 4)
+        assert np.array_equal(pout.cpu().numpy(), po) and np.array_equal(psizes.cpu().numpy(), ps)
+    finally:
+        mdx.set_tuning(mdx.ELEM_U32, 4, 0, 33)
+        mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
