@@ -13,12 +13,14 @@ from mdiscriminator_b200 import build as mdx_build
 
 def test_tuning_table_roundtrip_and_validation():
     mdx_build.build()
+    other_bucket = mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20)
+    other_layout = mdx.get_tuning(mdx.ELEM_REC8, 7, 3000)
     mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12, run_tiles=4, group_batch=16, lag_slack_pct=25,
                    plain_ctas_per_sm=2)
     t = mdx.get_tuning(mdx.ELEM_U32, 7, 3000)  # m=7 -> class bound 8, log2 3000 -> 12
     assert t == {"plain_ctas_per_sm": 2, "run_tiles": 4, "group_batch": 16, "lag_slack_pct": 25}
-    assert mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20)["run_tiles"] == 8  # other bucket: default
-    assert mdx.get_tuning(mdx.ELEM_REC8, 7, 3000)["run_tiles"] == 8    # other element layout
+    assert mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20) == other_bucket   # other bucket untouched
+    assert mdx.get_tuning(mdx.ELEM_REC8, 7, 3000) == other_layout     # other element layout
     with pytest.raises(mdx.MdxError):
         mdx.set_tuning(mdx.ELEM_U32, 4, 5, 3, run_tiles=8)   # empty range
     with pytest.raises(mdx.MdxError):
@@ -26,6 +28,7 @@ def test_tuning_table_roundtrip_and_validation():
     with pytest.raises(mdx.MdxError):
         mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, run_tiles=1000)
     mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12)  # back to the defaults
+    mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
 
 
 def test_committed_table_is_well_formed():
