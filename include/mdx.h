@@ -164,7 +164,7 @@ mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segmen
                            void* d_ws, size_t ws_bytes, mdx_stream_t stream);
 
 /*
- * CUDA-graph capture and replay (SURVEY's mdx_graph_*; the reference launches
+ * CUDA-graph capture and replay (no reference counterpart: the reference launches
  * every kernel from the host each call, cuda_code/MdiscrSegmHost.cu.h:70-158).
  * mdx_graph_partition / mdx_graph_partition_segmented record one call with
  * the given arguments into a CUDA graph (captured on a private stream of the
