@@ -73,7 +73,9 @@ size_t mdx_mdiscr_segm_workspace_size(uint64_t n, mdx_elem elem, uint32_t m);
 mdx_status mdx_workspace_init(void* d_ws, size_t ws_bytes, mdx_stream_t stream);
 
 /* Synchronise `stream`, return the latched device error of the workspace
- * (MDX_OK or MDX_ERR_TIMEOUT) and clear it. */
+ * (MDX_OK; MDX_ERR_TIMEOUT: a bounded wait ran out; MDX_ERR_SEGMENTS:
+ * malformed segments; MDX_ERR_INVALID: inconsistent class counts handed to
+ * mdx_dist_scatter) and clear it. */
 mdx_status mdx_workspace_error(void* d_ws, mdx_stream_t stream);
 
 /*
@@ -213,6 +215,51 @@ mdx_status mdx_graph_destroy(mdx_graph graph);
 mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
                                  mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
                                  mdx_stream_t stream);
+
+/*
+ * Distributed plain partition (no reference counterpart: the reference is
+ * single-GPU; this is mdiscr<DISCR> of cuda_code/MdiscrHost_optimized_clean.cu.h:9-15
+ * over one array spread across R ranks, one GPU each).  Rank r holds a
+ * contiguous chunk of the global input; the global stable partition is written
+ * into R output chunks: chunk q holds output positions
+ * [q * out_chunk, (q + 1) * out_chunk) within [0, n_total) (so trailing chunks
+ * may be short or empty), the last chunk every position from
+ * (R - 1) * out_chunk on.
+ *   1. mdx_dist_count: count this rank's chunk; its m class counts go to
+ *      d_counts (device).
+ *   2. the caller all-gathers the counts of every rank into d_all_counts
+ *      ([R][m], rank-major; one tiny collective, e.g. an NCCL all-gather);
+ *   3. mdx_dist_scatter (same workspace, same n_local): each element is stored
+ *      straight into the chunk that owns its output position -- through
+ *      out_chunks[q], a HOST array of R device pointers, peers' chunks mapped
+ *      into this process (mdx_ipc_*) -- by the same kernel that ranks it; the
+ *      global m sizes go to d_sizes (device, may be NULL).  A barrier across
+ *      ranks (any collective after this call on the same stream) must precede
+ *      reading an output chunk.
+ * m <= 16 (MDX_ERR_UNSUPPORTED otherwise); out_chunk a multiple of 16 bytes
+ * of elements; chunk pointers 16-byte aligned; n_total < 2^32.  Counts that do
+ * not match this rank's own count or do not add up to n_total make the
+ * scatter write nothing and latch an error (mdx_workspace_error:
+ * MDX_ERR_INVALID).
+ */
+mdx_status mdx_dist_count(const void* d_in, uint64_t n_local, mdx_elem elem, mdx_discr discr,
+                          uint32_t* d_counts, void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+mdx_status mdx_dist_scatter(const void* d_in, uint64_t n_local, mdx_elem elem, mdx_discr discr,
+                            const uint32_t* d_all_counts, uint32_t num_ranks, uint32_t rank,
+                            void* const* out_chunks, uint64_t out_chunk, uint64_t n_total,
+                            uint32_t* d_sizes, void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+/*
+ * Peer mappings for mdx_dist_scatter's output chunks (CUDA IPC, no multicast):
+ * mdx_ipc_get_handle gives the 64-byte handle of the allocation holding d_ptr
+ * and d_ptr's offset in it; another process on the same node opens it with
+ * mdx_ipc_open (peer access enabled on demand) and releases it with
+ * mdx_ipc_close(d_ptr, offset).
+ */
+mdx_status mdx_ipc_get_handle(const void* d_ptr, void* handle, uint64_t* offset);
+mdx_status mdx_ipc_open(const void* handle, uint64_t offset, void** d_ptr);
+mdx_status mdx_ipc_close(void* d_ptr, uint64_t offset);
 
 /*
  * Serving loop (continuous batching; no reference counterpart -- the

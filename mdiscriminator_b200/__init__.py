@@ -151,6 +151,17 @@ def lib() -> ctypes.CDLL:
             L.mdx_set_tuning.restype = st
             L.mdx_get_tuning.argtypes = [ctypes.c_int, u32, u64, ctypes.POINTER(Tuning)]
             L.mdx_get_tuning.restype = st
+            L.mdx_dist_count.argtypes = [vp, u64, ctypes.c_int, Discr, vp, vp, sz, vp]
+            L.mdx_dist_count.restype = st
+            L.mdx_dist_scatter.argtypes = [vp, u64, ctypes.c_int, Discr, vp, u32, u32,
+                                           ctypes.POINTER(vp), u64, u64, vp, vp, sz, vp]
+            L.mdx_dist_scatter.restype = st
+            L.mdx_ipc_get_handle.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(u64)]
+            L.mdx_ipc_get_handle.restype = st
+            L.mdx_ipc_open.argtypes = [ctypes.c_char_p, u64, ctypes.POINTER(vp)]
+            L.mdx_ipc_open.restype = st
+            L.mdx_ipc_close.argtypes = [vp, u64]
+            L.mdx_ipc_close.restype = st
             L.mdx_strerror.argtypes = [st]
             L.mdx_strerror.restype = ctypes.c_char_p
             L.mdx_version.argtypes = []
@@ -304,6 +315,64 @@ def partition(d_in, discr, out=None, sizes=None, headflags=False, ws: Optional[W
                                    ctypes.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(stream), ev)
     _check(st, "mdx_partition")
     return (out, sizes, hf) if hf is not None else (out, sizes)
+
+
+# ------------------------------------------------- distributed plain path --
+def dist_count(d_in, discr, ws: Workspace, counts=None, stream=None):
+    """Step 1 of the distributed partition (mdx_dist_count): this rank's m
+    class counts (device u32 tensor).  Step 2 must use the same workspace."""
+    torch = _torch()
+    _require_cuda(d_in)
+    dc = make_discr(discr)
+    if counts is None:
+        counts = torch.empty(dc.m, dtype=torch.uint32, device=d_in.device)
+    _require_cuda(counts)
+    _check(lib().mdx_dist_count(ctypes.c_void_p(d_in.data_ptr()), d_in.numel(), _elem_of(d_in), dc,
+                                ctypes.c_void_p(counts.data_ptr()), ctypes.c_void_p(ws.ptr),
+                                ws.nbytes, _stream_ptr(stream)), "mdx_dist_count")
+    return counts
+
+
+def dist_scatter(d_in, discr, all_counts, rank: int, out_chunk_ptrs, out_chunk: int, n_total: int,
+                 ws: Workspace, sizes=None, stream=None):
+    """Step 3 of the distributed partition (mdx_dist_scatter): store this
+    rank's elements into the output chunks of every rank.  ``all_counts`` is
+    the [R, m] device u32 tensor of every rank's counts, ``out_chunk_ptrs``
+    the R device addresses (ints) of the output chunks.  Returns the global
+    class sizes (device u32 tensor)."""
+    torch = _torch()
+    _require_cuda(d_in, all_counts)
+    dc = make_discr(discr)
+    R = len(out_chunk_ptrs)
+    if sizes is None:
+        sizes = torch.empty(dc.m, dtype=torch.uint32, device=d_in.device)
+    ptrs = (ctypes.c_void_p * R)(*[ctypes.c_void_p(int(p)) for p in out_chunk_ptrs])
+    _check(lib().mdx_dist_scatter(ctypes.c_void_p(d_in.data_ptr()), d_in.numel(), _elem_of(d_in),
+                                  dc, ctypes.c_void_p(all_counts.data_ptr()), R, int(rank),
+                                  ptrs, int(out_chunk), int(n_total),
+                                  ctypes.c_void_p(sizes.data_ptr()), ctypes.c_void_p(ws.ptr),
+                                  ws.nbytes, _stream_ptr(stream)), "mdx_dist_scatter")
+    return sizes
+
+
+def ipc_handle(t) -> Tuple[bytes, int]:
+    """(64-byte CUDA IPC handle of the allocation holding tensor t, t's offset in it)."""
+    buf = ctypes.create_string_buffer(64)
+    off = ctypes.c_uint64(0)
+    _check(lib().mdx_ipc_get_handle(ctypes.c_void_p(t.data_ptr()), buf, ctypes.byref(off)),
+           "mdx_ipc_get_handle")
+    return buf.raw, int(off.value)
+
+
+def ipc_open(handle: bytes, offset: int) -> int:
+    """Map another process's allocation; the device address at `offset` in it."""
+    p = ctypes.c_void_p(0)
+    _check(lib().mdx_ipc_open(handle, int(offset), ctypes.byref(p)), "mdx_ipc_open")
+    return int(p.value)
+
+
+def ipc_close(ptr: int, offset: int) -> None:
+    _check(lib().mdx_ipc_close(ctypes.c_void_p(int(ptr)), int(offset)), "mdx_ipc_close")
 
 
 def mdiscr(d_in, discr, d_out=None, num_hwd_thds: int = 1 << 16, ws: Optional[Workspace] = None,

@@ -5,6 +5,10 @@
 // is a run-time parameter of the functor).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
 #include "mdx_host.cuh"
 
 
@@ -37,6 +41,7 @@ mdx_status mdx_workspace_error(void* d_ws, mdx_stream_t stream) {
     if (err != 0 && cudaMemset(d_err, 0, sizeof(err)) != cudaSuccess) return MDX_ERR_CUDA;
     if (err & kErrTimeout) return MDX_ERR_TIMEOUT;
     if (err & kErrSegments) return MDX_ERR_SEGMENTS;
+    if (err & kErrCounts) return MDX_ERR_INVALID;
     return MDX_OK;
 }
 
@@ -76,6 +81,138 @@ mdx_status mdx_partition(const void* d_in, void* d_out, uint64_t n, mdx_elem ele
                          size_t ws_bytes, mdx_stream_t stream) {
     return mdx_partition_timed(d_in, d_out, n, elem, discr, d_sizes, d_headflags, d_ws, ws_bytes,
                                stream, nullptr);
+}
+
+mdx_status mdx_dist_count(const void* d_in, uint64_t n_local, mdx_elem elem, mdx_discr discr,
+                          uint32_t* d_counts, void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
+    mdx_status s = check_elem(elem);
+    if (s != MDX_OK) return s;
+    if ((s = check_discr(discr)) != MDX_OK) return s;
+    if (discr.m > 16) return MDX_ERR_UNSUPPORTED;
+    if (n_local > MDX_MAX_ELEMS || d_counts == nullptr) return MDX_ERR_INVALID;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (n_local == 0)
+        return cudaMemsetAsync(d_counts, 0, discr.m * sizeof(uint32_t), st) == cudaSuccess
+                   ? MDX_OK
+                   : MDX_ERR_CUDA;
+    if (d_in == nullptr || reinterpret_cast<uintptr_t>(d_in) % elem_bytes(elem)) return MDX_ERR_INVALID;
+    const PlainLayout L = plain_layout(n_local, elem, discr.m);
+    if (d_ws == nullptr || ws_bytes < L.total) return MDX_ERR_WORKSPACE;
+    if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
+    unsigned char* ws = static_cast<unsigned char*>(d_ws);
+    if (elem == MDX_ELEM_U32)
+        return dispatch_plain<uint32_t>(d_in, nullptr, n_local, discr, d_counts, nullptr, ws, L, st,
+                                        nullptr, PlainStep::kCount);
+    return dispatch_plain<uint64_t>(d_in, nullptr, n_local, discr, d_counts, nullptr, ws, L, st,
+                                    nullptr, PlainStep::kCount);
+}
+
+mdx_status mdx_dist_scatter(const void* d_in, uint64_t n_local, mdx_elem elem, mdx_discr discr,
+                            const uint32_t* d_all_counts, uint32_t num_ranks, uint32_t rank,
+                            void* const* out_chunks, uint64_t out_chunk, uint64_t n_total,
+                            uint32_t* d_sizes, void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
+    mdx_status s = check_elem(elem);
+    if (s != MDX_OK) return s;
+    if ((s = check_discr(discr)) != MDX_OK) return s;
+    if (discr.m > 16) return MDX_ERR_UNSUPPORTED;
+    if (num_ranks == 0 || num_ranks > static_cast<uint32_t>(kMaxRanks) || rank >= num_ranks ||
+        d_all_counts == nullptr || out_chunks == nullptr)
+        return MDX_ERR_INVALID;
+    const uint64_t w = elem_bytes(elem);
+    if (n_total > MDX_MAX_ELEMS || n_local > n_total || out_chunk == 0 ||
+        out_chunk % (16 / w) != 0 || out_chunk > MDX_MAX_ELEMS)
+        return MDX_ERR_INVALID;
+    // chunk q: [q * out_chunk, (q + 1) * out_chunk) within [0, n_total); the
+    // last chunk: everything from (R - 1) * out_chunk on
+    auto chunk_len = [&](uint32_t q) -> uint64_t {
+        const uint64_t a = static_cast<uint64_t>(q) * out_chunk;
+        if (a >= n_total) return 0;
+        return q + 1 < num_ranks ? std::min<uint64_t>(out_chunk, n_total - a) : n_total - a;
+    };
+    DistOut dist;
+    dist.all_counts = d_all_counts;
+    dist.R = num_ranks;
+    dist.rank = rank;
+    dist.n_total = n_total;
+    dist.chunk = out_chunk;
+    for (uint32_t q = 0; q < num_ranks; q++) {
+        if (chunk_len(q) > 0 &&
+            (out_chunks[q] == nullptr || reinterpret_cast<uintptr_t>(out_chunks[q]) % 16))
+            return MDX_ERR_INVALID;
+        dist.chunks[q] = out_chunks[q];
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (d_ws == nullptr || reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
+    unsigned char* ws = static_cast<unsigned char*>(d_ws);
+    if (n_local == 0) {  // nothing to send; still check the counts and give the sizes
+        if (ws_bytes < kHeaderBytes) return MDX_ERR_WORKSPACE;
+        uint32_t* skip = reinterpret_cast<uint32_t*>(ws + kDistSkipOffset);
+        uint32_t* err = &reinterpret_cast<WsHeader*>(ws)->error;
+        switch (class_bound(discr.m)) {
+            case 2: plain_dist_bases_kernel<2><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
+            case 4: plain_dist_bases_kernel<4><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
+            case 8: plain_dist_bases_kernel<8><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
+            default: plain_dist_bases_kernel<16><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
+        }
+        return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+    }
+    if (d_in == nullptr || reinterpret_cast<uintptr_t>(d_in) % w) return MDX_ERR_INVALID;
+    {  // the input must not overlap this rank's own output chunk
+        const uint64_t own = chunk_len(rank);
+        const char* ib = static_cast<const char*>(d_in);
+        const char* ob = static_cast<const char*>(out_chunks[rank]);
+        if (own > 0 && ib < ob + own * w && ob < ib + n_local * w) return MDX_ERR_INVALID;
+    }
+    const PlainLayout L = plain_layout(n_local, elem, discr.m);
+    if (ws_bytes < L.total) return MDX_ERR_WORKSPACE;
+    if (elem == MDX_ELEM_U32)
+        return dispatch_plain<uint32_t>(d_in, nullptr, n_local, discr, d_sizes, nullptr, ws, L, st,
+                                        nullptr, PlainStep::kScatter, &dist);
+    return dispatch_plain<uint64_t>(d_in, nullptr, n_local, discr, d_sizes, nullptr, ws, L, st,
+                                    nullptr, PlainStep::kScatter, &dist);
+}
+
+mdx_status mdx_ipc_get_handle(const void* d_ptr, void* handle, uint64_t* offset) {
+    if (d_ptr == nullptr || handle == nullptr || offset == nullptr) return MDX_ERR_INVALID;
+    using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+    static RangeFn range = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &p, 12000, cudaEnableDefault,
+                                             &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            range = reinterpret_cast<RangeFn>(p);
+    });
+    if (range == nullptr) return MDX_ERR_UNSUPPORTED;
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (range(&base, &size, reinterpret_cast<CUdeviceptr>(d_ptr)) != CUDA_SUCCESS)
+        return MDX_ERR_INVALID;
+    cudaIpcMemHandle_t h;
+    if (cudaIpcGetMemHandle(&h, reinterpret_cast<void*>(base)) != cudaSuccess) return MDX_ERR_CUDA;
+    std::memcpy(handle, &h, sizeof(h));
+    *offset = reinterpret_cast<CUdeviceptr>(d_ptr) - base;
+    return MDX_OK;
+}
+
+mdx_status mdx_ipc_open(const void* handle, uint64_t offset, void** d_ptr) {
+    if (handle == nullptr || d_ptr == nullptr) return MDX_ERR_INVALID;
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle, sizeof(h));
+    void* p = nullptr;
+    if (cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    *d_ptr = static_cast<unsigned char*>(p) + offset;
+    return MDX_OK;
+}
+
+mdx_status mdx_ipc_close(void* d_ptr, uint64_t offset) {
+    if (d_ptr == nullptr) return MDX_ERR_INVALID;
+    return cudaIpcCloseMemHandle(static_cast<unsigned char*>(d_ptr) - offset) == cudaSuccess
+               ? MDX_OK
+               : MDX_ERR_CUDA;
 }
 
 mdx_status mdx_mdiscr(uint32_t n, uint32_t num_hwd_thds, const void* d_in, void* d_out,

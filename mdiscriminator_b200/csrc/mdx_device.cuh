@@ -17,6 +17,7 @@ constexpr uint64_t kWaitLimitNs = 1000ull * 1000ull * 1000ull;  // 1 s
 // Error bits latched in the workspace header.
 constexpr uint32_t kErrTimeout = 1u;
 constexpr uint32_t kErrSegments = 2u;
+constexpr uint32_t kErrCounts = 4u;  // distributed: other ranks' class counts inconsistent
 
 // ----------------------------------------------------------- discriminators --
 // The reference's functor concept (HelpersCommon.h:587-596, 840-849,

@@ -225,10 +225,28 @@ inline Tuning tuning_for(mdx_elem e, uint32_t M, uint64_t n) {
     return tt.t[e == MDX_ELEM_REC8 ? 1 : 0][bound_index(M)][log2_ceil(n)];
 }
 
+// Steps of a plain call: both kernels, or (distributed partition) the count
+// alone and later the scatter alone into a sharded output.
+enum class PlainStep { kBoth, kCount, kScatter };
+
+// Sharded output of a distributed partition (kScatter).
+struct DistOut {
+    const uint32_t* all_counts;  // [R][m] class counts of every rank (device)
+    uint32_t R, rank;
+    uint64_t n_total;            // elements over all ranks
+    void* chunks[kMaxRanks];     // output chunk of each rank (device pointers, peers' included)
+    uint64_t chunk;              // elements per chunk (the last chunk: the rest)
+};
+// Set by plain_dist_bases_kernel when the counts are inconsistent.
+constexpr size_t kDistSkipOffset = 196;
+static_assert(kDistSkipOffset >= kPlainDoneOffset + 4 && kDistSkipOffset + 4 <= kHeaderBytes,
+              "skip word inside the header, clear of the plain ticket");
+
 template <class V, class D, int M>
 mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
                      uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
-                     cudaStream_t stream, cudaEvent_t ev_mid) {
+                     cudaStream_t stream, cudaEvent_t ev_mid, PlainStep step = PlainStep::kBoth,
+                     const DistOut* dist = nullptr) {
     constexpr int ITEMS = ElemCfg<V>::kItems;
     constexpr int TILE = kThreads * ITEMS;
     auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
@@ -269,19 +287,43 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.error = &reinterpret_cast<WsHeader*>(ws)->error;
     a.m = m;
     a.use_tma = 0;
-    // head flags: all zero but for count_c at offset_c, which the last
-    // counting CTA writes
-    if (d_headflags != nullptr &&
-        cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    count<<<G, kThreads, 0, stream>>>(a, d);
-    if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
+    a.skip = nullptr;
+    if (step != PlainStep::kScatter) {
+        // head flags: all zero but for count_c at offset_c, which the last
+        // counting CTA writes
+        if (d_headflags != nullptr &&
+            cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess)
+            return MDX_ERR_CUDA;
+        count<<<G, kThreads, 0, stream>>>(a, d);
+        if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
+    }
+    if (step == PlainStep::kCount) return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     if constexpr (M <= 16) {
         using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
         CUtensorMap map;
         a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
-        plain_scatter_tma_kernel<V, D, M, kThreads, kStages><<<G, kThreads, smem, stream>>>(a, d, map);
+        if (dist == nullptr) {
+            const OutFlat<V> o{static_cast<V*>(d_out),
+                               static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
+                                                     (16u / sizeof(V) - 1u))};
+            plain_scatter_tma_kernel<V, D, M, kThreads, kStages>
+                <<<G, kThreads, smem, stream>>>(a, d, map, o);
+        } else {
+            uint32_t* skip = reinterpret_cast<uint32_t*>(ws + kDistSkipOffset);
+            plain_dist_bases_kernel<M><<<1, 64, 0, stream>>>(
+                dist->all_counts, dist->R, dist->rank, m, dist->n_total, a.class_base, a.class_tot,
+                d_sizes, skip, a.error);
+            a.skip = skip;
+            OutSharded<V> o;
+            for (uint32_t q = 0; q < dist->R; q++) o.chunks[q] = static_cast<V*>(dist->chunks[q]);
+            for (uint32_t q = dist->R; q < static_cast<uint32_t>(kMaxRanks); q++) o.chunks[q] = nullptr;
+            o.chunk = static_cast<uint32_t>(dist->chunk);
+            o.R = dist->R;
+            plain_scatter_tma_kernel<V, D, M, kThreads, kStages, OutSharded<V>>
+                <<<G, kThreads, smem, stream>>>(a, d, map, o);
+        }
     } else {
+        if (dist != nullptr) return MDX_ERR_UNSUPPORTED;
         plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages><<<G, kThreads, smem, stream>>>(a, d);
     }
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
@@ -290,14 +332,14 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
 template <class V, class D>
 mdx_status dispatch_plain_m(const void* in, void* out, uint64_t n, D d, uint32_t m, uint32_t* sz,
                             uint32_t* hf, unsigned char* ws, const PlainLayout& L,
-                            cudaStream_t st, cudaEvent_t ev) {
+                            cudaStream_t st, cudaEvent_t ev, PlainStep step, const DistOut* dist) {
     switch (class_bound(m)) {
-        case 2: return run_plain<V, D, 2>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 4: return run_plain<V, D, 4>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 8: return run_plain<V, D, 8>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 16: return run_plain<V, D, 16>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 32: return run_plain<V, D, 32>(in, out, n, d, m, sz, hf, ws, L, st, ev);
-        case 64: return run_plain<V, D, 64>(in, out, n, d, m, sz, hf, ws, L, st, ev);
+        case 2: return run_plain<V, D, 2>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
+        case 4: return run_plain<V, D, 4>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
+        case 8: return run_plain<V, D, 8>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
+        case 16: return run_plain<V, D, 16>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
+        case 32: return run_plain<V, D, 32>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
+        case 64: return run_plain<V, D, 64>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
         default: return MDX_ERR_INVALID;
     }
 }
@@ -309,10 +351,13 @@ inline bool use_mask(mdx_discr dc) { return dc.kind == MDX_DISCR_MASK || is_pow2
 template <class V>
 mdx_status dispatch_plain(const void* in, void* out, uint64_t n, mdx_discr dc, uint32_t* sz,
                           uint32_t* hf, unsigned char* ws, const PlainLayout& L, cudaStream_t st,
-                          cudaEvent_t ev) {
+                          cudaEvent_t ev, PlainStep step = PlainStep::kBoth,
+                          const DistOut* dist = nullptr) {
     if (use_mask(dc))
-        return dispatch_plain_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, sz, hf, ws, L, st, ev);
-    return dispatch_plain_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, sz, hf, ws, L, st, ev);
+        return dispatch_plain_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, sz, hf, ws, L, st, ev,
+                                   step, dist);
+    return dispatch_plain_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, sz, hf, ws, L, st, ev, step,
+                               dist);
 }
 
 // ------------------------------------------------------------- segmented --

@@ -197,10 +197,14 @@ mdx_status run(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint3
     a.done = reinterpret_cast<uint32_t*>(ws);
     a.error = reinterpret_cast<uint32_t*>(ws) + 1;
     a.m = m;
+    a.skip = nullptr;
     CUtensorMap map;
     a.use_tma = row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
+    const OutFlat<V> o{static_cast<V*>(d_out),
+                       static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
+                                             (16u / sizeof(V) - 1u))};
     count<<<G, kThreadsN, 0, st>>>(a, d);
-    scatter<<<G, kThreadsN, SL::kBytes, st>>>(a, d, map);
+    scatter<<<G, kThreadsN, SL::kBytes, st>>>(a, d, map, o);
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
 }
 

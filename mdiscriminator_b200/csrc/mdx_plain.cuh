@@ -36,6 +36,8 @@
 
 #include <cuda.h>  // CUtensorMap (type only; maps are encoded by the host)
 
+#include <type_traits>
+
 #include "mdx_device.cuh"
 #include "mdx_tile.cuh"
 
@@ -57,6 +59,7 @@ struct PlainArgs {
     uint32_t* error;      // latched error bits
     uint32_t m;
     int use_tma;          // the tensor map passed to the scatter kernel is valid
+    const uint32_t* skip; // scatter: return at once if *skip != 0 (null: never)
 };
 
 // Chunk k covers tiles [k*T/G, (k+1)*T/G).
@@ -423,14 +426,14 @@ struct ScatterTmaSmem {
 // (mdx_tile.cuh): thread-local nibble ranks, a block scan over the
 // [class][thread] count matrix, a shared-memory stage at the destination's
 // 16-byte phase and bulk stores of every class run.
-template <class V, class D, int M, int THREADS, int STAGES>
+template <class V, class D, int M, int THREADS, int STAGES, class OUT = OutFlat<V>>
 __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 64 registers
-    plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
+    plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap,
+                             const __grid_constant__ OUT out) {
     using L = ScatterTmaSmem<V, THREADS, STAGES, M>;
     constexpr int ITEMS = L::kItems;
     constexpr int TILE = L::kTile;
     constexpr int ROWS = L::kRows;
-    constexpr uint32_t AU = L::G::kAU;
     static_assert(ROWS <= 256, "TMA box height");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -450,10 +453,10 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     const uint32_t cnt = t1 - t0;
     if (cnt == 0) return;
     const V* in = static_cast<const V*>(a.in);
-    V* out = static_cast<V*>(a.out);
-    const uint32_t out_phase =
-        static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
     const bool tma_ok = a.use_tma != 0;
+    // sharded output: the class bases came from other ranks' counts; a
+    // mismatch found by plain_dist_bases_kernel leaves everything unwritten
+    if (a.skip != nullptr && *a.skip != 0u) return;
 
     if (tid < M)
         sh.cursor[0][tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
@@ -497,7 +500,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
             for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
         }
         const bool done = tile_scatter<V, D, M, THREADS, false>(
-            d, v, 0u, valid, full, stage, cnt_sm, sh, i & 1u, out, out_phase, ok, [&] {
+            d, v, 0u, valid, full, stage, cnt_sm, sh, i & 1u, out, ok, [&] {
                 // the ring slot is consumed (values are in registers): refill it
                 if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
             });
@@ -511,6 +514,59 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         }
     }
     if (tid < M) bulk_wait_all();
+    if constexpr (!std::is_same<OUT, OutFlat<V>>::value) {
+        // writes into other GPUs' memory: make them visible system-wide
+        // before the kernel ends
+        __threadfence_system();
+    }
+}
+
+// Sharded output (distributed partition): this rank's class bases in the
+// whole output from the class counts of all ranks, all_counts[r * m + c]:
+// base_c = (elements of classes < c on every rank) + (elements of class c on
+// ranks < rank).  The counts of this rank must equal its own count (class_tot,
+// from plain_count_kernel; null: a rank without elements, all zero) and all
+// counts must add up to n_total; otherwise *skip = 1, the error is latched and
+// the scatter writes nothing.  class_base may be null (no elements to place).
+template <int M>
+__global__ void plain_dist_bases_kernel(const uint32_t* all_counts, uint32_t R, uint32_t rank,
+                                        uint32_t m, uint64_t n_total, uint32_t* class_base,
+                                        const uint32_t* class_tot, uint32_t* sizes, uint32_t* skip,
+                                        uint32_t* error) {
+    __shared__ uint64_t tot[M];
+    __shared__ uint32_t bad;
+    const uint32_t c = threadIdx.x;
+    if (c == 0) bad = 0u;
+    __syncthreads();
+    uint64_t below = 0;
+    if (c < static_cast<uint32_t>(M)) {
+        uint64_t t = 0;
+        for (uint32_t r = 0; r < R; r++) {
+            const uint32_t x = c < m ? all_counts[static_cast<uint64_t>(r) * m + c] : 0u;
+            t += x;
+            if (r < rank) below += x;
+            const uint32_t own = (c < m && class_tot != nullptr) ? class_tot[c] : 0u;
+            if (r == rank && x != own) atomicOr(&bad, 1u);
+        }
+        tot[c] = t;
+    }
+    __syncthreads();
+    if (c == 0) {
+        uint64_t sum = 0;
+        for (int q = 0; q < M; q++) sum += tot[q];
+        if (sum != n_total) bad = 1u;
+    }
+    __syncthreads();
+    if (c < static_cast<uint32_t>(M)) {
+        uint64_t base = below;
+        for (uint32_t q = 0; q < c; q++) base += tot[q];
+        if (class_base != nullptr) class_base[c] = static_cast<uint32_t>(base);
+        if (sizes != nullptr && c < m) sizes[c] = static_cast<uint32_t>(tot[c]);
+    }
+    if (c == 0) {
+        *skip = bad;
+        if (bad) atomicOr(error, kErrCounts);
+    }
 }
 
 }  // namespace mdx

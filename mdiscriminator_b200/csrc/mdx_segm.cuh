@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(THREADS, 3)
                     v[q] = (e0 + q >= lo && e0 + q < hi) ? in[ts + e0 + q] : V();
             }
             const bool done = tile_scatter<V, D, M, THREADS, true>(
-                dj, v, lo, hi, full, stage, cnt_sm, sh, i & 1u, out, out_phase, ok, [&] {
+                dj, v, lo, hi, full, stage, cnt_sm, sh, i & 1u, OutFlat<V>{out, out_phase}, ok, [&] {
                     if (tid == 0 && i + STAGES < ntiles) issue(i + STAGES);
                 });
             if (!done) {

@@ -82,6 +82,47 @@ struct TileShared {
     uint32_t run_start[M], run_cnt[M], run_dst[M], rowtot[M];
 };
 
+// Where a tile's class runs go.  `idx` is an element's position in the whole
+// output (< 2^32).
+//
+// OutFlat: one array.  phase = (out / sizeof(V)) mod (16 / sizeof(V)).
+template <class V>
+struct OutFlat {
+    V* out;
+    uint32_t phase_;
+    __device__ __forceinline__ uint32_t phase() const { return phase_; }
+    __device__ __forceinline__ V* at(uint32_t idx) const { return out + idx; }
+    // End of the piece [idx, end) that lies in one buffer.
+    __device__ __forceinline__ uint32_t piece_end(uint32_t, uint32_t end) const { return end; }
+};
+
+// OutSharded: the output is cut into R chunks that live in different buffers
+// (one per rank, typically on other GPUs, reached through peer mappings):
+// chunk q holds positions [q * chunk, (q + 1) * chunk) (trailing chunks may
+// be short or empty), the last chunk everything from (R - 1) * chunk on.
+// Every chunk pointer is 16-byte aligned and `chunk` is a multiple of
+// 16 / sizeof(V) elements, so a position's 16-byte phase is the same in every
+// chunk and a run that crosses a chunk boundary splits into pieces that each
+// stay bulk-store aligned.
+constexpr int kMaxRanks = 128;
+template <class V>
+struct OutSharded {
+    V* chunks[kMaxRanks];
+    uint32_t chunk;
+    uint32_t R;
+    __device__ __forceinline__ uint32_t phase() const { return 0u; }
+    __device__ __forceinline__ V* at(uint32_t idx) const {
+        const uint32_t q = min(idx / chunk, R - 1u);
+        return chunks[q] + (idx - q * chunk);
+    }
+    __device__ __forceinline__ uint32_t piece_end(uint32_t idx, uint32_t end) const {
+        const uint32_t q = idx / chunk;
+        if (q + 1u >= R) return end;
+        const uint64_t b = static_cast<uint64_t>(q + 1u) * chunk;
+        return b < end ? static_cast<uint32_t>(b) : end;
+    }
+};
+
 // Take a thread's 64 bytes of a tile that TMA placed in shared memory with
 // the 128-byte swizzle (16-byte chunk q of 128-byte row r sits at chunk
 // q ^ (r & 7)).
@@ -104,12 +145,11 @@ __device__ __forceinline__ void take_swizzled(const V* tile, V (&v)[ITEMS]) {
 // `after_counts` runs right after the first barrier (the input ring slot is
 // consumed by then).  Returns false, having written nothing, when `ok` is
 // false on any thread.
-template <class V, class D, int M, int THREADS, bool FORWARD, class AfterCounts>
+template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts>
 __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeof(V)], uint32_t lo,
                                              uint32_t hi, bool full, V* stage, uint16_t* cnt_sm,
-                                             TileShared<M>& sh, uint32_t par, V* out,
-                                             uint32_t out_phase, bool ok,
-                                             AfterCounts after_counts) {
+                                             TileShared<M>& sh, uint32_t par, const OUT& out,
+                                             bool ok, AfterCounts after_counts) {
     using G = TileGeom<V, THREADS, M>;
     constexpr int ITEMS = G::kItems;
     constexpr uint32_t AU = G::kAU;
@@ -190,7 +230,7 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeo
         const uint32_t dst = FORWARD ? cur : cur - cc;
         const uint32_t room = cc + (cls ? AU : 0u);
         const uint32_t q0 = warp_incl_scan(room) - room;
-        const uint32_t st = q0 + (((out_phase + dst) - q0) & (AU - 1u));
+        const uint32_t st = q0 + (((out.phase() + dst) - q0) & (AU - 1u));
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int row = warp + h * W;
@@ -243,7 +283,14 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeo
         uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
         if (head > cc) head = cc;
         const uint32_t body = ((cc - head) / AU) * AU;
-        if (body > 0) bulk_store_s2g(out + sh.run_dst[tid] + head, stage + s + head, body * sizeof(V));
+        uint32_t a0 = sh.run_dst[tid] + head, sl = s + head;
+        const uint32_t a1 = a0 + body;
+        while (a0 < a1) {  // one piece per destination buffer
+            const uint32_t b = out.piece_end(a0, a1);
+            bulk_store_s2g(out.at(a0), stage + sl, (b - a0) * sizeof(V));
+            sl += b - a0;
+            a0 = b;
+        }
         bulk_commit();
     } else if (tid >= 32 && tid < 32 + M * 2 * static_cast<int>(AU)) {
         const uint32_t c = (tid - 32) / (2 * AU), q = (tid - 32) % (2 * AU);
@@ -257,7 +304,7 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeo
         } else if (head + body + (q - AU) < cc) {
             off = head + body + (q - AU);
         }
-        if (off != 0xffffffffu) out[sh.run_dst[c] + off] = stage[s + off];
+        if (off != 0xffffffffu) *out.at(sh.run_dst[c] + off) = stage[s + off];
     }
     return true;
 }
