@@ -309,6 +309,14 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
             plain_scatter_tma_kernel<V, D, M, kThreads, kStages>
                 <<<G, kThreads, smem, stream>>>(a, d, map, o);
         } else {
+            // the sharded instantiation is a kernel of its own: give it the
+            // shared-memory attribute too (the grid stays the count's G, the
+            // chunks of both steps must match)
+            int b2 = 0, s2 = 0;
+            if (occupancy(reinterpret_cast<const void*>(
+                              plain_scatter_tma_kernel<V, D, M, kThreads, kStages, OutSharded<V>>),
+                          smem, &b2, &s2) != cudaSuccess)
+                return MDX_ERR_CUDA;
             uint32_t* skip = reinterpret_cast<uint32_t*>(ws + kDistSkipOffset);
             plain_dist_bases_kernel<M><<<1, 64, 0, stream>>>(
                 dist->all_counts, dist->R, dist->rank, m, dist->n_total, a.class_base, a.class_tot,
