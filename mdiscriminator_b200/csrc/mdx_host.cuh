@@ -252,14 +252,11 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
     const void* scatter_fn;
     size_t smem;
-    if constexpr (M <= 16) {
+    {
         using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
         static_assert(SL::kTile == TILE, "both kernels use the same tiles");
         scatter_fn = reinterpret_cast<const void*>(plain_scatter_tma_kernel<V, D, M, kThreads, kStages>);
         smem = SL::kBytes;
-    } else {
-        scatter_fn = reinterpret_cast<const void*>(plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages>);
-        smem = plain_scatter_smem<V, TILE, kStages>();
     }
     int blocks = 0, sms = 0;
     if (occupancy(scatter_fn, smem, &blocks, &sms) != cudaSuccess) return MDX_ERR_CUDA;
@@ -298,7 +295,7 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
     }
     if (step == PlainStep::kCount) return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
-    if constexpr (M <= 16) {
+    {
         using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
         CUtensorMap map;
         a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
@@ -330,9 +327,6 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
             plain_scatter_tma_kernel<V, D, M, kThreads, kStages, OutSharded<V>>
                 <<<G, kThreads, smem, stream>>>(a, d, map, o);
         }
-    } else {
-        if (dist != nullptr) return MDX_ERR_UNSUPPORTED;
-        plain_scatter_kernel<V, D, M, kThreads, ITEMS, kStages><<<G, kThreads, smem, stream>>>(a, d);
     }
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
 }

@@ -12,15 +12,15 @@
 //                        per-chunk counts into per-chunk class prefixes, the
 //                        class bases (exclusive scan of the totals, the
 //                        `offsets` of SeqMdiscr.h:34-38) and the class sizes.
-//   plain_scatter_tma_kernel (m <= 16) / plain_scatter_kernel (m <= 64)
-//                        re-read each element (4 B) and write it once (4 B):
-//                        per tile, element ranks (thread-local byte counters
-//                        and a block scan; or warp ranks from __match_any_sync
-//                        + __popc for more classes),
-//                        a block scan of the per-warp class counts, a
-//                        shared-memory staged scatter so every class run leaves
-//                        the SM as coalesced stores.  Tiles are staged into
-//                        shared memory by TMA bulk copies (cp.async.bulk, no
+//   plain_scatter_tma_kernel
+//                        re-reads each element (4 B) and writes it once (4 B):
+//                        per tile, element ranks (m <= 16: thread-local
+//                        nibble counters and a block scan, mdx_tile.cuh
+//                        tile_scatter; more classes: warp ranks from ballots
+//                        of the class bits + __popc, tile_scatter_wide), a
+//                        shared-memory staged scatter so every class run
+//                        leaves the SM as bulk stores.  Tiles are staged into
+//                        shared memory by TMA (cp.async.bulk.tensor, no
 //                        multicast) through an mbarrier ring.  Each CTA walks
 //                        its chunk from the end backwards, so the tiles the
 //                        count kernel read last are still in L2.
@@ -258,157 +258,6 @@ __global__ void __launch_bounds__(THREADS) plain_count_kernel(PlainArgs a, D d) 
     plain_finish_scan<M, THREADS>(a, tot_sh);
 }
 
-// Shared-memory bytes of plain_scatter_kernel's dynamic part.
-template <class V, int TILE, int STAGES>
-constexpr size_t plain_scatter_smem() {
-    return static_cast<size_t>(STAGES + 1) * TILE * sizeof(V) + TILE;  // ring + stage + class bytes
-}
-
-template <class V, class D, int M, int THREADS, int ITEMS, int STAGES>
-__global__ void __launch_bounds__(THREADS) plain_scatter_kernel(PlainArgs a, D d) {
-    constexpr int TILE = THREADS * ITEMS;
-    constexpr int W = THREADS / 32;
-    constexpr int WSPAN = 32 * ITEMS;  // elements per warp per tile
-    static_assert(WSPAN <= 65536, "warp-local ranks are packed in 16 bits");
-    static_assert(M <= 64 && M >= 2, "class bound");
-
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    V* ring = reinterpret_cast<V*>(smem_raw);       // STAGES tiles, filled by TMA
-    V* stage = ring + STAGES * TILE;                // one tile, class-sorted
-    uint8_t* stage_cls = reinterpret_cast<uint8_t*>(stage + TILE);
-
-    __shared__ __align__(8) uint64_t bars[STAGES];
-    __shared__ uint32_t whist[W][M];  // per-warp running class counts
-    __shared__ uint32_t wbase[W][M];  // tile-local start of warp w's class-c run
-    __shared__ uint32_t cursor[M];    // global end cursor of this chunk's class-c run
-    __shared__ uint32_t delta[M];     // dst = slot + delta[c] (mod 2^32)
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t G = a.num_chunks, k = blockIdx.x;
-    uint32_t t0, t1;
-    chunk_tiles(k, a.num_tiles, G, t0, t1);
-    const uint32_t cnt = t1 - t0;
-    if (cnt == 0) return;
-    const V* in = static_cast<const V*>(a.in);
-    V* out = static_cast<V*>(a.out);
-    const bool tma_ok = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
-
-    if (tid < M) cursor[tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
-    if (tid == 0) {
-#pragma unroll
-        for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-
-    // Issue the load of the i-th tile in processing order (tile t1-1-i) into
-    // ring slot i % STAGES.  Full tiles go by TMA; the partial last tile of
-    // the array (or any tile when `in` is not 16-byte aligned) is read by the
-    // threads straight from global memory, and the barrier is only arrived on
-    // so that its phase still advances once per use.
-    auto issue = [&](uint32_t i) {
-        const uint32_t tile = t1 - 1u - i;
-        const uint64_t ts = static_cast<uint64_t>(tile) * TILE;
-        uint64_t* bar = &bars[i % STAGES];
-        if (tma_ok && ts + TILE <= a.n) {
-            mbar_arrive_expect_tx(bar, TILE * sizeof(V));
-            bulk_load_g2s(ring + (i % STAGES) * TILE, in + ts, TILE * sizeof(V), bar);
-        } else {
-            mbar_arrive(bar);
-        }
-    };
-    if (tid == 0)
-        for (uint32_t i = 0; i < STAGES && i < cnt; i++) issue(i);
-
-    for (uint32_t i = 0; i < cnt; i++) {
-        const uint32_t tile = t1 - 1u - i;
-        const uint64_t ts = static_cast<uint64_t>(tile) * TILE;
-        const uint32_t valid = static_cast<uint32_t>(min(static_cast<uint64_t>(TILE), a.n - ts));
-        const bool from_ring = tma_ok && valid == TILE;
-        const V* src = ring + (i % STAGES) * TILE;
-        const bool ok = mbar_wait_bounded(&bars[i % STAGES], (i / STAGES) & 1u);
-
-        // ---- warp ranks: element (warp, j, lane) is tile slot warp*WSPAN + j*32 + lane
-        for (int c = lane; c < M; c += 32) whist[warp][c] = 0;
-        __syncwarp();
-        V vals[ITEMS];
-        uint32_t info[ITEMS];  // class << 16 | warp-local rank
-        const uint32_t lt = lanemask_lt();
-#pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            const uint32_t idx = warp * WSPAN + j * 32 + lane;
-            const bool live = idx < valid;
-            V v = V();
-            if (live) v = from_ring ? src[idx] : in[ts + idx];
-            const uint32_t c = live ? d(v) : static_cast<uint32_t>(M);
-            const uint32_t peers = __match_any_sync(0xffffffffu, c);
-            const uint32_t before = live ? whist[warp][c] : 0u;
-            const uint32_t rank = before + __popc(peers & lt);
-            __syncwarp();
-            if (live && (peers >> lane) == 1u) whist[warp][c] = rank + 1u;  // last lane of its class
-            __syncwarp();
-            vals[j] = v;
-            info[j] = (c << 16) | rank;
-        }
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicOr(a.error, kErrTimeout);
-            // drain: wait (bounded) for the copies this CTA still has in flight
-            for (uint32_t q = i + 1; q < cnt && q < i + STAGES; q++)
-                if (tid == 0) (void)mbar_wait_bounded(&bars[q % STAGES], (q / STAGES) & 1u);
-            return;
-        }
-
-        // ---- block scan: per class, over warps (wprefix) and over classes (tile start)
-        if (warp == 0) {
-            uint32_t carry = 0;
-#pragma unroll
-            for (int c0 = 0; c0 < M; c0 += 32) {
-                const int c = c0 + lane;
-                uint32_t tcnt = 0;
-                if (c < M) {
-#pragma unroll
-                    for (int w = 0; w < W; w++) {
-                        const uint32_t x = whist[w][c];
-                        wbase[w][c] = tcnt;
-                        tcnt += x;
-                    }
-                }
-                const uint32_t incl = warp_incl_scan(tcnt);
-                const uint32_t tstart = carry + incl - tcnt;
-                carry += __shfl_sync(0xffffffffu, incl, 31);
-                if (c < M) {
-                    const uint32_t cur = cursor[c] - tcnt;
-                    cursor[c] = cur;
-                    delta[c] = cur - tstart;
-#pragma unroll
-                    for (int w = 0; w < W; w++) wbase[w][c] += tstart;
-                }
-            }
-        }
-        __syncthreads();
-
-        // ---- scatter into the class-sorted stage
-#pragma unroll
-        for (int j = 0; j < ITEMS; j++) {
-            const uint32_t c = info[j] >> 16;
-            if (c < static_cast<uint32_t>(M)) {
-                const uint32_t slot = wbase[warp][c] + (info[j] & 0xffffu);
-                stage[slot] = vals[j];
-                stage_cls[slot] = static_cast<uint8_t>(c);
-            }
-        }
-        __syncthreads();
-        if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
-
-        // ---- coalesced write-out of the class runs
-        for (uint32_t slot = tid; slot < valid; slot += THREADS) {
-            const uint32_t c = stage_cls[slot];
-            const uint32_t dst = slot + delta[c];
-            out[dst] = stage[slot];
-        }
-    }
-}
-
 template <class V, int THREADS, int STAGES, int M>
 struct ScatterTmaSmem {
     using G = TileGeom<V, THREADS, M>;
@@ -420,12 +269,15 @@ struct ScatterTmaSmem {
     static constexpr size_t kBytes = 1024 + kRingBytes + G::kStageBytes + G::kCntBytes;
 };
 
-// Scatter kernel for m <= 16.  Same contract as plain_scatter_kernel; tiles
-// arrive by tensor TMA (one 2-D box of 128-byte rows per tile, 128-byte
-// swizzle, STAGES-deep mbarrier ring) and go through tile_scatter
-// (mdx_tile.cuh): thread-local nibble ranks, a block scan over the
-// [class][thread] count matrix, a shared-memory stage at the destination's
-// 16-byte phase and bulk stores of every class run.
+// Scatter kernel: CTA k re-reads chunk k (tiles in reverse order) and writes
+// every element at class_base[c] + chunk_pre[c][k] + its rank in the chunk.
+// Tiles arrive by tensor TMA (one 2-D box of 128-byte rows per tile, 128-byte
+// swizzle, STAGES-deep mbarrier ring) and go through tile_scatter (m <= 16:
+// thread-local nibble ranks, a block scan over the [class][thread] count
+// matrix) or tile_scatter_wide (17..64 classes: warp ranks from ballots),
+// then a shared-memory stage at the destination's 16-byte phase and bulk
+// stores of every class run (mdx_tile.cuh).  OUT: one output array, or the
+// output chunks of several ranks (distributed partition).
 template <class V, class D, int M, int THREADS, int STAGES, class OUT = OutFlat<V>>
 __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 64 registers
     plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap,
@@ -490,20 +342,36 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         const bool full = valid == TILE;
         const bool ok = mbar_wait_bounded(&bars[i % STAGES], (i / STAGES) & 1u);
         V v[ITEMS];
-        if (tma_ok && full) {
-            take_swizzled<V, ITEMS>(ring + (i % STAGES) * TILE, v);
-        } else if (full) {
+        // the ring slot is consumed (values are in registers): refill it
+        auto refill = [&] {
+            if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
+        };
+        bool done;
+        if constexpr (M <= 16) {  // thread-contiguous elements
+            if (tma_ok && full) {
+                take_swizzled<V, ITEMS>(ring + (i % STAGES) * TILE, v);
+            } else if (full) {
 #pragma unroll
-            for (int j = 0; j < ITEMS; j++) v[j] = in[ts + e0 + j];
-        } else {
+                for (int j = 0; j < ITEMS; j++) v[j] = in[ts + e0 + j];
+            } else {
 #pragma unroll
-            for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
+                for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
+            }
+            done = tile_scatter<V, D, M, THREADS, false>(d, v, 0u, valid, full, stage, cnt_sm, sh,
+                                                         i & 1u, out, ok, refill);
+        } else {  // striped elements (warp ranks)
+            const uint32_t w0 = static_cast<uint32_t>(tid >> 5) * 32u * ITEMS + (tid & 31);
+            if (tma_ok && full) {
+                take_striped_swizzled<V, ITEMS>(ring + (i % STAGES) * TILE, v);
+            } else {
+#pragma unroll
+                for (int j = 0; j < ITEMS; j++)
+                    v[j] = (w0 + j * 32u < valid) ? in[ts + w0 + j * 32u] : V();
+            }
+            done = tile_scatter_wide<V, D, M, THREADS, false>(
+                d, v, 0u, valid, full, stage, reinterpret_cast<uint32_t*>(cnt_sm), sh, i & 1u, out,
+                ok, refill);
         }
-        const bool done = tile_scatter<V, D, M, THREADS, false>(
-            d, v, 0u, valid, full, stage, cnt_sm, sh, i & 1u, out, ok, [&] {
-                // the ring slot is consumed (values are in registers): refill it
-                if (tid == 0 && i + STAGES < cnt) issue(i + STAGES);
-            });
         if (!done) {
             if (tid == 0) {
                 atomicOr(a.error, kErrTimeout);

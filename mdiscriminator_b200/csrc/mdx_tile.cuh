@@ -71,7 +71,10 @@ struct TileGeom {
     // every class run gets kAU slots of slack for its 16-byte phase
     static constexpr int kStageElems = kTile + static_cast<int>(kAU) * M;
     static constexpr size_t kStageBytes = static_cast<size_t>(kStageElems) * sizeof(V);
-    static constexpr size_t kCntBytes = static_cast<size_t>(M) * THREADS * 2;  // u16 counts
+    // m <= 16: [class][thread] u16 counts; more classes: [warp][class] u32
+    // counts, then stage bases (tile_scatter_wide)
+    static constexpr size_t kCntBytes = M <= 16 ? static_cast<size_t>(M) * THREADS * 2
+                                                : static_cast<size_t>(THREADS / 32) * M * 4;
     static_assert(kStageElems < 65536, "stage slots are kept in 16 bits");
 };
 
@@ -294,6 +297,186 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeo
         bulk_commit();
     } else if (tid >= 32 && tid < 32 + M * 2 * static_cast<int>(AU)) {
         const uint32_t c = (tid - 32) / (2 * AU), q = (tid - 32) % (2 * AU);
+        const uint32_t s = sh.run_start[c], cc = sh.run_cnt[c];
+        uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
+        if (head > cc) head = cc;
+        const uint32_t body = ((cc - head) / AU) * AU;
+        uint32_t off = 0xffffffffu;
+        if (q < AU) {
+            if (q < head) off = q;
+        } else if (head + body + (q - AU) < cc) {
+            off = head + body + (q - AU);
+        }
+        if (off != 0xffffffffu) *out.at(sh.run_dst[c] + off) = stage[s + off];
+    }
+    return true;
+}
+
+// ------------------------------------------------------------ 17..64 classes --
+// With more than 16 classes the per-thread nibble counters no longer fit in a
+// register pair, so ranks come from the warp instead (striped layout):
+//  * in round j lane l of warp w holds tile element w*32*ITEMS + j*32 + l, so
+//    (warp, round, lane) is input order;
+//  * the lanes of a round that share a class are found from log2(M) ballots
+//    of the class bits (peers = AND over bits of ballot or ~ballot), the rank
+//    in the round is popc(peers & lanemask_lt);
+//  * lane k keeps the warp's running count of class k (and k + 32 when M = 64)
+//    in a register, read by one shuffle per element and advanced by a popcount
+//    of the lanes of class k (the same AND over bits with k's own bits);
+//  * warp 0 turns the [warp][class] counts into class runs at the
+//    destination's 16-byte phase and stage bases per (warp, class); pass 2 and
+//    the write-out are those of tile_scatter.
+
+// A warp's striped elements of a tile that TMA placed in shared memory with
+// the 128-byte swizzle.
+template <class V, int ITEMS>
+__device__ __forceinline__ void take_striped_swizzled(const V* tile, V (&v)[ITEMS]) {
+    const unsigned char* tb = reinterpret_cast<const unsigned char*>(tile);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    constexpr uint32_t PER_ROW = 128 / sizeof(V);
+#pragma unroll
+    for (int j = 0; j < ITEMS; j++) {
+        const uint32_t e = warp * 32u * ITEMS + j * 32u + lane;
+        const uint32_t row = e / PER_ROW, col = (e % PER_ROW) * sizeof(V);
+        const uint32_t chunk = (col >> 4) ^ (row & 7u);
+        v[j] = *reinterpret_cast<const V*>(tb + row * 128u + chunk * 16u + (col & 15u));
+    }
+}
+
+template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts>
+__device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[64 / sizeof(V)],
+                                                  uint32_t lo, uint32_t hi, bool full, V* stage,
+                                                  uint32_t* wtab, TileShared<M>& sh, uint32_t par,
+                                                  const OUT& out, bool ok,
+                                                  AfterCounts after_counts) {
+    using G = TileGeom<V, THREADS, M>;
+    constexpr int ITEMS = G::kItems;
+    constexpr uint32_t AU = G::kAU;
+    constexpr int W = THREADS / 32;
+    constexpr int B = M == 32 ? 5 : 6;
+    static_assert(M == 32 || M == 64, "17..64 classes (class bound 32 or 64)");
+    static_assert(32 * ITEMS <= 512, "warp ranks < 512 fit the packed 16-bit slots");
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt = lanemask_lt();
+
+    // ---- pass 1: warp ranks.  Lane k builds the mask of the lanes holding
+    // class k (and k + 32): one LOP3 per class bit against its own bits; an
+    // element's peers are then lane (c mod 32)'s mask, fetched by a shuffle.
+    uint32_t inv[5];  // bit i of the lane id set: ballot as is, else its complement
+#pragma unroll
+    for (int i = 0; i < 5; i++) inv[i] = ((lane >> i) & 1) ? 0u : 0xffffffffu;
+    uint32_t runs = 0;       // warp's running count of class lane (low 16 bits), lane + 32 (high)
+    uint32_t rk[ITEMS / 2];  // ranks, two per word
+#pragma unroll
+    for (int q = 0; q < ITEMS / 2; q++) rk[q] = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; j++) {
+        const uint32_t e = static_cast<uint32_t>(warp) * 32u * ITEMS + j * 32u + lane;
+        const bool valid = full || (e >= lo && e < hi);
+        const uint32_t c = valid ? d(v[j]) : 0u;
+        uint32_t com = full ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int i = 0; i < 5; i++) com &= __ballot_sync(0xffffffffu, (c >> i) & 1u) ^ inv[i];
+        uint32_t peers, base;
+        const uint32_t x = __shfl_sync(0xffffffffu, runs, c & 31u);
+        if constexpr (B == 6) {
+            const uint32_t b5 = __ballot_sync(0xffffffffu, (c >> 5) & 1u);
+            const uint32_t com0 = com & ~b5, com1 = com & b5;
+            const uint32_t p0 = __shfl_sync(0xffffffffu, com0, c & 31u);
+            const uint32_t p1 = __shfl_sync(0xffffffffu, com1, c & 31u);
+            peers = (c >> 5) ? p1 : p0;
+            base = (c >> 5) ? (x >> 16) : (x & 0xffffu);
+            runs += static_cast<uint32_t>(__popc(com0)) | (static_cast<uint32_t>(__popc(com1)) << 16);
+        } else {
+            peers = __shfl_sync(0xffffffffu, com, c);
+            base = x;
+            runs += static_cast<uint32_t>(__popc(com));
+        }
+        const uint32_t r = base + __popc(peers & lt);
+        rk[j >> 1] |= (r & 0xffffu) << (16 * (j & 1));
+    }
+    wtab[warp * M + lane] = runs & 0xffffu;
+    if constexpr (M == 64) wtab[warp * M + lane + 32] = runs >> 16;
+    if (__syncthreads_or(!ok)) return false;  // (A)
+    after_counts();
+
+    // ---- class runs (warp 0, lane = classes lane and lane + 32): totals over
+    // warps, runs at the destination's 16-byte phase, stage base per (warp, class)
+    if (warp == 0) {
+        constexpr int KL = M / 32;
+        uint32_t st_prev = 0;  // end of the rooms of the classes scanned so far
+#pragma unroll
+        for (int h = 0; h < KL; h++) {
+            const uint32_t c = static_cast<uint32_t>(lane + 32 * h);
+            uint32_t pre[W];
+            uint32_t cc = 0;
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                pre[w] = cc;
+                cc += wtab[w * M + c];
+            }
+            const uint32_t cur = sh.cursor[par][c];
+            const uint32_t dst = FORWARD ? cur : cur - cc;
+            const uint32_t room = cc + AU;
+            const uint32_t incl = warp_incl_scan(room);
+            const uint32_t q0 = st_prev + incl - room;
+            st_prev += __shfl_sync(0xffffffffu, incl, 31);
+            const uint32_t st = q0 + (((out.phase() + dst) - q0) & (AU - 1u));
+#pragma unroll
+            for (int w = 0; w < W; w++) wtab[w * M + c] = st + pre[w];
+            sh.cursor[par ^ 1u][c] = FORWARD ? cur + cc : dst;
+            sh.run_start[c] = st;
+            sh.run_cnt[c] = cc;
+            sh.run_dst[c] = dst;
+        }
+    }
+    // the stage is about to be rewritten: the previous tile's bulk stores
+    // must have finished reading it
+    if (tid < M) bulk_wait_read<0>();
+    __syncthreads();  // (B)
+
+    // ---- pass 2: stage slot = base of (warp, class) + warp rank
+    const uint32_t sb0 = wtab[warp * M + lane];
+    uint32_t sb1 = 0u;
+    if constexpr (M == 64) sb1 = wtab[warp * M + lane + 32];
+#pragma unroll
+    for (int j = 0; j < ITEMS; j++) {
+        const uint32_t e = static_cast<uint32_t>(warp) * 32u * ITEMS + j * 32u + lane;
+        const bool valid = full || (e >= lo && e < hi);
+        const uint32_t c = valid ? d(v[j]) : 0u;
+        uint32_t sb;
+        if constexpr (M == 64) {
+            const uint32_t x0 = __shfl_sync(0xffffffffu, sb0, c & 31u);
+            const uint32_t x1 = __shfl_sync(0xffffffffu, sb1, c & 31u);
+            sb = (c >> 5) ? x1 : x0;
+        } else {
+            sb = __shfl_sync(0xffffffffu, sb0, c);
+        }
+        if (valid) stage[sb + ((rk[j >> 1] >> (16 * (j & 1))) & 0xffffu)] = v[j];
+    }
+    fence_proxy_async_smem();
+    __syncthreads();  // (C)
+
+    // ---- write-out: bulk store of each run's aligned interior; all threads
+    // store the unaligned heads and tails
+    if (tid < M) {
+        const uint32_t s = sh.run_start[tid], cc = sh.run_cnt[tid];
+        uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
+        if (head > cc) head = cc;
+        const uint32_t body = ((cc - head) / AU) * AU;
+        uint32_t a0 = sh.run_dst[tid] + head, sl = s + head;
+        const uint32_t a1 = a0 + body;
+        while (a0 < a1) {
+            const uint32_t b = out.piece_end(a0, a1);
+            bulk_store_s2g(out.at(a0), stage + sl, (b - a0) * sizeof(V));
+            sl += b - a0;
+            a0 = b;
+        }
+        bulk_commit();
+    }
+    for (int t = tid; t < M * 2 * static_cast<int>(AU); t += THREADS) {
+        const uint32_t c = static_cast<uint32_t>(t) / (2 * AU), q = static_cast<uint32_t>(t) % (2 * AU);
         const uint32_t s = sh.run_start[c], cc = sh.run_cnt[c];
         uint32_t head = (AU - (s & (AU - 1u))) & (AU - 1u);
         if (head > cc) head = cc;
