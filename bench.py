@@ -280,6 +280,21 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
                     "requests": k, "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
                     "gelem_per_s": elems / st["window_s"] / 1e9 if st["window_s"] > 0 else None,
                     "batches": st["batches"], "mean_request_elems": elems / k})
+    # capacity: every request of a closed batch submitted at once
+    reqs = make_requests(2000)
+    srv.reset_stats()
+    t0 = time.perf_counter()
+    tickets = [srv.submit(d_in, d_out, sz, m) for d_in, d_out, sz, m, _ in reqs]
+    for t in tickets:
+        srv.wait(t)
+    t_all = time.perf_counter() - t0
+    st = srv.stats()
+    elems = sum(r[4] for r in reqs)
+    saturated = {"requests": len(reqs), "gelem_per_s": elems / t_all / 1e9,
+                 "req_per_s": len(reqs) / t_all, "batches": st["batches"],
+                 "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
+                 "sample": "2000 requests of the same mix submitted at once (host wall clock "
+                           "from the first submit to the last completion)"}
     srv.close()
     # one plain launch per request, back to back, on the same request mix
     reqs = make_requests(400)
@@ -297,6 +312,7 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
     return {"workload": "served requests: Poisson arrivals, n log-uniform [2^10, 2^24] int32, "
                         "m uniform {2,4,8,16}, 16 GiB budget, device-resident request data",
             "loads": res,
+            "saturated": saturated,
             "per_request_plain": {"value": plain, "unit": "Gelem/s",
                                   "sample": "400 requests of the same mix, one mdx_partition each, "
                                             "back to back on one stream (host wall clock)"}}

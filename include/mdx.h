@@ -236,8 +236,7 @@ mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint64_t n, mdx_
  *      global m sizes go to d_sizes (device, may be NULL).  A barrier across
  *      ranks (any collective after this call on the same stream) must precede
  *      reading an output chunk.
- * m <= 16 (MDX_ERR_UNSUPPORTED otherwise); out_chunk a multiple of 16 bytes
- * of elements; chunk pointers 16-byte aligned; n_total < 2^32.  Counts that do
+ * m <= 64; out_chunk a multiple of 16 bytes of elements; chunk pointers 16-byte aligned; n_total < 2^32.  Counts that do
  * not match this rank's own count or do not add up to n_total make the
  * scatter write nothing and latch an error (mdx_workspace_error:
  * MDX_ERR_INVALID).

@@ -88,7 +88,6 @@ mdx_status mdx_dist_count(const void* d_in, uint64_t n_local, mdx_elem elem, mdx
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
     if ((s = check_discr(discr)) != MDX_OK) return s;
-    if (discr.m > 16) return MDX_ERR_UNSUPPORTED;
     if (n_local > MDX_MAX_ELEMS || d_counts == nullptr) return MDX_ERR_INVALID;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (n_local == 0)
@@ -114,7 +113,6 @@ mdx_status mdx_dist_scatter(const void* d_in, uint64_t n_local, mdx_elem elem, m
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
     if ((s = check_discr(discr)) != MDX_OK) return s;
-    if (discr.m > 16) return MDX_ERR_UNSUPPORTED;
     if (num_ranks == 0 || num_ranks > static_cast<uint32_t>(kMaxRanks) || rank >= num_ranks ||
         d_all_counts == nullptr || out_chunks == nullptr)
         return MDX_ERR_INVALID;
@@ -152,7 +150,9 @@ mdx_status mdx_dist_scatter(const void* d_in, uint64_t n_local, mdx_elem elem, m
             case 2: plain_dist_bases_kernel<2><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
             case 4: plain_dist_bases_kernel<4><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
             case 8: plain_dist_bases_kernel<8><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
-            default: plain_dist_bases_kernel<16><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
+            case 16: plain_dist_bases_kernel<16><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
+            case 32: plain_dist_bases_kernel<32><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
+            default: plain_dist_bases_kernel<64><<<1, 64, 0, st>>>(d_all_counts, num_ranks, rank, discr.m, n_total, nullptr, nullptr, d_sizes, skip, err); break;
         }
         return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     }

@@ -48,17 +48,47 @@ struct CopyJob {            // one request in a batch
     const uint32_t* sizes_src;  // scatter only: this segment's row of class sizes
     uint32_t* sizes_dst;        // scatter only: the request's m sizes
     uint32_t m;
+    uint32_t first_chunk;       // index of this job's first chunk in the launch
 };
 
-// blockIdx.y = request, blockIdx.x = chunk of kCopyChunk elements.
-__global__ void __launch_bounds__(kCopyThreads) copy_jobs(const CopyJob* jobs) {
-    const CopyJob j = jobs[blockIdx.y];
-    const uint64_t a = static_cast<uint64_t>(blockIdx.x) * kCopyChunk;
-    if (blockIdx.x == 0 && j.sizes_dst != nullptr && threadIdx.x < j.m)
+// One CTA per chunk of kCopyChunk elements over all the jobs of a launch
+// (jobs in order of first_chunk; every job has n >= 1).  8 independent loads
+// in flight per thread; accesses are coalesced 4-byte words, so the source
+// and destination need no common alignment.
+constexpr int kCopyUnroll = 8;
+__global__ void __launch_bounds__(kCopyThreads) copy_jobs(const CopyJob* jobs, uint32_t num_jobs) {
+    __shared__ uint32_t js;
+    const uint32_t bid = blockIdx.x;
+    if (threadIdx.x == 0) {  // the last job whose first chunk is <= bid
+        uint32_t lo = 0, hi = num_jobs;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (jobs[mid].first_chunk <= bid) lo = mid; else hi = mid;
+        }
+        js = lo;
+    }
+    __syncthreads();
+    const CopyJob j = jobs[js];
+    const uint64_t a = static_cast<uint64_t>(bid - j.first_chunk) * kCopyChunk;
+    if (a == 0 && j.sizes_dst != nullptr && threadIdx.x < j.m)
         j.sizes_dst[threadIdx.x] = j.sizes_src[threadIdx.x];
     if (a >= j.n) return;
-    const uint64_t b = min(a + kCopyChunk, j.n);
-    for (uint64_t e = a + threadIdx.x; e < b; e += kCopyThreads) j.dst[e] = j.src[e];
+    const uint32_t cnt = static_cast<uint32_t>(min(static_cast<uint64_t>(kCopyChunk), j.n - a));
+    const uint32_t* src = j.src + a;
+    uint32_t* dst = j.dst + a;
+    for (uint32_t base = 0; base < cnt; base += kCopyThreads * kCopyUnroll) {
+        uint32_t v[kCopyUnroll];
+#pragma unroll
+        for (int u = 0; u < kCopyUnroll; u++) {
+            const uint32_t e = base + u * kCopyThreads + threadIdx.x;
+            if (e < cnt) v[u] = __ldg(src + e);
+        }
+#pragma unroll
+        for (int u = 0; u < kCopyUnroll; u++) {
+            const uint32_t e = base + u * kCopyThreads + threadIdx.x;
+            if (e < cnt) dst[e] = v[u];
+        }
+    }
 }
 
 // The device-side address of a buffer, or null when kernels cannot reach it
@@ -214,20 +244,19 @@ mdx_status launch_batch(Server* s, Slot& sl, const std::vector<Req*>& batch) {
     const uint64_t base = batch.front()->off;
     const uint32_t S = static_cast<uint32_t>(batch.size());
     uint64_t acc = 0;
+    uint32_t chunks = 0;
     for (uint32_t i = 0; i < S; i++) {
         Req* r = batch[i];
         sl.h_offsets[i] = acc;
         sl.h_seg_m[i] = r->m;
-        sl.h_jobs[i] = CopyJob{r->in, s->d_in + r->off, r->n, nullptr, nullptr, 0};
+        sl.h_jobs[i] = CopyJob{r->in, s->d_in + r->off, r->n, nullptr, nullptr, 0, chunks};
         sl.h_jobs[S + i] = CopyJob{s->d_out + r->off, r->out, r->n,
                                    sl.d_seg_sizes + static_cast<uint64_t>(i) * s->cfg.m_max,
-                                   r->sizes, r->m};
+                                   r->sizes, r->m, chunks};
+        chunks += static_cast<uint32_t>((r->n + kCopyChunk - 1) / kCopyChunk);
         acc += r->n;
     }
     sl.h_offsets[S] = acc;
-    uint64_t max_n = 0;
-    for (Req* r : batch) max_n = std::max(max_n, r->n);
-    const uint32_t chunks = static_cast<uint32_t>((max_n + kCopyChunk - 1) / kCopyChunk);
     cudaStream_t st = sl.stream;
     if (cudaMemcpyAsync(sl.d_offsets, sl.h_offsets, sizeof(uint64_t) * (S + 1),
                         cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -236,13 +265,13 @@ mdx_status launch_batch(Server* s, Slot& sl, const std::vector<Req*>& batch) {
         cudaMemcpyAsync(sl.d_jobs, sl.h_jobs, sizeof(CopyJob) * 2 * S, cudaMemcpyHostToDevice, st) !=
             cudaSuccess)
         return MDX_ERR_CUDA;
-    copy_jobs<<<dim3(std::max(chunks, 1u), S), kCopyThreads, 0, st>>>(sl.d_jobs);
+    copy_jobs<<<chunks, kCopyThreads, 0, st>>>(sl.d_jobs, S);
     mdx_status r = mdx_partition_segmented_multi(
         s->d_in + base, s->d_out + base, acc, MDX_ELEM_U32, sl.d_seg_m, s->cfg.m_max,
         sl.d_offsets, S, sl.d_seg_sizes, nullptr, sl.ws, sl.ws_bytes,
         reinterpret_cast<mdx_stream_t>(st));
     if (r != MDX_OK) return r;
-    copy_jobs<<<dim3(std::max(chunks, 1u), S), kCopyThreads, 0, st>>>(sl.d_jobs + S);
+    copy_jobs<<<chunks, kCopyThreads, 0, st>>>(sl.d_jobs + S, S);
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
 }
 

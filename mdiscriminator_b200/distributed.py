@@ -157,7 +157,7 @@ def partition_distributed(x_local, discr, group=None, transport: str = "auto", o
     elif out.numel() != b - a or out.dtype != x_local.dtype:
         raise MdxError(MDX_ERR_INVALID, "partition_distributed: out has the wrong shape or type")
     if transport == "auto":
-        transport = "p2p" if (x_local.is_cuda and m <= 16) else "nccl"
+        transport = "p2p" if x_local.is_cuda else "nccl"
 
     if transport == "p2p":
         elem = ELEM_REC8 if ebytes == 8 else 0

@@ -131,7 +131,7 @@ def _emulate(torch, mdx, x, lens, discr, m, elem_dtype):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("R", [1, 2, 3, 4, 7])
-@pytest.mark.parametrize("m", [2, 5, 8, 16])
+@pytest.mark.parametrize("m", [2, 5, 8, 16, 40])
 def test_sharded_scatter_equals_global_partition(cuda_ready, R, m):
     torch = cuda_ready
     import mdiscriminator_b200 as mdx
