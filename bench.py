@@ -145,17 +145,25 @@ def lognormal_lengths(S: int, seed: int, mu: float, sigma: float, hi: int):
     return np.clip(np.rint(rng.lognormal(mu, sigma, size=S)), 1, hi).astype(np.int64)
 
 
-def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segments=2000):
+def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segments=2000,
+                        num_segments=100_000, keep="all", with_plain=True):
     """Batched segmented partition: 100,000 segments, lengths
     LogNormal(ln 1024, 1.5) clamped to [1, 2^22] (~3e8 int32), m = 4,
     class = v mod 4, as one segmented call replayed from a CUDA graph, against
     one plain partition per segment (a CUDA graph of per-segment calls over a
-    sample of consecutive segments)."""
+    sample of consecutive segments).  ``keep`` = "large" / "small" keeps only
+    the segments longer than / at most one 4096-element tile (for profiling the
+    two halves of the kernel)."""
     import math
 
     import numpy as np
-    S, m = 100_000, 4
-    lengths = lognormal_lengths(S, 2024, math.log(1024), 1.5, 1 << 22)
+    m = 4
+    lengths = lognormal_lengths(num_segments, 2024, math.log(1024), 1.5, 1 << 22)
+    if keep == "large":
+        lengths = lengths[lengths > 4096]
+    elif keep == "small":
+        lengths = lengths[lengths <= 4096]
+    S = len(lengths)
     offs = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)
     n = int(offs[-1])
     d_in = make_input(torch, n, 99, dev)
@@ -183,6 +191,17 @@ def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segmen
         raise SystemExit("device error in the batched measurement")
     t_b = e0.elapsed_time(e1) * 1e-3 / steps
     alg = 2 * n * 4 + 8 * (S + 1) + 4 * m * S
+    workload = (f"{S:,} segments, LogNormal(ln 1024, 1.5) clamped [1, 2^22]"
+                + ("" if keep == "all" else f" (only the {keep} ones of {num_segments:,})")
+                + ", int32, m=4, segment offsets, one segmented launch sequence replayed from a "
+                  "CUDA graph")
+    res = {"workload": workload, "n": n, "segments": S, "value": n / t_b / 1e9, "unit": "Gelem/s",
+           "ms": t_b * 1e3,
+           "roofline": {"bound": "hbm", "achieved": alg / t_b / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": alg / t_b / 1e9 / peak, "alg_bytes": "2*N*4 + 8*(S+1) + 4*m*S"}}
+    if not with_plain:
+        del g
+        return res
     # one plain launch per segment, on a sample of consecutive segments
     s0 = S // 2
     s1 = s0 + sample_segments
@@ -207,21 +226,13 @@ def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segmen
         e1.record(stream)
         stream.synchronize()
     t_p = e0.elapsed_time(e1) * 1e-3 / reps
-    v_b = n / t_b / 1e9
     v_p = (a1 - a0) / t_p / 1e9
     del g, gp
-    return {
-        "workload": "100,000 segments, LogNormal(ln 1024, 1.5) clamped [1, 2^22], int32, m=4, "
-                    "segment offsets, one segmented launch sequence replayed from a CUDA graph",
-        "n": n, "segments": S, "value": v_b, "unit": "Gelem/s", "ms": t_b * 1e3,
-        "roofline": {"bound": "hbm", "achieved": alg / t_b / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": alg / t_b / 1e9 / peak,
-                     "alg_bytes": "2*N*4 + 8*(S+1) + 4*m*S"},
-        "per_segment_plain": {"value": v_p, "unit": "Gelem/s",
-                              "sample": f"segments {s0}..{s1 - 1} ({a1 - a0} elements), one "
-                                        "mdx_partition per segment, CUDA graph of the calls"},
-        "speedup_vs_per_segment": v_b / v_p,
-    }
+    res["per_segment_plain"] = {"value": v_p, "unit": "Gelem/s",
+                                "sample": f"segments {s0}..{s1 - 1} ({a1 - a0} elements), one "
+                                          "mdx_partition per segment, CUDA graph of the calls"}
+    res["speedup_vs_per_segment"] = res["value"] / v_p
+    return res
 
 
 def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), duration_s=1.0):
@@ -391,6 +402,10 @@ def main():
                     help="skip the batched segmented measurement")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served-requests measurement")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched segmented measurement and print its JSON")
+    ap.add_argument("--batched-segments", type=int, default=100_000)
+    ap.add_argument("--batched-keep", default="all", choices=["all", "large", "small"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -411,6 +426,14 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
+
+    if args.batched_only:
+        peak, _ = peaks()
+        res = batched_measurement(torch, mdx, dev, peak, steps=args.steps, warmup=args.warmup,
+                                  num_segments=args.batched_segments, keep=args.batched_keep,
+                                  with_plain=False)
+        print(json.dumps(res))
+        return
 
     n, m = args.n, args.m
     discr = ("mask", m) if (m & (m - 1)) == 0 else ("mod", m)
