@@ -235,6 +235,32 @@ def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segmen
     return res
 
 
+def sort_measurement(torch, d_in, d_out, m, reps=3):
+    """The sort-based alternative on the same GPU and input (the reference's
+    SortTest.cu:130-154 uses thrust::stable_sort_by_key): a stable library
+    radix sort of the class keys (torch.sort, stable) and a gather of the
+    values by the sorted indices.  Library code, timed as a reference point;
+    its result is checked against mdx's."""
+    keys = d_in % m if (m & (m - 1)) else d_in & (m - 1)
+    _, idx = torch.sort(keys, stable=True)
+    same = bool(torch.equal(d_in[idx], d_out))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        k = d_in % m if (m & (m - 1)) else d_in & (m - 1)
+        _, idx = torch.sort(k, stable=True)
+        out = d_in[idx]
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del keys, idx, out
+    return {"value": d_in.numel() / ms / 1e6, "unit": "Gelem/s", "ms": ms,
+            "equal_to_mdx": same,
+            "what": "torch.sort(class keys, stable=True) + gather by the indices, same input, "
+                    "CUDA events (library code, reference point)"}
+
+
 def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), duration_s=1.0):
     """Served partition requests: open-loop Poisson arrivals at each offered
     load; lengths log-uniform over [2^10, 2^24], values uniform over [0, 2^31),
@@ -402,6 +428,8 @@ def main():
                     help="skip the batched segmented measurement")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served-requests measurement")
+    ap.add_argument("--no-sort", action="store_true",
+                    help="skip the sort-based reference point")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched segmented measurement and print its JSON")
     ap.add_argument("--batched-segments", type=int, default=100_000)
@@ -563,6 +591,9 @@ def main():
         batched = None
         if world == 1 and not args.no_batched:
             batched = batched_measurement(torch, mdx, dev, peak)
+        sort_ref = None
+        if world == 1 and not args.no_sort:
+            sort_ref = sort_measurement(torch, d_in, d_out, m)
         served = None
         if world == 1 and not args.no_served:
             served = served_measurement(torch, mdx, dev, peak)
@@ -586,6 +617,7 @@ def main():
             "cpu_baseline": cpu,
             "batched": batched,
             "served": served,
+            "sort_baseline": sort_ref,
             "clocks": clk,
             "gpu_launches": 2 * args.steps,
         }

@@ -285,6 +285,17 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.m = m;
     a.use_tma = 0;
     a.skip = nullptr;
+    if (m == 1 && step == PlainStep::kBoth) {  // one class: the partition is a copy
+        if ((d_headflags != nullptr &&
+             cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess) ||
+            cudaMemcpyAsync(d_out, d_in, n * sizeof(V), cudaMemcpyDeviceToDevice, stream) !=
+                cudaSuccess)
+            return MDX_ERR_CUDA;
+        plain_single_class_kernel<<<1, 32, 0, stream>>>(n, a.class_base, a.class_tot, d_sizes,
+                                                         d_headflags);
+        if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
+        return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+    }
     if (step != PlainStep::kScatter) {
         // head flags: all zero but for count_c at offset_c, which the last
         // counting CTA writes

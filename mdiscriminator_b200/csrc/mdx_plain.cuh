@@ -389,6 +389,19 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     }
 }
 
+// m = 1: every element is in class 0, the partition is a copy (made by the
+// host with cudaMemcpyAsync); this kernel fills in the class total and base,
+// the sizes and the head flag (count_0 at offset 0; the array was zeroed).
+static __global__ void plain_single_class_kernel(uint64_t n, uint32_t* class_base, uint32_t* class_tot,
+                                          uint32_t* sizes, uint32_t* headflags) {
+    if (threadIdx.x == 0) {
+        class_base[0] = 0u;
+        class_tot[0] = static_cast<uint32_t>(n);
+        if (sizes != nullptr) sizes[0] = static_cast<uint32_t>(n);
+        if (headflags != nullptr) headflags[0] = static_cast<uint32_t>(n);
+    }
+}
+
 // Sharded output (distributed partition): this rank's class bases in the
 // whole output from the class counts of all ranks, all_counts[r * m + c]:
 // base_c = (elements of classes < c on every rank) + (elements of class c on

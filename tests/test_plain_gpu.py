@@ -192,3 +192,16 @@ def test_full_size_records_permutation_proof(cuda_ready):
     same = cls[1:] == cls[:-1]
     assert bool((payload[1:][same] > payload[:-1][same]).all())
     assert torch.equal(okeys, keys[payload])
+
+
+def test_single_class_is_a_copy(cuda_ready):
+    """m = 1 takes the copy path: output = input, one class of size n, head
+    flag n at 0 -- for values and records, through both plain entry points."""
+    torch = cuda_ready
+    import mdiscriminator_b200 as mdx
+    for n in (1, 4097, 1 << 20):
+        check(torch, oracle.fill_uniform_u32(n, n), 1)
+        check(torch, records(n, n + 1), 1, "mod")
+        out, sizes = mdx.mdiscr(torch.from_numpy(oracle.fill_uniform_u32(n, 5)).cuda(), ("mod", 1))
+        assert list(sizes) == [n]
+        assert np.array_equal(out.cpu().numpy(), oracle.fill_uniform_u32(n, 5))
