@@ -81,35 +81,70 @@ __device__ __forceinline__ void unpack16<uint64_t>(const uint4& r, uint64_t (&e)
     e[1] = static_cast<uint64_t>(r.z) | (static_cast<uint64_t>(r.w) << 32);
 }
 
-// Per-thread class counters for M <= 16: 8-bit lanes packed in u64 words,
-// flushed into u32 accumulators before any lane can reach 256.
+// 1 << s with the shift clamped as PTX defines it (s >= 32 gives 0), so one
+// increment is added to the right 32-bit word without a select.
+__device__ __forceinline__ uint32_t shl1_clamped(uint32_t s) {
+    uint32_t r;
+    asm("shl.b32 %0, 1, %1;" : "=r"(r) : "r"(s));
+    return r;
+}
+
+// Per-thread class counters for M <= 16: 4-bit lanes in one or two u32 words
+// (an increment is one shift and one add per word), folded into 8-bit lanes
+// (even / odd classes of each nibble word) at least every 8 increments and
+// into u32 totals at least every 31 folds, before any lane can overflow.
 template <int M>
 struct PackedCounts {
     static_assert(M <= 16, "packed counters cover at most 16 classes");
     static constexpr int NW = (M + 7) / 8;
-    uint64_t pk[NW];
+    uint32_t nib[NW];
+    uint32_t byt[2 * NW];
     uint32_t acc[M];
+    uint32_t folds;
     __device__ __forceinline__ void init() {
 #pragma unroll
-        for (int w = 0; w < NW; w++) pk[w] = 0;
+        for (int w = 0; w < NW; w++) nib[w] = 0;
+#pragma unroll
+        for (int w = 0; w < 2 * NW; w++) byt[w] = 0;
 #pragma unroll
         for (int c = 0; c < M; c++) acc[c] = 0;
+        folds = 0;
     }
+    // At most 8 calls between fold() calls.
     __device__ __forceinline__ void add(uint32_t c) {
         if constexpr (NW == 1) {
-            pk[0] += 1ull << (c << 3);
+            nib[0] += 1u << (c << 2);
         } else {
-            const uint64_t inc = 1ull << ((c & 7u) << 3);
-            pk[0] += (c < 8u) ? inc : 0ull;
-            pk[1] += (c < 8u) ? 0ull : inc;
+            const uint32_t s = c << 2;
+            nib[0] += shl1_clamped(s);
+            nib[1] += shl1_clamped(s - 32u);
         }
     }
-    __device__ __forceinline__ void flush() {
+    __device__ __forceinline__ void flush() {  // bytes -> u32 totals
 #pragma unroll
-        for (int c = 0; c < M; c++)
-            acc[c] += static_cast<uint32_t>(pk[c >> 3] >> ((c & 7) * 8)) & 0xffu;
+        for (int w = 0; w < NW; w++) {
 #pragma unroll
-        for (int w = 0; w < NW; w++) pk[w] = 0;
+            for (int j = 0; j < 4; j++) {
+                if (8 * w + 2 * j < M) acc[8 * w + 2 * j] += (byt[2 * w] >> (8 * j)) & 0xffu;
+                if (8 * w + 2 * j + 1 < M) acc[8 * w + 2 * j + 1] += (byt[2 * w + 1] >> (8 * j)) & 0xffu;
+            }
+            byt[2 * w] = 0;
+            byt[2 * w + 1] = 0;
+        }
+        folds = 0;
+    }
+    __device__ __forceinline__ void fold() {  // nibbles -> bytes
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            byt[2 * w] += nib[w] & 0x0f0f0f0fu;
+            byt[2 * w + 1] += (nib[w] >> 4) & 0x0f0f0f0fu;
+            nib[w] = 0;
+        }
+        if (++folds == 31u) flush();
+    }
+    __device__ __forceinline__ void finish() {
+        fold();
+        flush();
     }
 };
 
@@ -172,7 +207,6 @@ __global__ void __launch_bounds__(THREADS) plain_count_kernel(PlainArgs a, D d) 
         if (vec_ok) {
             const uint4* vp = reinterpret_cast<const uint4*>(in + e0);
             const uint64_t nv = (e1 - e0) / VEC;
-            int since_flush = 0;
             for (uint64_t i = tid; i < nv; i += static_cast<uint64_t>(THREADS) * UNROLL) {
                 uint4 r[UNROLL];
 #pragma unroll
@@ -189,24 +223,28 @@ __global__ void __launch_bounds__(THREADS) plain_count_kernel(PlainArgs a, D d) 
 #pragma unroll
                         for (int q = 0; q < VEC; q++) pc.add(d(e[q]));
                     }
-                }
-                if (++since_flush == 15) {  // <= 15 * 16 = 240 increments per lane
-                    pc.flush();
-                    since_flush = 0;
+                    if (u & 1) pc.fold();  // every two vectors: <= 8 increments
                 }
             }
-            for (uint64_t e = e0 + nv * VEC + tid; e < e1; e += THREADS) pc.add(d(in[e]));
+            uint32_t k = 0;
+            for (uint64_t e = e0 + nv * VEC + tid; e < e1; e += THREADS) {
+                pc.add(d(in[e]));
+                if (++k == 8u) {
+                    pc.fold();
+                    k = 0;
+                }
+            }
         } else {
-            int since_flush = 0;
+            uint32_t k = 0;
             for (uint64_t e = e0 + tid; e < e1; e += THREADS) {
                 pc.add(d(in[e]));
-                if (++since_flush == 255) {
-                    pc.flush();
-                    since_flush = 0;
+                if (++k == 8u) {
+                    pc.fold();
+                    k = 0;
                 }
             }
         }
-        pc.flush();
+        pc.finish();
 #pragma unroll
         for (int c = 0; c < M; c++) {
             const uint32_t s = warp_sum(pc.acc[c]);

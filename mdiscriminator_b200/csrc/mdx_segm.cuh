@@ -623,12 +623,27 @@ __global__ void __launch_bounds__(THREADS, 3)
             const uint64_t p0 = ent.p0, p1 = ent.p1;
             const uint64_t vs = in_vec ? ((p0 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u)) : p1;
             const uint64_t ve = in_vec ? max(vs, p1 & ~static_cast<uint64_t>(AU - 1u)) : p1;
-            for (uint64_t e = p0 + tid; e < min(vs, p1); e += THREADS) pc.add(dj(in[e]));
-            for (uint64_t e = ve + tid; e < p1 && vs < p1; e += THREADS) pc.add(dj(in[e]));
+            {
+                uint32_t k = 0;
+                for (uint64_t e = p0 + tid; e < min(vs, p1); e += THREADS) {
+                    pc.add(dj(in[e]));
+                    if (++k == 8u) {
+                        pc.fold();
+                        k = 0;
+                    }
+                }
+                for (uint64_t e = ve + tid; e < p1 && vs < p1; e += THREADS) {
+                    pc.add(dj(in[e]));
+                    if (++k == 8u) {
+                        pc.fold();
+                        k = 0;
+                    }
+                }
+                pc.fold();
+            }
             {
                 const uint4* vp = reinterpret_cast<const uint4*>(in + vs);
                 const uint32_t nv = static_cast<uint32_t>((ve - vs) / AU);
-                int since_flush = 0;
                 constexpr int UNROLL = 4;
                 for (uint32_t q = tid; q < nv; q += THREADS * UNROLL) {
                     uint4 r[UNROLL];
@@ -636,20 +651,18 @@ __global__ void __launch_bounds__(THREADS, 3)
                     for (int uu = 0; uu < UNROLL; uu++)
                         if (q + uu * THREADS < nv) r[uu] = __ldg(vp + q + uu * THREADS);
 #pragma unroll
-                    for (int uu = 0; uu < UNROLL; uu++)
+                    for (int uu = 0; uu < UNROLL; uu++) {
                         if (q + uu * THREADS < nv) {
                             V e[AU];
                             unpack16_to<V>(r[uu], e);
 #pragma unroll
                             for (uint32_t z = 0; z < AU; z++) pc.add(dj(e[z]));
                         }
-                    if (++since_flush == 14) {  // <= 14 * 16 + 2 * 3 edge elements < 256
-                        pc.flush();
-                        since_flush = 0;
+                        if (uu & 1) pc.fold();  // every two vectors: <= 8 increments
                     }
                 }
             }
-            pc.flush();
+            pc.finish();
 #pragma unroll
             for (int c = 0; c < M; c++) {
                 const uint32_t x = warp_sum(pc.acc[c]);
