@@ -217,6 +217,35 @@ mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint64_t n, mdx_
                                  mdx_stream_t stream);
 
 /*
+ * Wide elements.  Records of record_bytes (a multiple of 4) whose class comes
+ * from their first u32 word: mdiscr<ModArray<N,LEN>, LEN> over arrays of LEN
+ * unsigned ints (cuda_code/MdiscrHost_arrays.cu.h:26-36,250-430) is
+ * mdx_partition_records with record_bytes = 4 * LEN.  Columns permuted
+ * together (cuda_code/MdiscrHost_tuples.cu.h:262-429 partitions a u32, a u8 and
+ * a bool array by a functor of the first): column 0 is the u32 key the class
+ * comes from, the others (1, 2, 4 or 8 bytes per row, up to 8 columns in all)
+ * follow its rows.  Both build {key, row} 8-byte records, partition them with
+ * the 8-byte-record kernels and gather the rows (4- and 8-byte records take the
+ * direct paths); workspaces from the two size functions (they hold the record
+ * arrays: about 16 bytes per row).  Outputs must not overlap any input.
+ */
+size_t mdx_records_workspace_size(uint64_t n, uint32_t record_bytes, uint32_t m);
+mdx_status mdx_partition_records(const void* d_in, void* d_out, uint64_t n, uint32_t record_bytes,
+                                 mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                                 void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+typedef struct {
+    const void* in;      /* device, n rows */
+    void* out;           /* device, n rows */
+    uint32_t elem_bytes; /* 1, 2, 4 or 8 (column 0: 4, the key) */
+} mdx_column;
+
+size_t mdx_columns_workspace_size(uint64_t n, uint32_t m);
+mdx_status mdx_partition_columns(const mdx_column* cols, uint32_t num_cols, uint64_t n,
+                                 mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                                 void* d_ws, size_t ws_bytes, mdx_stream_t stream);
+
+/*
  * Distributed plain partition (no reference counterpart: the reference is
  * single-GPU; this is mdiscr<DISCR> of cuda_code/MdiscrHost_optimized_clean.cu.h:9-15
  * over one array spread across R ranks, one GPU each).  Rank r holds a

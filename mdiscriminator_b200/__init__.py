@@ -57,6 +57,10 @@ class Discr(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("m", ctypes.c_uint32)]
 
 
+class Column(ctypes.Structure):
+    _fields_ = [("inp", ctypes.c_void_p), ("out", ctypes.c_void_p), ("elem_bytes", ctypes.c_uint32)]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("plain_ctas_per_sm", ctypes.c_uint32), ("run_tiles", ctypes.c_uint32),
                 ("group_batch", ctypes.c_uint32), ("lag_slack_pct", ctypes.c_uint32)]
@@ -151,6 +155,15 @@ def lib() -> ctypes.CDLL:
             L.mdx_set_tuning.restype = st
             L.mdx_get_tuning.argtypes = [ctypes.c_int, u32, u64, ctypes.POINTER(Tuning)]
             L.mdx_get_tuning.restype = st
+            L.mdx_records_workspace_size.argtypes = [u64, u32, u32]
+            L.mdx_records_workspace_size.restype = sz
+            L.mdx_partition_records.argtypes = [vp, vp, u64, u32, Discr, vp, vp, vp, sz, vp]
+            L.mdx_partition_records.restype = st
+            L.mdx_columns_workspace_size.argtypes = [u64, u32]
+            L.mdx_columns_workspace_size.restype = sz
+            L.mdx_partition_columns.argtypes = [ctypes.POINTER(Column), u32, u64, Discr, vp, vp, vp,
+                                                sz, vp]
+            L.mdx_partition_columns.restype = st
             L.mdx_dist_count.argtypes = [vp, u64, ctypes.c_int, Discr, vp, vp, sz, vp]
             L.mdx_dist_count.restype = st
             L.mdx_dist_scatter.argtypes = [vp, u64, ctypes.c_int, Discr, vp, u32, u32,
@@ -315,6 +328,64 @@ def partition(d_in, discr, out=None, sizes=None, headflags=False, ws: Optional[W
                                    ctypes.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(stream), ev)
     _check(st, "mdx_partition")
     return (out, sizes, hf) if hf is not None else (out, sizes)
+
+
+# ------------------------------------------------------------ wide elements --
+def partition_records(d_in, record_bytes: int, discr, out=None, sizes=None, headflags=False,
+                      ws: Optional[Workspace] = None, stream=None):
+    """Stable partition of n records of ``record_bytes`` (a multiple of 4) held
+    in the byte view of ``d_in`` (any dtype, n * record_bytes bytes); the class
+    comes from each record's first u32 word (mdx_partition_records).  Returns
+    ``(out, sizes)`` [, head flags]."""
+    torch = _torch()
+    _require_cuda(d_in)
+    dc = make_discr(discr)
+    nbytes = d_in.numel() * d_in.element_size()
+    if record_bytes < 4 or record_bytes % 4 or nbytes % record_bytes:
+        raise MdxError(MDX_ERR_INVALID, "partition_records: bad record size")
+    n = nbytes // record_bytes
+    if out is None:
+        out = torch.empty_like(d_in)
+    if sizes is None:
+        sizes = torch.empty(dc.m, dtype=torch.uint32, device=d_in.device)
+    hf = torch.empty(n, dtype=torch.uint32, device=d_in.device) if headflags is True else (
+        headflags if headflags not in (False, None) else None)
+    need = int(lib().mdx_records_workspace_size(n, record_bytes, dc.m))
+    ws = ws or workspace(need, d_in.device, stream)
+    _check(lib().mdx_partition_records(ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                       n, record_bytes, dc, ctypes.c_void_p(sizes.data_ptr()),
+                                       ctypes.c_void_p(hf.data_ptr() if hf is not None else 0),
+                                       ctypes.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(stream)),
+           "mdx_partition_records")
+    return (out, sizes, hf) if hf is not None else (out, sizes)
+
+
+def partition_columns(columns, discr, outs=None, sizes=None, headflags=False,
+                      ws: Optional[Workspace] = None, stream=None):
+    """Stable partition of rows held in several 1-D CUDA tensors of equal
+    length (``columns[0]``: the u32/i32 key the class comes from; the others
+    of 1, 2, 4 or 8 bytes per element follow its rows; mdx_partition_columns).
+    Returns ``(outs, sizes)`` [, head flags]."""
+    torch = _torch()
+    _require_cuda(*columns)
+    dc = make_discr(discr)
+    n = columns[0].numel()
+    if any(c.numel() != n for c in columns) or columns[0].element_size() != 4:
+        raise MdxError(MDX_ERR_INVALID, "partition_columns: columns of one length, a 4-byte key")
+    outs = outs or [torch.empty_like(c) for c in columns]
+    if sizes is None:
+        sizes = torch.empty(dc.m, dtype=torch.uint32, device=columns[0].device)
+    hf = torch.empty(n, dtype=torch.uint32, device=columns[0].device) if headflags is True else (
+        headflags if headflags not in (False, None) else None)
+    arr = (Column * len(columns))(*[Column(c.data_ptr(), o.data_ptr(), c.element_size())
+                                    for c, o in zip(columns, outs)])
+    need = int(lib().mdx_columns_workspace_size(n, dc.m))
+    ws = ws or workspace(need, columns[0].device, stream)
+    _check(lib().mdx_partition_columns(arr, len(columns), n, dc, ctypes.c_void_p(sizes.data_ptr()),
+                                       ctypes.c_void_p(hf.data_ptr() if hf is not None else 0),
+                                       ctypes.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(stream)),
+           "mdx_partition_columns")
+    return (outs, sizes, hf) if hf is not None else (outs, sizes)
 
 
 # ------------------------------------------------- distributed plain path --

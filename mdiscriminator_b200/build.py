@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libmdx.so")
 SOURCES = [os.path.join(HERE, "csrc", "mdx_capi.cu"), os.path.join(HERE, "csrc", "mdx_noalloc.cu"),
-           os.path.join(HERE, "csrc", "mdx_server.cu")]
+           os.path.join(HERE, "csrc", "mdx_server.cu"), os.path.join(HERE, "csrc", "mdx_wide.cu")]
 HEADERS_DIRS = [os.path.join(HERE, "csrc"), os.path.join(os.path.dirname(HERE), "include")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
