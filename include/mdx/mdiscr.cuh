@@ -6,6 +6,8 @@
 //   #include "MdiscrHost_optimized_clean.cu.h"   ->   #include "mdx/mdiscr.cuh"
 //   mdiscr<Mod8>(n, 1 << 16, d_in, d_out)          (same call)
 //   mdiscrSegm<Mod4>(n, in, segment_sizes, out, new_sizes)   (same call)
+//   mdiscr<ModArray<N, LEN>, LEN>(n, hw, d_in, d_out)         (arrays, same call)
+//   mdiscr<ModTuple<N>>(n, hw, in1, in2, in3, out1, out2, out3) (tuples, same call)
 //
 // Signatures (reference):
 //   template<class DISCR> typename DISCR::TupleType
@@ -113,6 +115,91 @@ constexpr mdx_elem elem_kind() {
     return sizeof(T) == 4 ? MDX_ELEM_U32 : MDX_ELEM_REC8;
 }
 
+// Wide rows (arrays of LEN values, or a tuple of three arrays): each row's
+// class from the user's functor and its index as one 8-byte record, the stable
+// order of those records by class (the 8-byte-record kernels, class < M kept
+// by a mask), then every row moved to its place.
+constexpr int kRowThreads = 256;
+inline uint32_t row_grid(uint64_t work) {
+    uint64_t g = (work + kRowThreads - 1) / kRowThreads;
+    if (g > 148ull * 16) g = 148ull * 16;
+    return static_cast<uint32_t>(g < 1 ? 1 : g);
+}
+
+template <class DISCR, unsigned LEN, int M>
+__global__ void array_rows(const typename DISCR::InType* in, uint64_t n, uint64_t* rec) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * kRowThreads + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * kRowThreads) {
+        uint32_t c = DISCR::apply(const_cast<typename DISCR::InType*>(in + i * LEN));
+        c = c < static_cast<uint32_t>(M) ? c : static_cast<uint32_t>(M - 1);
+        rec[i] = static_cast<uint64_t>(c) | (i << 32);
+    }
+}
+
+template <class DISCR, int M>
+__global__ void tuple_rows(const typename DISCR::InType1* a, const typename DISCR::InType2* b,
+                           const typename DISCR::InType3* c3, uint64_t n, uint64_t* rec) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * kRowThreads + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * kRowThreads) {
+        uint32_t c = DISCR::apply(a[i], b[i], c3[i]);
+        c = c < static_cast<uint32_t>(M) ? c : static_cast<uint32_t>(M - 1);
+        rec[i] = static_cast<uint64_t>(c) | (i << 32);
+    }
+}
+
+template <class T>
+__global__ void gather_rows(const T* in, T* out, const uint64_t* perm, uint64_t n, unsigned len) {
+    const uint64_t total = n * len;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * kRowThreads + threadIdx.x; t < total;
+         t += static_cast<uint64_t>(gridDim.x) * kRowThreads) {
+        const uint64_t p = t / len;
+        out[t] = in[(perm[p] >> 32) * len + (t - p * len)];
+    }
+}
+
+template <class T1, class T2, class T3>
+__global__ void gather_tuple(const T1* a, const T2* b, const T3* c, T1* oa, T2* ob, T3* oc,
+                             const uint64_t* perm, uint64_t n) {
+    for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * kRowThreads + threadIdx.x; p < n;
+         p += static_cast<uint64_t>(gridDim.x) * kRowThreads) {
+        const uint64_t s = perm[p] >> 32;
+        oa[p] = a[s];
+        ob[p] = b[s];
+        oc[p] = c[s];
+    }
+}
+
+struct RowsLayout {
+    host::PlainLayout L;
+    size_t rec_in, rec_out, total;
+};
+inline RowsLayout rows_layout(uint64_t n, unsigned m) {
+    RowsLayout r;
+    r.L = host::plain_layout(n, MDX_ELEM_REC8, m);
+    r.rec_in = host::align_up(r.L.total, host::kAlign);
+    r.rec_out = host::align_up(r.rec_in + 8 * n, host::kAlign);
+    r.total = host::align_up(r.rec_out + 8 * n, host::kAlign);
+    return r;
+}
+
+// Stable order of the {class, row} records in rec_in into rec_out; class sizes.
+template <class TupleT, unsigned m>
+TupleT order_rows(uint64_t n, unsigned char* ws, const RowsLayout& R) {
+    constexpr int M = class_bound_of<m>();
+    const uint64_t* rin = reinterpret_cast<const uint64_t*>(ws + R.rec_in);
+    uint64_t* rout = reinterpret_cast<uint64_t*>(ws + R.rec_out);
+    check(host::run_plain<uint64_t, DiscrMask, M>(rin, rout, n, DiscrMask{M - 1u}, m, nullptr,
+                                                  nullptr, ws, R.L, nullptr, nullptr),
+          __FILE__, __LINE__);
+    check(take_error(ws), __FILE__, __LINE__);
+    uint32_t h[64];
+    if (cudaMemcpy(h, ws + R.L.class_tot, m * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        check(MDX_ERR_CUDA, __FILE__, __LINE__);
+    TupleT result;
+    for (unsigned c = 0; c < m; c++) result[c] = h[c];
+    return result;
+}
+
 }  // namespace detail
 
 template <class DISCR>
@@ -142,6 +229,73 @@ typename DISCR::TupleType mdiscr(const unsigned int num_elems, const unsigned in
     if (cudaMemcpy(h, ws + L.class_tot, m * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
         detail::check(MDX_ERR_CUDA, __FILE__, __LINE__);
     for (unsigned c = 0; c < m; c++) result[c] = h[c];
+    return result;
+}
+
+// Arrays of LEN values per element, class from the element's values
+// (mdiscr<DISCR, LEN>, cuda_code/MdiscrHost_arrays.cu.h:250-430; DISCR::apply
+// takes a pointer to the element's first value, as ModArray<N, LEN> does).
+template <class DISCR, unsigned int LEN>
+typename DISCR::TupleType mdiscr(const unsigned int num_elems, const unsigned int num_hwd_thds,
+                                 typename DISCR::InType* d_in, typename DISCR::InType* d_out) {
+    using In = typename DISCR::InType;
+    constexpr unsigned m = DISCR::TupleType::cardinal;
+    static_assert(m >= 1 && m <= 64, "1 <= m <= 64");
+    static_assert(LEN >= 1, "LEN >= 1");
+    (void)num_hwd_thds;
+    typename DISCR::TupleType result;
+    for (unsigned c = 0; c < m; c++) result[c] = 0;
+    if (num_elems == 0) return result;
+    const detail::RowsLayout R = detail::rows_layout(num_elems, m);
+    unsigned char* ws = detail::workspace(R.total);
+    if (ws == nullptr) detail::check(MDX_ERR_CUDA, __FILE__, __LINE__);
+    const char* ib = reinterpret_cast<const char*>(d_in);
+    const char* ob = reinterpret_cast<const char*>(d_out);
+    const uint64_t bytes = static_cast<uint64_t>(num_elems) * LEN * sizeof(In);
+    if (d_in == nullptr || d_out == nullptr || (ib < ob + bytes && ob < ib + bytes))
+        detail::check(MDX_ERR_INVALID, __FILE__, __LINE__);
+    constexpr int M = detail::class_bound_of<m>();
+    uint64_t* rin = reinterpret_cast<uint64_t*>(ws + R.rec_in);
+    detail::array_rows<DISCR, LEN, M><<<detail::row_grid(num_elems), detail::kRowThreads>>>(
+        d_in, num_elems, rin);
+    result = detail::order_rows<typename DISCR::TupleType, m>(num_elems, ws, R);
+    detail::gather_rows<In><<<detail::row_grid(static_cast<uint64_t>(num_elems) * LEN),
+                              detail::kRowThreads>>>(
+        d_in, d_out, reinterpret_cast<const uint64_t*>(ws + R.rec_out), num_elems, LEN);
+    detail::check(cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA, __FILE__, __LINE__);
+    detail::check(detail::take_error(ws), __FILE__, __LINE__);
+    return result;
+}
+
+// Three arrays partitioned together by a functor of their values
+// (cuda_code/MdiscrHost_tuples.cu.h:262-429: DISCR has InType1..3 and
+// apply(x, y, z)).
+template <class DISCR>
+typename DISCR::TupleType mdiscr(const unsigned int num_elems, const unsigned int num_hwd_thds,
+                                 typename DISCR::InType1* d_in1, typename DISCR::InType2* d_in2,
+                                 typename DISCR::InType3* d_in3, typename DISCR::InType1* d_out1,
+                                 typename DISCR::InType2* d_out2, typename DISCR::InType3* d_out3) {
+    constexpr unsigned m = DISCR::TupleType::cardinal;
+    static_assert(m >= 1 && m <= 64, "1 <= m <= 64");
+    (void)num_hwd_thds;
+    typename DISCR::TupleType result;
+    for (unsigned c = 0; c < m; c++) result[c] = 0;
+    if (num_elems == 0) return result;
+    if (!d_in1 || !d_in2 || !d_in3 || !d_out1 || !d_out2 || !d_out3)
+        detail::check(MDX_ERR_INVALID, __FILE__, __LINE__);
+    const detail::RowsLayout R = detail::rows_layout(num_elems, m);
+    unsigned char* ws = detail::workspace(R.total);
+    if (ws == nullptr) detail::check(MDX_ERR_CUDA, __FILE__, __LINE__);
+    constexpr int M = detail::class_bound_of<m>();
+    uint64_t* rin = reinterpret_cast<uint64_t*>(ws + R.rec_in);
+    detail::tuple_rows<DISCR, M><<<detail::row_grid(num_elems), detail::kRowThreads>>>(
+        d_in1, d_in2, d_in3, num_elems, rin);
+    result = detail::order_rows<typename DISCR::TupleType, m>(num_elems, ws, R);
+    detail::gather_tuple<<<detail::row_grid(num_elems), detail::kRowThreads>>>(
+        d_in1, d_in2, d_in3, d_out1, d_out2, d_out3,
+        reinterpret_cast<const uint64_t*>(ws + R.rec_out), num_elems);
+    detail::check(cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA, __FILE__, __LINE__);
+    detail::check(detail::take_error(ws), __FILE__, __LINE__);
     return result;
 }
 

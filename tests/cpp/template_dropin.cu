@@ -50,6 +50,25 @@ struct Decades {  // a functor that is not a remainder: class = (x / 10) % 6
     __host__ __device__ static inline unsigned int apply(volatile InType x) { return (x / 10u) % 6u; }
 };
 
+template <unsigned N, unsigned LEN>
+struct ArrayRemainder {  // records of LEN unsigned ints, class = x[0] % N (ModArray's concept)
+    typedef unsigned int InType;
+    typedef Counts<N> TupleType;
+    static const InType padelm = N - 1;
+    __host__ __device__ static inline unsigned int apply(volatile InType* x) { return x[0] % N; }
+};
+
+struct MixedTuple {  // (u32, u8, bool) rows, class from all three fields (tuple concept)
+    typedef unsigned int InType1;
+    typedef unsigned char InType2;
+    typedef bool InType3;
+    typedef Counts<7> TupleType;
+    __host__ __device__ static inline unsigned int apply(volatile InType1 x, volatile InType2 y,
+                                                         volatile InType3 z) {
+        return z ? x % 7u : y % 7u;
+    }
+};
+
 static unsigned long long rng_state = 88172645463325252ull;
 static unsigned int next_u32() {  // xorshift64
     rng_state ^= rng_state << 13;
@@ -151,6 +170,83 @@ static int segm_case(const char* name, unsigned n) {
     return ok ? 0 : 1;
 }
 
+template <class D, unsigned LEN>
+static int array_case(const char* name, unsigned n) {
+    const unsigned m = D::TupleType::cardinal;
+    std::vector<unsigned> h(static_cast<size_t>(n) * LEN), want(h.size());
+    for (auto& v : h) v = next_u32();
+    std::vector<unsigned> wsz(m, 0), cur(m, 0);
+    for (unsigned i = 0; i < n; i++) wsz[D::apply(&h[static_cast<size_t>(i) * LEN])]++;
+    for (unsigned c = 1; c < m; c++) cur[c] = cur[c - 1] + wsz[c - 1];
+    for (unsigned i = 0; i < n; i++) {
+        const unsigned p = cur[D::apply(&h[static_cast<size_t>(i) * LEN])]++;
+        std::memcpy(&want[static_cast<size_t>(p) * LEN], &h[static_cast<size_t>(i) * LEN], LEN * 4);
+    }
+    unsigned *d_in, *d_out;
+    cudaMalloc(&d_in, h.size() * 4);
+    cudaMalloc(&d_out, h.size() * 4);
+    cudaMemcpy(d_in, h.data(), h.size() * 4, cudaMemcpyHostToDevice);
+    typename D::TupleType sizes = mdiscr<D, LEN>(n, 1 << 16, d_in, d_out);
+    std::vector<unsigned> got(h.size());
+    cudaMemcpy(got.data(), d_out, h.size() * 4, cudaMemcpyDeviceToHost);
+    cudaFree(d_in);
+    cudaFree(d_out);
+    bool ok = got == want;
+    for (unsigned c = 0; c < m; c++) ok = ok && sizes[c] == wsz[c];
+    std::printf("%s n=%u: %s\n", name, n, ok ? "VALID" : "INVALID");
+    return ok ? 0 : 1;
+}
+
+static int tuple_case(const char* name, unsigned n) {
+    typedef MixedTuple D;
+    const unsigned m = D::TupleType::cardinal;
+    std::vector<unsigned> a(n), wa(n);
+    std::vector<unsigned char> b(n), wb(n);
+    bool* c = new bool[n];
+    bool* wc = new bool[n];
+    for (unsigned i = 0; i < n; i++) {
+        a[i] = next_u32();
+        b[i] = static_cast<unsigned char>(next_u32());
+        c[i] = (next_u32() & 1u) != 0;
+    }
+    std::vector<unsigned> wsz(m, 0), cur(m, 0);
+    for (unsigned i = 0; i < n; i++) wsz[D::apply(a[i], b[i], c[i])]++;
+    for (unsigned k = 1; k < m; k++) cur[k] = cur[k - 1] + wsz[k - 1];
+    for (unsigned i = 0; i < n; i++) {
+        const unsigned p = cur[D::apply(a[i], b[i], c[i])]++;
+        wa[p] = a[i];
+        wb[p] = b[i];
+        wc[p] = c[i];
+    }
+    unsigned *da, *oa;
+    unsigned char *db, *ob;
+    bool *dc, *oc;
+    cudaMalloc(&da, n * 4);
+    cudaMalloc(&oa, n * 4);
+    cudaMalloc(&db, n);
+    cudaMalloc(&ob, n);
+    cudaMalloc(&dc, n);
+    cudaMalloc(&oc, n);
+    cudaMemcpy(da, a.data(), n * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(db, b.data(), n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dc, c, n, cudaMemcpyHostToDevice);
+    typename D::TupleType sizes = mdiscr<D>(n, 1 << 16, da, db, dc, oa, ob, oc);
+    std::vector<unsigned> ga(n);
+    std::vector<unsigned char> gb(n);
+    bool* gc = new bool[n];
+    cudaMemcpy(ga.data(), oa, n * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(gb.data(), ob, n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(gc, oc, n, cudaMemcpyDeviceToHost);
+    cudaFree(da); cudaFree(oa); cudaFree(db); cudaFree(ob); cudaFree(dc); cudaFree(oc);
+    bool ok = ga == wa && gb == wb && std::memcmp(gc, wc, n) == 0;
+    for (unsigned k = 0; k < m; k++) ok = ok && sizes[k] == wsz[k];
+    delete[] c;
+    delete[] wc;
+    delete[] gc;
+    std::printf("%s n=%u: %s\n", name, n, ok ? "VALID" : "INVALID");
+    return ok ? 0 : 1;
+}
+
 int main() {
     int bad = 0;
     bad |= plain_case<LowBits8>("mdiscr<LowBits8>", 1u << 20);
@@ -161,5 +257,8 @@ int main() {
     bad |= segm_case<Remainder<4>>("mdiscrSegm<Remainder<4>>", 2000000u);
     bad |= segm_case<KeyRemainder<3>>("mdiscrSegm<KeyRemainder<3>>", 500000u);
     bad |= segm_case<Decades>("mdiscrSegm<Decades>", 300000u);
+    bad |= array_case<ArrayRemainder<5, 3>, 3>("mdiscr<ArrayRemainder<5,3>, 3>", 400003u);
+    bad |= array_case<ArrayRemainder<16, 8>, 8>("mdiscr<ArrayRemainder<16,8>, 8>", 100000u);
+    bad |= tuple_case("mdiscr<MixedTuple>", 500009u);
     return bad;
 }
