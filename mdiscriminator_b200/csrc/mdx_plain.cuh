@@ -156,13 +156,26 @@ __device__ void plain_finish_scan(const PlainArgs& a, uint32_t* tot_sh) {
     constexpr int W = THREADS / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t G = a.num_chunks;
+    // a warp per class; each lane takes PER consecutive chunk counts with all
+    // its loads in flight at once (this runs while the rest of the GPU waits)
+    constexpr uint32_t PER = 8;
     for (int c = warp; c < M; c += W) {
         uint32_t run = 0;
-        for (uint32_t k0 = 0; k0 < G; k0 += 32) {
-            const uint32_t kk = k0 + lane;
-            const uint32_t x = kk < G ? __ldcg(&a.chunk_cnt[c * G + kk]) : 0u;
-            const uint32_t incl = warp_incl_scan(x);
-            if (kk < G) a.chunk_pre[c * G + kk] = run + incl - x;
+        for (uint32_t k0 = 0; k0 < G; k0 += 32 * PER) {
+            const uint32_t kb = k0 + lane * PER;
+            uint32_t x[PER];
+#pragma unroll
+            for (uint32_t q = 0; q < PER; q++) x[q] = kb + q < G ? __ldcg(&a.chunk_cnt[c * G + kb + q]) : 0u;
+            uint32_t s = 0;
+#pragma unroll
+            for (uint32_t q = 0; q < PER; q++) s += x[q];
+            const uint32_t incl = warp_incl_scan(s);
+            uint32_t pre = run + incl - s;
+#pragma unroll
+            for (uint32_t q = 0; q < PER; q++) {
+                if (kb + q < G) a.chunk_pre[c * G + kb + q] = pre;
+                pre += x[q];
+            }
             run += __shfl_sync(0xffffffffu, incl, 31);
         }
         if (lane == 0) tot_sh[c] = run;
