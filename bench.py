@@ -315,6 +315,8 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
         elems = sum(r[4] for r in reqs)
         res.append({"offered_req_per_s": load, "achieved_submit_rate": k / t_sub,
                     "requests": k, "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
+                    "queue_p99_ms": st["queue_p99_s"] * 1e3, "exec_p99_ms": st["exec_p99_s"] * 1e3,
+                    "direct": st["direct"],
                     "gelem_per_s": elems / st["window_s"] / 1e9 if st["window_s"] > 0 else None,
                     "batches": st["batches"], "mean_request_elems": elems / k})
     # capacity: every request of a closed batch submitted at once

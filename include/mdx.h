@@ -299,7 +299,9 @@ mdx_status mdx_ipc_close(void* d_ptr, uint64_t offset);
  * allows, coalesces consecutive admitted requests into batched segmented
  * launches on up to num_streams streams at once (new requests are admitted
  * and launched while earlier batches run), and records every request's
- * latency from submit to completion.
+ * latency from submit to completion.  Long requests in device memory
+ * (direct_min_elems) still take their place in the pool but are partitioned
+ * in place by the plain kernels, one launch each, without the pool's copies.
  */
 typedef struct mdx_server_st* mdx_server;
 
@@ -309,6 +311,9 @@ typedef struct {
     uint32_t max_batch_requests;  /* requests per batched launch (0: 1024, <= 65535) */
     uint64_t max_batch_elems;     /* elements per batched launch (0: ring size) */
     uint32_t m_max;               /* largest m a request may use (0: 16, <= 16) */
+    uint64_t direct_min_elems;    /* requests at least this long whose buffers are device
+                                     memory are partitioned in place, without the pool's
+                                     copies (0: 2^20; UINT64_MAX: never) */
 } mdx_server_config;
 
 typedef struct {
@@ -316,6 +321,9 @@ typedef struct {
     uint64_t waiting, inflight_batches;
     double p50_s, p99_s, mean_s;  /* latency of completed requests, submit to completion */
     double window_s;              /* from the last reset to the last completion */
+    uint64_t direct;              /* requests partitioned in place */
+    double queue_p50_s, queue_p99_s;  /* submit -> launch of the request's batch (or lane) */
+    double exec_p50_s, exec_p99_s;    /* launch -> completion stamp */
 } mdx_server_stats;
 
 mdx_status mdx_server_create(mdx_server* server, const mdx_server_config* config);

@@ -639,7 +639,7 @@ def capture_partition_segmented(d_in, d_offsets, discr, out, seg_sizes, headflag
 class ServerConfig(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_uint64), ("num_streams", ctypes.c_uint32),
                 ("max_batch_requests", ctypes.c_uint32), ("max_batch_elems", ctypes.c_uint64),
-                ("m_max", ctypes.c_uint32)]
+                ("m_max", ctypes.c_uint32), ("direct_min_elems", ctypes.c_uint64)]
 
 
 class ServerStats(ctypes.Structure):
@@ -647,7 +647,9 @@ class ServerStats(ctypes.Structure):
                 ("batches", ctypes.c_uint64), ("elements", ctypes.c_uint64),
                 ("waiting", ctypes.c_uint64), ("inflight_batches", ctypes.c_uint64),
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("mean_s", ctypes.c_double),
-                ("window_s", ctypes.c_double)]
+                ("window_s", ctypes.c_double), ("direct", ctypes.c_uint64),
+                ("queue_p50_s", ctypes.c_double), ("queue_p99_s", ctypes.c_double),
+                ("exec_p50_s", ctypes.c_double), ("exec_p99_s", ctypes.c_double)]
 
 
 def _bind_server(L):
@@ -678,9 +680,10 @@ class Server:
     batched segmented launch; up to ``num_streams`` batches run at once."""
 
     def __init__(self, budget_bytes: int, num_streams: int = 2, max_batch_requests: int = 1024,
-                 max_batch_elems: int = 0, m_max: int = 16):
+                 max_batch_elems: int = 0, m_max: int = 16, direct_min_elems: int = 0):
         L = _bind_server(lib())
-        cfg = ServerConfig(budget_bytes, num_streams, max_batch_requests, max_batch_elems, m_max)
+        cfg = ServerConfig(budget_bytes, num_streams, max_batch_requests, max_batch_elems, m_max,
+                           direct_min_elems)
         h = ctypes.c_void_p()
         _check(L.mdx_server_create(ctypes.byref(h), ctypes.byref(cfg)), "mdx_server_create")
         self._h = h

@@ -15,10 +15,17 @@
 //    issues, on that slot's stream: a gather kernel copying every request's
 //    input into its ring slot, the per-segment-m segmented partition
 //    (mdx_partition_segmented_multi: one segment per request), a scatter
-//    kernel copying results and class sizes back to each request, and a host
-//    function stamping the completion time.  Requests that arrive while
+//    kernel copying results and class sizes back to each request, and an
+//    event whose completion the slot's waiter thread stamps.  Requests that arrive while
 //    batches run are admitted as ring space frees and launched on another
 //    stream: their work overlaps the batches already on the device.
+//  * In place: a request of at least direct_min_elems whose buffers are all
+//    device memory (and do not overlap) takes no ring space; it is admitted in
+//    its FIFO turn and partitioned by the plain kernels straight on its own
+//    buffers, queued on two lanes (a stream and a workspace each, up to four
+//    requests in stream order on each), so
+//    the long requests that carry most elements skip the pool's two copies
+//    and do not cut the runs of short requests that share a batch.
 //  * Completion: ring space is released in admission order when a batch
 //    finishes; waiters are woken; the latency of every request (submit to
 //    completion stamp) goes into the p50 / p99 statistics.
@@ -28,6 +35,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -91,6 +99,16 @@ __global__ void __launch_bounds__(kCopyThreads) copy_jobs(const CopyJob* jobs, u
     }
 }
 
+// True if p points into device memory (not host memory mapped for the device).
+inline bool is_device_memory(const void* p) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice;
+}
+
 // The device-side address of a buffer, or null when kernels cannot reach it
 // (pageable host memory, unknown pointers).
 template <class T>
@@ -118,13 +136,28 @@ struct Req {
     uint32_t* out;
     uint32_t* sizes;
     uint64_t off = 0;  // ring slot
-    double t_submit = 0, t_done = 0;
+    double t_submit = 0, t_launch = 0, t_done = 0;
     bool done = false;
+    bool direct = false;  // partitioned in place (long, device-resident): no ring copies
 };
 
 struct Batch;
 
+// Completion of the work on one stream: the scheduler records an event after
+// each unit of work (a batch, an in-place request) and queues it here with
+// what to do when it is done; the waiter thread waits for the events in order
+// (cudaEventSynchronize, without the server's lock), stamps the time and runs
+// the action under the lock.  Nothing is queued on the stream itself, so the
+// stream never stalls on the host.
+struct Waiter {
+    std::deque<std::pair<cudaEvent_t, std::function<void(double)>>> q;  // under Server::mu
+    std::condition_variable cv;
+    bool stop = false;
+    std::thread th;
+};
+
 struct Slot {                   // one stream's worth of batch resources
+    Waiter waiter;
     cudaStream_t stream = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -136,6 +169,20 @@ struct Slot {                   // one stream's worth of batch resources
     uint32_t* h_seg_m = nullptr;
     CopyJob* h_jobs = nullptr;
     bool busy = false;
+};
+
+struct Server;
+
+// Requests partitioned in place (long, in device memory): a stream and a
+// workspace, up to kLaneDepth requests queued on it in stream order.
+constexpr uint32_t kLanes = 2;
+constexpr uint32_t kLaneDepth = 4;
+struct Lane {
+    cudaStream_t stream = nullptr;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    uint32_t inflight = 0;
+    Waiter waiter;
 };
 
 struct Batch {
@@ -161,6 +208,9 @@ struct Server {
     std::condition_variable cv_sched, cv_done;
     std::deque<Req*> waiting;   // submitted, not admitted
     std::deque<Req*> admitted;  // in the ring, not launched
+    std::deque<Req*> admitted_direct;  // partitioned in place, not launched
+    std::vector<Lane> lanes;
+    std::vector<cudaEvent_t> free_events;
     std::unordered_map<uint64_t, Req*> reqs;  // every request not yet collected
     std::deque<Batch*> inflight;  // launch order
     uint64_t next_id = 1;
@@ -169,8 +219,8 @@ struct Server {
     mdx_status sticky = MDX_OK;   // first failure of a launch (reported by wait)
 
     // statistics
-    uint64_t st_submitted = 0, st_completed = 0, st_batches = 0, st_elements = 0;
-    std::vector<double> latencies;
+    uint64_t st_submitted = 0, st_completed = 0, st_batches = 0, st_elements = 0, st_direct = 0;
+    std::vector<double> latencies, queue_lat, exec_lat;
     double st_t0 = 0, st_t_last = 0;
 
     // ring: [off, off + n) for a new request, or false if it does not fit now.
@@ -198,25 +248,68 @@ struct Server {
     }
 };
 
-void CUDART_CB batch_done_cb(void* p) {  // runs on the driver's thread: no CUDA calls
-    Batch* b = static_cast<Batch*>(p);
-    Server* s = b->server;
-    std::lock_guard<std::mutex> lk(s->mu);
-    b->done = true;
-    b->t_done = now_s();
-    s->cv_sched.notify_all();
+void waiter_loop(Server* s, Waiter* w) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        while (w->q.empty() && !w->stop) w->cv.wait(lk);
+        if (w->q.empty()) break;  // stopped with nothing in flight
+        cudaEvent_t ev = w->q.front().first;
+        lk.unlock();
+        cudaEventSynchronize(ev);
+        const double t = now_s();
+        lk.lock();
+        auto done = std::move(w->q.front().second);
+        w->q.pop_front();
+        done(t);
+        s->free_events.push_back(ev);
+        s->cv_sched.notify_all();
+    }
 }
 
-// Admit waiting requests (FIFO) while they fit.  Caller holds the lock.
+// Record an event on `st` and hand `done` to its waiter.  Caller holds the lock.
+bool track(Server* s, Waiter& w, cudaStream_t st, std::function<void(double)> done) {
+    cudaEvent_t ev = nullptr;
+    if (!s->free_events.empty()) {
+        ev = s->free_events.back();
+        s->free_events.pop_back();
+    } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        return false;
+    }
+    if (cudaEventRecord(ev, st) != cudaSuccess) {
+        s->free_events.push_back(ev);
+        return false;
+    }
+    w.q.emplace_back(ev, std::move(done));
+    w.cv.notify_one();
+    return true;
+}
+
+// Admit waiting requests (FIFO) while they fit.  In-place requests need no
+// ring space.  Caller holds the lock.
 void admit(Server* s) {
     while (!s->waiting.empty()) {
         Req* r = s->waiting.front();
-        uint64_t off = 0;
-        if (!s->ring_alloc(r->n, &off)) break;
-        r->off = off;
-        s->admitted.push_back(r);
+        if (r->direct) {
+            s->admitted_direct.push_back(r);
+        } else {
+            uint64_t off = 0;
+            if (!s->ring_alloc(r->n, &off)) break;
+            r->off = off;
+            s->admitted.push_back(r);
+        }
         s->waiting.pop_front();
     }
+}
+
+void complete(Server* s, Req* r, double t_done) {  // caller holds the lock
+    r->t_done = t_done;
+    r->done = true;
+    s->st_completed++;
+    s->st_elements += r->n;
+    s->latencies.push_back(r->t_done - r->t_submit);
+    s->queue_lat.push_back(r->t_launch - r->t_submit);
+    s->exec_lat.push_back(r->t_done - r->t_launch);
+    s->st_t_last = r->t_done;
 }
 
 // Retire finished batches in launch order.  Caller holds the lock.
@@ -225,14 +318,8 @@ void retire(Server* s) {
         Batch* b = s->inflight.front();
         s->inflight.pop_front();
         for (uint64_t id : b->ids) {
-            Req* r = s->reqs[id];
-            r->t_done = b->t_done;
-            r->done = true;
             s->live.pop_front();
-            s->st_completed++;
-            s->st_elements += r->n;
-            s->latencies.push_back(r->t_done - r->t_submit);
-            s->st_t_last = r->t_done;
+            complete(s, s->reqs[id], b->t_done);
         }
         s->slots[b->slot].busy = false;
         delete b;
@@ -281,15 +368,51 @@ void scheduler(Server* s) {
     for (;;) {
         retire(s);
         admit(s);
+        // long requests in device memory: the plain kernels straight on their
+        // buffers, queued on the least loaded lane up to its depth
+        while (!s->admitted_direct.empty()) {
+            Lane* l = nullptr;
+            for (Lane& c : s->lanes)
+                if (c.inflight < kLaneDepth && (l == nullptr || c.inflight < l->inflight)) l = &c;
+            if (l == nullptr) break;
+            Req* r = s->admitted_direct.front();
+            s->admitted_direct.pop_front();
+            l->inflight++;
+            r->t_launch = now_s();
+            s->st_direct++;
+            lk.unlock();
+            const mdx_discr dc = {MDX_DISCR_MOD, r->m};
+            mdx_status st = mdx_partition(r->in, r->out, r->n, MDX_ELEM_U32, dc, r->sizes, nullptr,
+                                          l->ws, l->ws_bytes, reinterpret_cast<mdx_stream_t>(l->stream));
+            lk.lock();
+            auto done = [s, l, r](double t) {
+                complete(s, r, t);
+                l->inflight--;
+            };
+            if (st != MDX_OK || !track(s, l->waiter, l->stream, done)) {
+                // nothing will complete this request: finish it now
+                if (s->sticky == MDX_OK) s->sticky = st != MDX_OK ? st : MDX_ERR_CUDA;
+                done(now_s());
+            }
+        }
         int free_slot = -1;
         for (size_t k = 0; k < s->slots.size(); k++)
             if (!s->slots[k].busy) { free_slot = static_cast<int>(k); break; }
-        if (s->stop && s->admitted.empty() && s->waiting.empty() && s->inflight.empty()) break;
-        if (free_slot < 0 || s->admitted.empty()) {
-            s->cv_sched.wait(lk);
+        bool lanes_busy = false, lane_free = false;
+        for (const Lane& l : s->lanes) {
+            lanes_busy = lanes_busy || l.inflight > 0;
+            lane_free = lane_free || l.inflight < kLaneDepth;
+        }
+        if (s->stop && s->admitted.empty() && s->admitted_direct.empty() && s->waiting.empty() &&
+            s->inflight.empty() && !lanes_busy)
+            break;
+        const bool can_batch = free_slot >= 0 && !s->admitted.empty();
+        const bool can_direct = lane_free && !s->admitted_direct.empty();
+        if (!can_batch) {
+            if (!can_direct) s->cv_sched.wait(lk);
             continue;
         }
-        // the longest contiguous run of admitted requests, within the caps
+        // the longest contiguous run of admitted ring requests, within the caps
         std::vector<Req*> batch;
         uint64_t elems = 0, end = 0;
         while (!s->admitted.empty() && batch.size() < s->cfg.max_batch_requests) {
@@ -303,19 +426,24 @@ void scheduler(Server* s) {
         Slot& sl = s->slots[free_slot];
         sl.busy = true;
         Batch* b = new Batch{free_slot, {}, end, false, 0, s};
-        for (Req* r : batch) b->ids.push_back(r->id);
+        const double t_launch = now_s();
+        for (Req* r : batch) {
+            b->ids.push_back(r->id);
+            r->t_launch = t_launch;
+        }
         s->inflight.push_back(b);
         s->st_batches++;
         lk.unlock();
         mdx_status st = launch_batch(s, sl, batch);
-        if (st == MDX_OK &&
-            cudaLaunchHostFunc(sl.stream, batch_done_cb, b) != cudaSuccess)
-            st = MDX_ERR_CUDA;
         lk.lock();
-        if (st != MDX_OK) {  // nothing will complete this batch: finish it now
-            if (s->sticky == MDX_OK) s->sticky = st;
+        auto done = [b](double t) {
             b->done = true;
-            b->t_done = now_s();
+            b->t_done = t;
+        };
+        if (st != MDX_OK || !track(s, sl.waiter, sl.stream, done)) {
+            // nothing will complete this batch: finish it now
+            if (s->sticky == MDX_OK) s->sticky = st != MDX_OK ? st : MDX_ERR_CUDA;
+            done(now_s());
         }
     }
 }
@@ -339,6 +467,7 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
     if (cfg.max_batch_requests == 0) cfg.max_batch_requests = 1024;
     if (cfg.max_batch_requests > 65535) cfg.max_batch_requests = 65535;
     if (cfg.m_max == 0) cfg.m_max = 16;
+    if (cfg.direct_min_elems == 0) cfg.direct_min_elems = 1ull << 20;
     if (cfg.m_max > 16 || cfg.budget_bytes < 8 * 4096) return MDX_ERR_INVALID;
     auto* h = new mdx_server_st();
     Server& s = h->s;
@@ -350,7 +479,7 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
               cudaMalloc(&s.d_in, s.cap * 4) == cudaSuccess &&
               cudaMalloc(&s.d_out, s.cap * 4) == cudaSuccess;
     const uint32_t B = s.cfg.max_batch_requests;
-    s.slots.resize(cfg.num_streams);
+    s.slots = std::vector<Slot>(cfg.num_streams);  // sized once: completions hold pointers
     for (auto& sl : s.slots) {
         if (!ok) break;
         sl.ws_bytes = mdx_segmented_workspace_size(s.cfg.max_batch_elems, B, MDX_ELEM_U32, cfg.m_max);
@@ -365,11 +494,21 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
              cudaMallocHost(&sl.h_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
              cudaMallocHost(&sl.h_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess;
     }
+    s.lanes = std::vector<Lane>(kLanes);  // sized once: completions hold Lane pointers
+    for (auto& l : s.lanes) {
+        if (!ok) break;
+        l.ws_bytes = mdx_workspace_size(s.cfg.max_batch_elems, MDX_ELEM_U32, cfg.m_max);
+        ok = cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaMalloc(&l.ws, l.ws_bytes) == cudaSuccess &&
+             mdx_workspace_init(l.ws, l.ws_bytes, reinterpret_cast<mdx_stream_t>(l.stream)) == MDX_OK;
+    }
     if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
         mdx_server_destroy(h);
         return MDX_ERR_CUDA;
     }
     s.st_t0 = now_s();
+    for (auto& sl : s.slots) sl.waiter.th = std::thread(waiter_loop, &s, &sl.waiter);
+    for (auto& l : s.lanes) l.waiter.th = std::thread(waiter_loop, &s, &l.waiter);
     s.sched = std::thread(scheduler, &s);
     *out = h;
     return MDX_OK;
@@ -393,6 +532,12 @@ mdx_status mdx_server_submit(mdx_server h, const uint32_t* in, uint32_t* out, ui
     r->in = d_in;
     r->out = d_out;
     r->sizes = d_sizes;
+    if (n >= s.cfg.direct_min_elems && is_device_memory(in) && is_device_memory(out) &&
+        is_device_memory(sizes)) {
+        const char* ib = reinterpret_cast<const char*>(d_in);
+        const char* ob = reinterpret_cast<const char*>(d_out);
+        r->direct = !(ib < ob + n * 4 && ob < ib + n * 4);  // overlapping buffers go through the ring
+    }
     {
         std::lock_guard<std::mutex> lk(s.mu);
         r->id = s.next_id++;
@@ -430,17 +575,25 @@ mdx_status mdx_server_get_stats(mdx_server h, mdx_server_stats* out) {
     out->elements = s.st_elements;
     out->waiting = s.waiting.size();
     out->inflight_batches = s.inflight.size();
-    std::vector<double> v = s.latencies;
-    out->p50_s = out->p99_s = out->mean_s = 0;
-    if (!v.empty()) {
+    auto pct = [](std::vector<double> v, double q) {
+        if (v.empty()) return 0.0;
         std::sort(v.begin(), v.end());
-        out->p50_s = v[(v.size() - 1) / 2];
-        out->p99_s = v[std::min(v.size() - 1, static_cast<size_t>(0.99 * (v.size() - 1) + 0.5))];
+        return v[std::min(v.size() - 1, static_cast<size_t>(q * (v.size() - 1) + 0.5))];
+    };
+    out->p50_s = out->p99_s = out->mean_s = 0;
+    if (!s.latencies.empty()) {
+        out->p50_s = pct(s.latencies, 0.5);
+        out->p99_s = pct(s.latencies, 0.99);
         double sum = 0;
-        for (double x : v) sum += x;
-        out->mean_s = sum / v.size();
+        for (double x : s.latencies) sum += x;
+        out->mean_s = sum / s.latencies.size();
     }
+    out->queue_p50_s = pct(s.queue_lat, 0.5);
+    out->queue_p99_s = pct(s.queue_lat, 0.99);
+    out->exec_p50_s = pct(s.exec_lat, 0.5);
+    out->exec_p99_s = pct(s.exec_lat, 0.99);
     out->window_s = s.st_t_last > s.st_t0 ? s.st_t_last - s.st_t0 : 0.0;
+    out->direct = s.st_direct;
     return MDX_OK;
 }
 
@@ -448,8 +601,10 @@ mdx_status mdx_server_reset_stats(mdx_server h) {
     if (h == nullptr) return MDX_ERR_INVALID;
     Server& s = h->s;
     std::lock_guard<std::mutex> lk(s.mu);
-    s.st_submitted = s.st_completed = s.st_batches = s.st_elements = 0;
+    s.st_submitted = s.st_completed = s.st_batches = s.st_elements = s.st_direct = 0;
     s.latencies.clear();
+    s.queue_lat.clear();
+    s.exec_lat.clear();
     s.st_t0 = now_s();
     s.st_t_last = s.st_t0;
     return MDX_OK;
@@ -466,6 +621,20 @@ mdx_status mdx_server_destroy(mdx_server h) {
         s.cv_sched.notify_all();
         s.sched.join();
     }
+    {  // the scheduler left with nothing in flight: the waiters have no work left
+        std::lock_guard<std::mutex> lk(s.mu);
+        for (auto& sl : s.slots) sl.waiter.stop = true;
+        for (auto& l : s.lanes) l.waiter.stop = true;
+    }
+    for (auto& sl : s.slots) {
+        sl.waiter.cv.notify_all();
+        if (sl.waiter.th.joinable()) sl.waiter.th.join();
+    }
+    for (auto& l : s.lanes) {
+        l.waiter.cv.notify_all();
+        if (l.waiter.th.joinable()) l.waiter.th.join();
+    }
+    for (cudaEvent_t ev : s.free_events) cudaEventDestroy(ev);
     for (auto& sl : s.slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         cudaFree(sl.ws);
@@ -477,6 +646,11 @@ mdx_status mdx_server_destroy(mdx_server h) {
         cudaFreeHost(sl.h_seg_m);
         cudaFreeHost(sl.h_jobs);
         if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    for (auto& l : s.lanes) {
+        if (l.stream) cudaStreamSynchronize(l.stream);
+        cudaFree(l.ws);
+        if (l.stream) cudaStreamDestroy(l.stream);
     }
     cudaFree(s.d_in);
     cudaFree(s.d_out);

@@ -108,3 +108,38 @@ def test_admission_waits_for_budget(cuda_ready):
             eo, es = oracle.partition(x, 4)
             assert np.array_equal(o.cpu().numpy(), eo) and np.array_equal(s.cpu().numpy(), es)
         assert srv.stats()["batches"] > 1
+
+
+def test_long_device_requests_are_partitioned_in_place(cuda_ready):
+    """Requests of at least direct_min_elems in device memory skip the pool's
+    copies (plain kernels on their own buffers); mixed with short ones, their
+    results equal the oracle and the same requests served with that path
+    switched off."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    rng = np.random.default_rng(11)
+    specs = []
+    for i in range(24):
+        n = int(rng.choice([3000, 70_000, 1 << 20, 3_000_017, 5 << 20]))
+        specs.append((n, int(rng.choice([2, 5, 8, 16])), 500 + i))
+    results = {}
+    for direct_min in (0, 2**64 - 1):  # default threshold (2^20), then never
+        with mdx.Server(budget_bytes=1 << 30, num_streams=3, direct_min_elems=direct_min) as srv:
+            reqs = []
+            for n, m, seed in specs:
+                x, d, o = _request(torch, n, seed)
+                reqs.append((x, d, o, _sizes(torch, m), m))
+            tickets = [srv.submit(d, o, s, m) for (_, d, o, s, m) in reqs]
+            for t in tickets:
+                srv.wait(t)
+            st = srv.stats()
+            long_ones = sum(1 for n, _, _ in specs if n >= (1 << 20))
+            assert st["direct"] == (long_ones if direct_min == 0 else 0)
+            results[direct_min] = [(o.cpu().numpy(), s.cpu().numpy()) for (_, _, o, s, _) in reqs]
+            for k, (x, _, _, _, m) in enumerate(reqs):
+                if k % 3 == 0:
+                    eo, es = oracle.partition(x, m)
+                    assert np.array_equal(results[direct_min][k][0], eo), f"request {k}"
+                    assert np.array_equal(results[direct_min][k][1], es), f"request {k}"
+    for (a_o, a_s), (b_o, b_s) in zip(results[0], results[2**64 - 1]):
+        assert np.array_equal(a_o, b_o) and np.array_equal(a_s, b_s)
