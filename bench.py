@@ -379,6 +379,55 @@ def cpu_baseline(n_sample: int, m: int, reps: int):
                       f"best of {reps}, its own gettimeofday timer, OMP threads={threads}"}, None
 
 
+def distributed_main(args, torch, dist, mdx, dev, world, rank):
+    """--distributed: one array of world * N elements, rank r holding the r-th
+    chunk of N (weak scaling), partitioned by the "p2p" transport of
+    mdiscriminator_b200.distributed (count, all-gather of the counts, the
+    scatter kernel storing into every rank's output chunk through IPC
+    mappings, completion barrier).  Device time by CUDA events, max over
+    ranks."""
+    import socket
+
+    from mdiscriminator_b200 import distributed as D
+    if world == 1:
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            port = s.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                                world_size=1, device_id=dev)
+    n, m = args.n, args.m
+    discr = ("mask", m) if (m & (m - 1)) == 0 else ("mod", m)
+    x = make_input(torch, n, 1234 + rank, dev)
+    out = None
+    for _ in range(args.warmup):
+        out, _ = D.partition_distributed(x, discr, out=out)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        out, _ = D.partition_distributed(x, discr, out=out, check=False)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1) / args.steps], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Gelem/s, one array over the ranks (distributed partition)",
+            "value": world * n / ms / 1e6, "unit": "Gelem/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": f"stable partition of {world} x {n} int32, m={m}, rank r holds "
+                                   "chunk r; output in balanced chunks across the ranks",
+                       "n_per_rank": n, "m": m, "parallelism": f"p2p over {world} ranks"},
+            "gpu_launches": 3 * args.steps}))
+    D.close_peer_maps()
+    dist.destroy_process_group()
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU implementation, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -432,6 +481,8 @@ def main():
                     help="skip the served-requests measurement")
     ap.add_argument("--no-sort", action="store_true",
                     help="skip the sort-based reference point")
+    ap.add_argument("--distributed", action="store_true",
+                    help="partition one array spread over the ranks (p2p transport)")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched segmented measurement and print its JSON")
     ap.add_argument("--batched-segments", type=int, default=100_000)
@@ -456,6 +507,8 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
+    if args.distributed:
+        return distributed_main(args, torch, dist, mdx, dev, world, rank)
 
     if args.batched_only:
         peak, _ = peaks()
@@ -562,7 +615,27 @@ def main():
     e2e_value = world * n * args.e2e_steps / e2e_s / 1e9
     # sanity: the last result equals the device result of the same input
     assert torch.equal(e2e_sets[(args.e2e_steps - 1) % 2]["h_out"].to(dev), d_out)
-    del e2e_sets
+    # the bound of the e2e leg: the same two copies alone, in both directions at
+    # once (pinned memory, the same two streams), no partition
+    a, b = e2e_sets
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    c0.record(stream)
+    a["stream"].wait_event(c0)
+    b["stream"].wait_event(c0)
+    with torch.cuda.stream(a["stream"]):
+        a["d_in"].copy_(a["h_in"], non_blocking=True)
+    with torch.cuda.stream(b["stream"]):
+        b["h_out"].copy_(b["d_out"], non_blocking=True)
+    stream.wait_stream(a["stream"])
+    stream.wait_stream(b["stream"])
+    c1.record(stream)
+    torch.cuda.synchronize()
+    copy_s = c0.elapsed_time(c1) * 1e-3
+    pcie_gbs = n * 4 / copy_s / 1e9        # per direction, both directions busy
+    e2e_bound = world * n / copy_s / 1e9   # elements/s if the copies were all a step cost
+    del e2e_sets, a, b
 
     if rank == 0:
         peak, peak_src = peaks()
@@ -614,7 +687,11 @@ def main():
                        "parallelism": f"independent arrays per rank x{world}" if world > 1
                        else "single GPU"},
             "e2e": {"value": e2e_value, "unit": "Gelem/s", "h2d_bytes_per_step": n * 4,
-                    "d2h_bytes_per_step": n * 4 + m * 4},
+                    "d2h_bytes_per_step": n * 4 + m * 4,
+                    "pcie_duplex_gbs": pcie_gbs, "copy_bound": e2e_bound,
+                    "frac_of_copy_bound": e2e_value / e2e_bound,
+                    "note": "copy_bound: 1 GiB host-to-device and 1 GiB device-to-host at once "
+                            "on the same streams, no partition (CUDA events)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "batched": batched,

@@ -16,15 +16,17 @@
 //                   resets the persistent kernel's ticket.
 //   seg_plan_emit   writes the run entries {segment, [p0, p1), last run of
 //                   the segment} and the group heads, in element order.
-//   seg_main        one persistent launch.  CTAs take tickets in order (each
-//                   CTA fetches its next ticket while it works on the current
-//                   one):
-//                     * small-segment groups: the group's range is read into
-//                       shared memory once, warps partition one segment each
-//                       (count pass, then __match_any_sync + __popc ranks with
-//                       running class counts) into a shared output image, and
-//                       the CTA writes the range back with 16-byte stores --
-//                       one HBM read and one write per element;
+//   seg_main        one persistent launch.  CTAs take tickets in order, a
+//                   ticket only when the CTA is ready to work on it:
+//                     * batches of small-segment groups: each group's range is
+//                       read into shared memory by one bulk copy (the next
+//                       group's copy overlaps the current group's work), warps
+//                       partition one segment each (lanes own odd-stride
+//                       contiguous sub-ranges: per-lane 16-bit class counters,
+//                       a warp scan, a second pass places the elements) into a
+//                       shared output image, and the CTA writes the range back
+//                       with 16-byte stores -- one HBM read and one write per
+//                       element;
 //                     * then, per run j of a large segment, a count item C(j)
 //                       (class counts of the run with 16-byte loads, published
 //                       to epoch-tagged per-class status words; decoupled

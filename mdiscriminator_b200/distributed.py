@@ -164,20 +164,26 @@ def partition_distributed(x_local, discr, group=None, transport: str = "auto", o
         ws = _workspace(max(workspace_size(max(n_local, 1), elem, m), 256), x_local.device)
         counts = dist_count(x_local, discr, ws)
         all_counts = _gather_counts(counts.to(torch.int64), group, R)
-        # every rank's output chunk mapped into this process
-        h, off = ipc_handle(out) if out.numel() > 0 else (b"", 0)
-        infos = [None] * R
-        dist.all_gather_object(infos, (h, off), group=group)
+        # every rank's output chunk mapped into this process: one small tensor
+        # all-gather of (offset in its allocation, allocation handle); a handle
+        # seen before reuses its mapping
+        h, off = ipc_handle(out) if out.numel() > 0 else (bytes(64), 0)
+        mine = torch.tensor([off] + list(np.frombuffer(h, dtype=np.int64)), dtype=torch.int64,
+                            device=x_local.device)
+        parts = [torch.empty_like(mine) for _ in range(R)]
+        dist.all_gather(parts, mine, group=group)
         ptrs = []
-        for q, (hq, offq) in enumerate(infos):
+        for q, t in enumerate(parts):
+            v = t.cpu().numpy()
+            hq = v[1:].tobytes()
             if q == rank:
                 ptrs.append(out.data_ptr())
-            elif not hq:
+            elif not any(hq):
                 ptrs.append(0)
             else:
                 if hq not in _peer_maps:
                     _peer_maps[hq] = ipc_open(hq, 0)
-                ptrs.append(_peer_maps[hq] + offq)
+                ptrs.append(_peer_maps[hq] + int(v[0]))
         sizes = dist_scatter(x_local, discr, all_counts.to(torch.uint32), rank, ptrs, chunk,
                              n_total, ws)
         # completion barrier: no rank reads its chunk before every rank's

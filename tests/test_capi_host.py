@@ -97,3 +97,33 @@ def test_no_cpu_fallback_for_host_tensors():
     x = torch.zeros(16, dtype=torch.int32)
     with pytest.raises(ValueError, match="CUDA tensors only"):
         mdx.partition(x, ("mod", 4))
+
+
+def test_distributed_entry_points_validate_before_device_work(L):
+    """mdx_dist_count / mdx_dist_scatter / mdx_ipc_* refuse bad arguments on the
+    host: rank counts, ranks, chunk sizes that break the 16-byte rule, null or
+    misaligned chunk pointers, counts larger than the total."""
+    d = mdx.make_discr(("mod", 5))
+    vp = ctypes.c_void_p
+    fake = vp(0x100000)  # never dereferenced: every call below fails its checks first
+    two = (vp * 2)(vp(0x200000), vp(0x300000))
+    E = mdx.MDX_ERR_INVALID
+    assert L.mdx_dist_count(fake, 10, mdx.ELEM_U32, d, None, None, 0, None) == E  # no counts
+    assert L.mdx_dist_count(fake, 10, 9, d, fake, None, 0, None) == E  # element layout
+    bad_m = mdx.Discr(mdx.DISCR_MOD, 65)
+    assert L.mdx_dist_count(fake, 10, mdx.ELEM_U32, bad_m, fake, None, 0, None) == E
+    args = lambda R, rank, ptrs, chunk, total, n=10: (fake, n, mdx.ELEM_U32, d, fake, R, rank, ptrs,
+                                                      chunk, total, None, fake, 1 << 20, None)
+    assert L.mdx_dist_scatter(*args(0, 0, two, 8, 16)) == E       # no ranks
+    assert L.mdx_dist_scatter(*args(2, 2, two, 8, 16)) == E       # rank out of range
+    assert L.mdx_dist_scatter(*args(129, 0, two, 8, 16)) == E     # more ranks than supported
+    assert L.mdx_dist_scatter(*args(2, 0, two, 6, 16)) == E       # chunk not 16 bytes of elements
+    assert L.mdx_dist_scatter(*args(2, 0, two, 0, 16)) == E       # empty chunk
+    assert L.mdx_dist_scatter(*args(2, 0, two, 8, 9, n=10)) == E  # more local rows than the total
+    misaligned = (vp * 2)(vp(0x200004), vp(0x300000))
+    assert L.mdx_dist_scatter(*args(2, 0, misaligned, 8, 16)) == E
+    nulls = (vp * 2)(vp(0x200000), vp(0))
+    assert L.mdx_dist_scatter(*args(2, 0, nulls, 8, 16)) == E     # rank 1's chunk is not empty
+    assert L.mdx_ipc_get_handle(None, None, None) == E
+    assert L.mdx_ipc_open(None, 0, None) == E
+    assert L.mdx_ipc_close(None, 0) == E
