@@ -40,8 +40,12 @@ typedef enum {
 /* Element layouts.  U32: one unsigned 32-bit value, class from the value
  * (InType = unsigned int of Mod4/Mod8/Mod<N>, HelpersCommon.h:587-596,840-849,
  * 1200-1210).  REC8: 8-byte record {u32 key; u32 payload}, class from the key
- * (ModArray<N,2>, MdiscrHost_arrays.cu.h:26-36 with LEN = 2). */
-typedef enum { MDX_ELEM_U32 = 0, MDX_ELEM_REC8 = 1 } mdx_elem;
+ * (ModArray<N,2>, MdiscrHost_arrays.cu.h:26-36 with LEN = 2).  REC16: 16-byte
+ * record {u32 key; 12 bytes of payload}, 16-byte aligned (ModArray<N,4>);
+ * plain partitions only (mdx_partition, mdx_partition_records): the
+ * segmented, distributed and no-allocation entry points return
+ * MDX_ERR_UNSUPPORTED for it. */
+typedef enum { MDX_ELEM_U32 = 0, MDX_ELEM_REC8 = 1, MDX_ELEM_REC16 = 2 } mdx_elem;
 
 /* Discriminator families.  MOD: class = key % m (Mod<N>::apply,
  * HelpersCommon.h:1207-1209).  MASK: class = key & (m-1), m a power of two

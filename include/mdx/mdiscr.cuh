@@ -108,11 +108,12 @@ constexpr int class_bound_of() {
 }
 
 template <class T>
-using elem_of = typename std::conditional<sizeof(T) == 4, uint32_t, uint64_t>::type;
+using elem_of = typename std::conditional<
+    sizeof(T) == 4, uint32_t, typename std::conditional<sizeof(T) == 8, uint64_t, Rec16>::type>::type;
 
 template <class T>
 constexpr mdx_elem elem_kind() {
-    return sizeof(T) == 4 ? MDX_ELEM_U32 : MDX_ELEM_REC8;
+    return sizeof(T) == 4 ? MDX_ELEM_U32 : sizeof(T) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_REC16;
 }
 
 // Wide rows (arrays of LEN values, or a tuple of three arrays): each row's
@@ -206,7 +207,8 @@ template <class DISCR>
 typename DISCR::TupleType mdiscr(const unsigned int num_elems, const unsigned int num_hwd_thds,
                                  typename DISCR::InType* d_in, typename DISCR::InType* d_out) {
     using In = typename DISCR::InType;
-    static_assert(sizeof(In) == 4 || sizeof(In) == 8, "4-byte values or 8-byte records");
+    static_assert(sizeof(In) == 4 || sizeof(In) == 8 || sizeof(In) == 16,
+                  "4-byte values, 8- or 16-byte records");
     constexpr unsigned m = DISCR::TupleType::cardinal;
     static_assert(m >= 1 && m <= 64, "1 <= m <= 64");
     constexpr int M = detail::class_bound_of<m>();

@@ -42,6 +42,7 @@ MDX_ERR_SEGMENTS = 6
 
 ELEM_U32 = 0
 ELEM_REC8 = 1
+ELEM_REC16 = 2  # 16-byte records, plain partitions only
 DISCR_MOD = 0
 DISCR_MASK = 1
 MAX_CLASSES = 64

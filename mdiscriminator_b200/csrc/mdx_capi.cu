@@ -1,6 +1,6 @@
 // mdx_capi.cu -- the C ABI (include/mdx.h) over pre-instantiated kernels.
 //
-// Instantiated families: element U32 / REC8 x discriminator MOD / MASK x class
+// Instantiated families: element U32 / REC8 / REC16 (plain only) x discriminator MOD / MASK x class
 // bound M in {2, 4, 8, 16, 32, 64} (the smallest bound >= m is used; m itself
 // is a run-time parameter of the functor).
 #include <cuda_runtime.h>
@@ -73,6 +73,8 @@ mdx_status mdx_partition_timed(const void* d_in, void* d_out, uint64_t n, mdx_el
     unsigned char* ws = static_cast<unsigned char*>(d_ws);
     if (elem == MDX_ELEM_U32)
         return dispatch_plain<uint32_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
+    if (elem == MDX_ELEM_REC16)
+        return dispatch_plain<Rec16>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
     return dispatch_plain<uint64_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
 }
 
@@ -87,6 +89,7 @@ mdx_status mdx_dist_count(const void* d_in, uint64_t n_local, mdx_elem elem, mdx
                           uint32_t* d_counts, void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
+    if (elem == MDX_ELEM_REC16) return MDX_ERR_UNSUPPORTED;
     if ((s = check_discr(discr)) != MDX_OK) return s;
     if (n_local > MDX_MAX_ELEMS || d_counts == nullptr) return MDX_ERR_INVALID;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
@@ -112,6 +115,7 @@ mdx_status mdx_dist_scatter(const void* d_in, uint64_t n_local, mdx_elem elem, m
                             uint32_t* d_sizes, void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
+    if (elem == MDX_ELEM_REC16) return MDX_ERR_UNSUPPORTED;
     if ((s = check_discr(discr)) != MDX_OK) return s;
     if (num_ranks == 0 || num_ranks > static_cast<uint32_t>(kMaxRanks) || rank >= num_ranks ||
         d_all_counts == nullptr || out_chunks == nullptr)
@@ -242,12 +246,14 @@ mdx_status mdx_mdiscr(uint32_t n, uint32_t num_hwd_thds, const void* d_in, void*
 
 size_t mdx_segmented_workspace_size(uint64_t n, uint64_t num_segments, mdx_elem elem,
                                     uint32_t m) {
-    if (check_elem(elem) != MDX_OK || m < 1 || m > MDX_MAX_CLASSES) return 0;
+    if (check_elem(elem) != MDX_OK || elem == MDX_ELEM_REC16 || m < 1 || m > MDX_MAX_CLASSES)
+        return 0;
     return seg_layout(n, num_segments, elem, m, false).total;
 }
 
 size_t mdx_mdiscr_segm_workspace_size(uint64_t n, mdx_elem elem, uint32_t m) {
-    if (check_elem(elem) != MDX_OK || m < 1 || m > MDX_MAX_CLASSES) return 0;
+    if (check_elem(elem) != MDX_OK || elem == MDX_ELEM_REC16 || m < 1 || m > MDX_MAX_CLASSES)
+        return 0;
     return seg_layout(n, n, elem, m, true).total;
 }
 
@@ -258,6 +264,7 @@ mdx_status mdx_partition_segmented(const void* d_in, void* d_out, uint64_t n, md
                                    mdx_stream_t stream) {
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
+    if (elem == MDX_ELEM_REC16) return MDX_ERR_UNSUPPORTED;  // plain path only
     if ((s = check_discr(discr)) != MDX_OK) return s;
     if (n > MDX_MAX_ELEMS || num_segments > MDX_MAX_ELEMS) return MDX_ERR_INVALID;
     if ((s = check_io(d_in, d_out, n, elem)) != MDX_OK) return s;
@@ -283,6 +290,7 @@ mdx_status mdx_partition_segmented_multi(const void* d_in, void* d_out, uint64_t
                                          void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
+    if (elem == MDX_ELEM_REC16) return MDX_ERR_UNSUPPORTED;  // plain path only
     if (m_max < 1 || m_max > 16) return m_max > 16 ? MDX_ERR_UNSUPPORTED : MDX_ERR_INVALID;
     if (n > MDX_MAX_ELEMS || num_segments > MDX_MAX_ELEMS) return MDX_ERR_INVALID;
     if ((s = check_io(d_in, d_out, n, elem)) != MDX_OK) return s;
@@ -311,6 +319,7 @@ mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segmen
                            void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
+    if (elem == MDX_ELEM_REC16) return MDX_ERR_UNSUPPORTED;  // plain path only
     if ((s = check_discr(discr)) != MDX_OK) return s;
     if ((s = check_io(d_in, d_out, n, elem)) != MDX_OK) return s;
     if (n == 0) return MDX_OK;

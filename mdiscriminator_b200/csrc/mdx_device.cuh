@@ -28,6 +28,12 @@ constexpr uint32_t kErrCounts = 4u;  // distributed: other ranks' class counts i
 // 8-byte {key, payload} record -- ModArray<N,2>::apply = x[0] % N,
 // MdiscrHost_arrays.cu.h:33-35).
 
+// 16-byte record {u32 key; 12 bytes of payload}: ModArray<N,4> over arrays of
+// four unsigned ints (MdiscrHost_arrays.cu.h:26-36, class from x[0]).
+struct alignas(16) Rec16 {
+    uint32_t w[4];
+};
+
 template <class V>
 __host__ __device__ __forceinline__ uint32_t key_of(const V& v);
 template <>
@@ -35,6 +41,10 @@ __host__ __device__ __forceinline__ uint32_t key_of<uint32_t>(const uint32_t& v)
 template <>
 __host__ __device__ __forceinline__ uint32_t key_of<uint64_t>(const uint64_t& v) {
     return static_cast<uint32_t>(v);  // little-endian {u32 key; u32 payload}
+}
+template <>
+__host__ __device__ __forceinline__ uint32_t key_of<Rec16>(const Rec16& v) {
+    return v.w[0];
 }
 
 // class = key & (m-1): Mod4 / Mod8 (x & 3, x & 7).

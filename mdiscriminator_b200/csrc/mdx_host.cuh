@@ -44,6 +44,10 @@ template <>
 struct ElemCfg<uint64_t> {
     static constexpr int kItems = 8;  // 2048-record tiles, 16 KB
 };
+template <>
+struct ElemCfg<Rec16> {
+    static constexpr int kItems = 4;  // 1024-record tiles, 16 KB
+};
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -53,9 +57,9 @@ inline uint32_t class_bound(uint32_t m) {
     return b;
 }
 
-inline size_t elem_bytes(mdx_elem e) { return e == MDX_ELEM_REC8 ? 8 : 4; }
-inline uint32_t tile_elems(mdx_elem e) {
-    return kThreads * (e == MDX_ELEM_REC8 ? ElemCfg<uint64_t>::kItems : ElemCfg<uint32_t>::kItems);
+inline size_t elem_bytes(mdx_elem e) { return e == MDX_ELEM_REC16 ? 16 : e == MDX_ELEM_REC8 ? 8 : 4; }
+inline uint32_t tile_elems(mdx_elem e) {  // 64 bytes per thread
+    return static_cast<uint32_t>(kThreads * 64 / elem_bytes(e));
 }
 
 inline uint32_t num_tiles_of(uint64_t n, mdx_elem e) {
@@ -94,7 +98,8 @@ inline mdx_status check_discr(mdx_discr d) {
 }
 
 inline mdx_status check_elem(mdx_elem e) {
-    return (e == MDX_ELEM_U32 || e == MDX_ELEM_REC8) ? MDX_OK : MDX_ERR_INVALID;
+    return (e == MDX_ELEM_U32 || e == MDX_ELEM_REC8 || e == MDX_ELEM_REC16) ? MDX_OK
+                                                                               : MDX_ERR_INVALID;
 }
 
 // Resident CTAs per SM of a kernel, cached per (device, kernel).
@@ -176,17 +181,16 @@ inline EncodeTiledFn tensor_map_encoder() {
 inline bool make_row_map(CUtensorMap* map, const void* base, uint64_t n, size_t elem, uint32_t box_rows) {
     std::memset(map, 0, sizeof(*map));
     if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return false;
-    const uint64_t per_row = 128 / elem;
-    const uint64_t rows = n / per_row;
+    const uint64_t rows = n * elem / 128;  // whole 128-byte rows
     if (rows < box_rows) return false;
     EncodeTiledFn enc = tensor_map_encoder();
     if (enc == nullptr) return false;
-    const cuuint64_t dims[2] = {per_row, rows};
+    // the rows as 32 u32 words each, whatever the element width
+    const cuuint64_t dims[2] = {32, rows};
     const cuuint64_t strides[1] = {128};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(per_row), box_rows};
+    const cuuint32_t box[2] = {32, box_rows};
     const cuuint32_t estr[2] = {1, 1};
-    const CUtensorMapDataType dt =
-        elem == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_UINT64;
+    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_UINT32;
     return enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
@@ -316,6 +320,8 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
                                                      (16u / sizeof(V) - 1u))};
             plain_scatter_tma_kernel<V, D, M, kThreads, kStages>
                 <<<G, kThreads, smem, stream>>>(a, d, map, o);
+        } else if constexpr (sizeof(V) == 16) {
+            return MDX_ERR_UNSUPPORTED;  // no sharded 16-byte record kernels
         } else {
             // the sharded instantiation is a kernel of its own: give it the
             // shared-memory attribute too (the grid stays the count's G, the

@@ -236,6 +236,7 @@ extern "C" mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint6
                                             mdx_discr discr, uint32_t* d_sizes,
                                             uint32_t* d_headflags, mdx_stream_t stream) {
     using namespace mdx::noalloc;
+    if (elem == MDX_ELEM_REC16) return MDX_ERR_UNSUPPORTED;  // 4- and 8-byte elements here
     if (elem != MDX_ELEM_U32 && elem != MDX_ELEM_REC8) return MDX_ERR_INVALID;
     if (discr.m < 1 || discr.m > MDX_MAX_CLASSES) return MDX_ERR_INVALID;
     if (discr.kind != MDX_DISCR_MOD && discr.kind != MDX_DISCR_MASK) return MDX_ERR_INVALID;

@@ -80,6 +80,10 @@ __device__ __forceinline__ void unpack16<uint64_t>(const uint4& r, uint64_t (&e)
     e[0] = static_cast<uint64_t>(r.x) | (static_cast<uint64_t>(r.y) << 32);
     e[1] = static_cast<uint64_t>(r.z) | (static_cast<uint64_t>(r.w) << 32);
 }
+template <>
+__device__ __forceinline__ void unpack16<Rec16>(const uint4& r, Rec16 (&e)[1]) {
+    unpack16_to<Rec16>(r, e);
+}
 
 // 1 << s with the shift clamped as PTX defines it (s >= 32 gives 0), so one
 // increment is added to the right 32-bit word without a select.

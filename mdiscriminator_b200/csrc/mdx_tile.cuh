@@ -61,6 +61,10 @@ __device__ __forceinline__ void unpack16_to<uint64_t>(const uint4& r, uint64_t* 
     e[0] = static_cast<uint64_t>(r.x) | (static_cast<uint64_t>(r.y) << 32);
     e[1] = static_cast<uint64_t>(r.z) | (static_cast<uint64_t>(r.w) << 32);
 }
+template <>
+__device__ __forceinline__ void unpack16_to<Rec16>(const uint4& r, Rec16* e) {
+    e[0].w[0] = r.x; e[0].w[1] = r.y; e[0].w[2] = r.z; e[0].w[3] = r.w;
+}
 
 template <class V, int THREADS, int M>
 struct TileGeom {
@@ -161,7 +165,7 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeo
     constexpr int LR = (ITEMS + 7) / 8;
     static_assert(M <= 16 && M >= 2, "class bound");
     static_assert(M <= 2 * W, "each warp scans at most two rows");
-    static_assert(ITEMS == 16 || ITEMS == 8, "64 bytes of 4- or 8-byte elements");
+    static_assert(ITEMS == 16 || ITEMS == 8 || ITEMS == 4, "64 bytes of 4-, 8- or 16-byte elements");
     static_assert(PER == 8, "row scans load 8 entries per lane");
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

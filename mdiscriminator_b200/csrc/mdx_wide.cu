@@ -12,10 +12,11 @@
 //   3. gather:    output row p = input row (rec_out[p] >> 32), for the whole
 //                 record or for every column; the key comes from rec_out[p].
 // Traffic per row: 4 + 8 (build) + 24 (partition) + 8 + 2R (gather) bytes for
-// R bytes of row data, against 2R for a kernel specialised to the width; 4-
-// and 8-byte records take the direct paths.
+// R bytes of row data, against 2R for a kernel specialised to the width; 4-,
+// 8- and (16-byte aligned) 16-byte records take the direct record kernels.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "mdx_host.cuh"
@@ -128,7 +129,9 @@ size_t mdx_records_workspace_size(uint64_t n, uint32_t record_bytes, uint32_t m)
     if (record_bytes < 4 || record_bytes % 4 != 0 || m < 1 || m > MDX_MAX_CLASSES) return 0;
     if (record_bytes == 4) return mdx_workspace_size(n, MDX_ELEM_U32, m);
     if (record_bytes == 8) return mdx_workspace_size(n, MDX_ELEM_REC8, m);
-    return wide::layout(n, m).total;
+    const size_t gathered = wide::layout(n, m).total;  // unaligned 16-byte records use it too
+    if (record_bytes == 16) return std::max(gathered, mdx_workspace_size(n, MDX_ELEM_REC16, m));
+    return gathered;
 }
 
 mdx_status mdx_partition_records(const void* d_in, void* d_out, uint64_t n, uint32_t record_bytes,
@@ -140,6 +143,10 @@ mdx_status mdx_partition_records(const void* d_in, void* d_out, uint64_t n, uint
                              ws_bytes, stream);
     if (record_bytes == 8)
         return mdx_partition(d_in, d_out, n, MDX_ELEM_REC8, discr, d_sizes, d_headflags, d_ws,
+                             ws_bytes, stream);
+    if (record_bytes == 16 && reinterpret_cast<uintptr_t>(d_in) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(d_out) % 16 == 0)  // the 16-byte record kernels
+        return mdx_partition(d_in, d_out, n, MDX_ELEM_REC16, discr, d_sizes, d_headflags, d_ws,
                              ws_bytes, stream);
     mdx_status s = host::check_discr(discr);
     if (s != MDX_OK) return s;

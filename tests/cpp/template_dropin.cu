@@ -44,6 +44,16 @@ struct KeyRemainder {  // 8-byte records, class = key % N
     __host__ __device__ static inline unsigned int apply(volatile InType x) { return x.key % N; }
 };
 
+struct Quad {
+    unsigned int key, a, b, c;
+};
+template <unsigned N>
+struct QuadRemainder {  // 16-byte records, class = key % N
+    typedef Quad InType;
+    typedef Counts<N> TupleType;
+    __host__ __device__ static inline unsigned int apply(volatile InType x) { return x.key % N; }
+};
+
 struct Decades {  // a functor that is not a remainder: class = (x / 10) % 6
     typedef unsigned int InType;
     typedef Counts<6> TupleType;
@@ -103,7 +113,7 @@ static int plain_case(const char* name, unsigned n) {
     typedef typename D::InType T;
     std::vector<T> h(n), want;
     for (unsigned i = 0; i < n; i++) {
-        unsigned v[2] = {next_u32(), i};
+        unsigned v[4] = {next_u32(), i, next_u32(), ~i};
         std::memcpy(&h[i], v, sizeof(T));
     }
     std::vector<unsigned> wsz;
@@ -254,6 +264,8 @@ int main() {
     bad |= plain_case<Remainder<40>>("mdiscr<Remainder<40>>", 777777u);
     bad |= plain_case<Decades>("mdiscr<Decades>", 100003u);
     bad |= plain_case<KeyRemainder<16>>("mdiscr<KeyRemainder<16>>", 1000003u);
+    bad |= plain_case<QuadRemainder<7>>("mdiscr<QuadRemainder<7>>", 654321u);
+    bad |= plain_case<QuadRemainder<64>>("mdiscr<QuadRemainder<64>>", 200003u);
     bad |= segm_case<Remainder<4>>("mdiscrSegm<Remainder<4>>", 2000000u);
     bad |= segm_case<KeyRemainder<3>>("mdiscrSegm<KeyRemainder<3>>", 500000u);
     bad |= segm_case<Decades>("mdiscrSegm<Decades>", 300000u);

@@ -1,7 +1,7 @@
 """The header-only C++ drop-in (include/mdx/mdiscr.cuh): a program written
 against the reference's template signatures, with its own functors (a mask,
 remainders, a non-remainder class function, 8-byte records, arrays of LEN
-values, a three-array tuple whose class reads every field), runs the plain,
+values, 16-byte records, a three-array tuple whose class reads every field), runs the plain,
 segmented, array and tuple templates and checks them against a CPU stable
 partition."""
 import subprocess
@@ -18,4 +18,4 @@ def test_template_dropin_program(cuda_ready):
     print(res.stdout)
     assert res.returncode == 0, res.stdout + res.stderr
     assert "INVALID" not in res.stdout
-    assert res.stdout.count("VALID") == 11
+    assert res.stdout.count("VALID") == 13

@@ -53,6 +53,28 @@ def test_small_records_take_the_direct_paths(cuda_ready):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("m", [3, 16, 64])
+def test_16_byte_records_aligned_and_not(cuda_ready, m):
+    """16-byte records at a 16-byte aligned address take the 16-byte record
+    kernels; 4 bytes off that alignment they take the gathered route.  Both
+    must give the oracle's order."""
+    torch = cuda_ready
+    import mdiscriminator_b200 as mdx
+    for n in (5, 4097, 1 << 19):
+        rng = np.random.default_rng(n * m)
+        recs = rng.integers(0, 2**32, size=(n, 4), dtype=np.uint64).astype(np.uint32)
+        recs[:, 0] = oracle.fill_uniform_u32(n, n + 7 * m)
+        perm, es, _ = expected_perm(recs[:, 0], m, "mod")
+        flat = torch.from_numpy(
+            np.concatenate([np.zeros(1, np.uint32), recs.reshape(-1)]).view(np.int32)).cuda()
+        for d in (flat[1:].clone(), flat[1:]):
+            out, sizes = mdx.partition_records(d, 16, ("mod", m))
+            got = out.cpu().numpy().view(np.uint32).reshape(n, 4)
+            assert np.array_equal(got, recs[perm]), (n, d.data_ptr() % 16)
+            assert np.array_equal(sizes.cpu().numpy(), es)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("m", [4, 13])
 def test_columns_follow_the_key(cuda_ready, m):
     """The reference's tuple layout (a u32, a u8 and a bool array) plus a
@@ -90,6 +112,10 @@ def test_wide_workspace_sizes_and_validation():
     assert L.mdx_records_workspace_size(1000, 4, 5) == mdx.workspace_size(1000, mdx.ELEM_U32, 5)
     assert L.mdx_records_workspace_size(1000, 6, 5) == 0  # not a multiple of 4
     assert L.mdx_records_workspace_size(1000, 16, 65) == 0
+    # 16-byte records: plain partitions only
+    assert mdx.workspace_size(1000, mdx.ELEM_REC16, 5) > 0
+    assert L.mdx_segmented_workspace_size(1000, 10, mdx.ELEM_REC16, 5) == 0
+    assert L.mdx_mdiscr_segm_workspace_size(1000, mdx.ELEM_REC16, 5) == 0
     assert L.mdx_columns_workspace_size(1000, 0) == 0
     d = mdx.make_discr(("mod", 3))
     assert L.mdx_partition_records(None, None, 10, 6, d, None, None, None, 0, None) == mdx.MDX_ERR_INVALID
