@@ -125,6 +125,76 @@ def _gather_counts(counts_i64, group, R):
     return torch.stack(parts)
 
 
+def _handle_row(out):
+    """(offset, 8 handle words) of a tensor's allocation; zeros for none."""
+    if out is not None and out.numel() > 0:
+        h, off = ipc_handle(out)
+        return [off] + [int(w) for w in np.frombuffer(h, dtype=np.int64)]
+    return [0] * 9
+
+
+def _peer_ptrs(rows, rank, out):
+    """Device addresses of every rank's output chunk in this process (a
+    handle seen before reuses its mapping)."""
+    ptrs = []
+    for q, v in enumerate(rows):
+        hq = np.asarray(v[1:], dtype=np.int64).tobytes()
+        if q == rank:
+            ptrs.append(out.data_ptr())
+        elif not any(hq):
+            ptrs.append(0)
+        else:
+            if hq not in _peer_maps:
+                _peer_maps[hq] = ipc_open(hq, 0)
+            ptrs.append(_peer_maps[hq] + int(v[0]))
+    return ptrs
+
+
+def _partition_p2p(x_local, discr, m, group, R, rank, out, check):
+    """The "p2p" transport: count, one all-gather of a row per rank (its m
+    counts, its length, and -- when ``out`` is given -- its output chunk's
+    allocation handle and offset), one read of the gathered table on the host
+    (the call's only wait), the sharded scatter into the mapped chunks, and an
+    all-reduce as the completion barrier."""
+    import torch
+    import torch.distributed as dist
+    dev = x_local.device
+    ebytes = x_local.element_size()
+    n_local = x_local.numel()
+    ws = _workspace(max(workspace_size(max(n_local, 1), ELEM_REC8 if ebytes == 8 else 0, m), 256),
+                    dev)
+    counts = dist_count(x_local, discr, ws)
+    tail = torch.tensor([n_local] + _handle_row(out), dtype=torch.int64).pin_memory()
+    row = torch.cat([counts.to(torch.int64), tail.to(dev, non_blocking=True)])
+    parts = [torch.empty_like(row) for _ in range(R)]
+    dist.all_gather(parts, row, group=group)
+    table_dev = torch.stack(parts)
+    table = table_dev.cpu().numpy()
+    n_total = int(table[:, m].sum())
+    chunk = out_chunk_elems(n_total, R, ebytes)
+    a, b = chunk_range(rank, R, chunk, n_total)
+    rows = table[:, m + 1:]
+    if out is None:  # first call: the chunk exists only now, its handle goes round once more
+        out = torch.empty(b - a, dtype=x_local.dtype, device=dev)
+        mine = torch.tensor(_handle_row(out), dtype=torch.int64, device=dev)
+        hparts = [torch.empty_like(mine) for _ in range(R)]
+        dist.all_gather(hparts, mine, group=group)
+        rows = torch.stack(hparts).cpu().numpy()
+    elif out.numel() != b - a or out.dtype != x_local.dtype:
+        raise MdxError(MDX_ERR_INVALID, "partition_distributed: out has the wrong shape or type")
+    ptrs = _peer_ptrs(rows, rank, out)
+    dist_scatter(x_local, discr, table_dev[:, :m].to(torch.uint32), rank, ptrs, chunk, n_total, ws)
+    # completion barrier: no rank reads its chunk before every rank's stores
+    # into it have finished
+    flag = torch.zeros(1, dtype=torch.int64, device=dev)
+    dist.all_reduce(flag, group=group)
+    if check:
+        err = ws.error()
+        if err != 0:
+            raise MdxError(err, "partition_distributed")
+    return out, table[:, :m].sum(axis=0)
+
+
 def partition_distributed(x_local, discr, group=None, transport: str = "auto", out=None,
                           local_partition: Optional[Callable] = None, check: bool = True):
     """Stable partition of the array whose rank-ordered chunks the ranks of
@@ -144,6 +214,10 @@ def partition_distributed(x_local, discr, group=None, transport: str = "auto", o
     rank = dist.get_rank(group)
     dc = make_discr(discr)
     m = dc.m
+    if transport == "auto":
+        transport = "p2p" if x_local.is_cuda else "nccl"
+    if transport == "p2p":
+        return _partition_p2p(x_local, discr, m, group, R, rank, out, check)
     ebytes = x_local.element_size()
     n_local = x_local.numel()
     n_all = torch.tensor([n_local], dtype=torch.int64, device=x_local.device)
@@ -156,45 +230,6 @@ def partition_distributed(x_local, discr, group=None, transport: str = "auto", o
         out = torch.empty(b - a, dtype=x_local.dtype, device=x_local.device)
     elif out.numel() != b - a or out.dtype != x_local.dtype:
         raise MdxError(MDX_ERR_INVALID, "partition_distributed: out has the wrong shape or type")
-    if transport == "auto":
-        transport = "p2p" if x_local.is_cuda else "nccl"
-
-    if transport == "p2p":
-        elem = ELEM_REC8 if ebytes == 8 else 0
-        ws = _workspace(max(workspace_size(max(n_local, 1), elem, m), 256), x_local.device)
-        counts = dist_count(x_local, discr, ws)
-        all_counts = _gather_counts(counts.to(torch.int64), group, R)
-        # every rank's output chunk mapped into this process: one small tensor
-        # all-gather of (offset in its allocation, allocation handle); a handle
-        # seen before reuses its mapping
-        h, off = ipc_handle(out) if out.numel() > 0 else (bytes(64), 0)
-        mine = torch.tensor([off] + list(np.frombuffer(h, dtype=np.int64)), dtype=torch.int64,
-                            device=x_local.device)
-        parts = [torch.empty_like(mine) for _ in range(R)]
-        dist.all_gather(parts, mine, group=group)
-        ptrs = []
-        for q, t in enumerate(parts):
-            v = t.cpu().numpy()
-            hq = v[1:].tobytes()
-            if q == rank:
-                ptrs.append(out.data_ptr())
-            elif not any(hq):
-                ptrs.append(0)
-            else:
-                if hq not in _peer_maps:
-                    _peer_maps[hq] = ipc_open(hq, 0)
-                ptrs.append(_peer_maps[hq] + int(v[0]))
-        sizes = dist_scatter(x_local, discr, all_counts.to(torch.uint32), rank, ptrs, chunk,
-                             n_total, ws)
-        # completion barrier: no rank reads its chunk before every rank's
-        # stores into it have finished
-        flag = torch.zeros(1, dtype=torch.int64, device=x_local.device)
-        dist.all_reduce(flag, group=group)
-        if check:
-            err = ws.error()
-            if err != 0:
-                raise MdxError(err, "partition_distributed")
-        return out, sizes.to(torch.int64).cpu().numpy()
 
     if transport != "nccl":
         raise MdxError(MDX_ERR_INVALID, f"unknown transport {transport!r}")
