@@ -387,8 +387,8 @@ constexpr int kFlagsTile = 4096;
 inline uint32_t window_elems(mdx_elem e) { return tile_elems(e); }
 
 struct SegLayout {
-    size_t run_loc, grp_loc, blk_runs, blk_grps, runs, groups, groups_end, status, excl, offsets,
-        flag_status, total;
+    size_t run_loc, grp_loc, blk_runs, blk_grps, runs, groups, groups_end, run_cnt, run_base,
+        offsets, flag_status, total;
     uint64_t max_runs, max_groups;
 };
 
@@ -399,7 +399,9 @@ inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool
     const uint64_t NW = (n + P - 1) / P;
     SegLayout L;
     L.max_runs = 2 * NW + 2;    // runs of segments that tile [0, n): far fewer
-    L.max_groups = 2 * NW + 2;  // at most one group per half tile (+ trailing empty segments)
+    // a group starts at a new window of 3P/8 elements or after kGroupSegs segments
+    const uint64_t GW = 3 * P / 8;  // group_window<P>()
+    L.max_groups = (n + GW - 1) / GW + S / kGroupSegs + 2;
     L.run_loc = kHeaderBytes;
     L.grp_loc = align_up(L.run_loc + 4 * (S + 1), kAlign);
     L.blk_runs = align_up(L.grp_loc + 4 * (S + 1), kAlign);
@@ -407,9 +409,9 @@ inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool
     L.runs = align_up(L.blk_grps + 4 * kMaxPlanBlocks, kAlign);
     L.groups = align_up(L.runs + sizeof(RunEntry) * L.max_runs, kAlign);
     L.groups_end = align_up(L.groups + 4 * L.max_groups, kAlign);
-    L.status = align_up(L.groups_end + 4 * L.max_groups, kAlign);
-    L.excl = align_up(L.status + 8ull * M * L.max_runs, kAlign);
-    L.offsets = align_up(L.excl + 4ull * M * L.max_runs, kAlign);
+    L.run_cnt = align_up(L.groups_end + 4 * L.max_groups, kAlign);
+    L.run_base = align_up(L.run_cnt + 4ull * M * L.max_runs, kAlign);
+    L.offsets = align_up(L.run_base + 4ull * M * L.max_runs, kAlign);
     L.flag_status = L.offsets;
     L.total = L.offsets;
     if (flags_form) {
@@ -434,8 +436,11 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     using SL = SegSmem<V, M, kThreads, kStages>;
     constexpr int P = SL::kTile;
     auto main_fn = seg_main<V, D, M, kThreads, kStages>;
-    int blocks = 0, sms = 0;
-    if (occupancy(reinterpret_cast<const void*>(main_fn), SL::kBytes, &blocks, &sms) != cudaSuccess)
+    auto scatter_fn = seg_run_scatter<V, D, M, kThreads, kStages>;
+    int blocks = 0, sms = 0, sblocks = 0;
+    if (occupancy(reinterpret_cast<const void*>(main_fn), SL::kBytes, &blocks, &sms) != cudaSuccess ||
+        occupancy(reinterpret_cast<const void*>(scatter_fn), SL::kRunBytes, &sblocks, &sms) !=
+            cudaSuccess)
         return MDX_ERR_CUDA;
     SegArgs a;
     a.in = d_in;
@@ -455,8 +460,8 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.runs = reinterpret_cast<RunEntry*>(ws + L.runs);
     a.groups = reinterpret_cast<uint32_t*>(ws + L.groups);
     a.groups_end = reinterpret_cast<uint32_t*>(ws + L.groups_end);
-    a.status = reinterpret_cast<uint64_t*>(ws + L.status);
-    a.excl = reinterpret_cast<uint32_t*>(ws + L.excl);
+    a.run_cnt = reinterpret_cast<uint32_t*>(ws + L.run_cnt);
+    a.run_base = reinterpret_cast<uint32_t*>(ws + L.run_base);
     a.plan_blocks = plan_blocks_for(S_bound);
     a.max_runs = static_cast<uint32_t>(L.max_runs);
     a.max_groups = static_cast<uint32_t>(L.max_groups);
@@ -466,23 +471,21 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         const Tuning tun = tuning_for(sizeof(V) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_U32, M, n);
         a.run_tiles = tun.run_tiles >= 1 ? tun.run_tiles : kRunTiles;
         a.group_batch = tun.group_batch >= 1 ? tun.group_batch : kGroupBatch;
-        a.lag_slack_pct = tun.lag_slack_pct;
     }
     CUtensorMap map;
     a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::G::kRows) ? 1 : 0;
     if (d_headflags != nullptr &&
         cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), st) != cudaSuccess)
         return MDX_ERR_CUDA;
-    // Look-back words start from zero every call: the workspace's layout moves
-    // with n, S and m, so the epoch tag alone cannot tell a status word from
-    // another call's data.
-    if (cudaMemsetAsync(a.status, 0, L.max_runs * M * sizeof(uint64_t), st) != cudaSuccess)
-        return MDX_ERR_CUDA;
     if (cudaMemsetAsync(a.groups_end, 0xff, L.max_groups * sizeof(uint32_t), st) != cudaSuccess)
         return MDX_ERR_CUDA;
     seg_plan_spans<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
     seg_plan_emit<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
-    main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d, map);
+    main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d);
+    // a warp per 32 runs (the run count is on the device: enough for the capacity)
+    const uint64_t scan_blocks = std::min<uint64_t>((L.max_runs + 255) / 256, 4096);
+    seg_run_scan<M><<<static_cast<uint32_t>(scan_blocks), 256, 0, st>>>(a);
+    scatter_fn<<<static_cast<uint32_t>(sblocks) * sms, kThreads, SL::kRunBytes, st>>>(a, d, map);
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
 }
 

@@ -3,43 +3,39 @@
 // Replaces mdiscrSegm<DISCR> (cuda_code/MdiscrSegmHost.cu.h:36-230: a chain
 // of ~12 kernels -- segmented scans of head flags and of N one-hot m-tuples,
 // per-element reductions, class offsets, indices, permute, sizes -- with nine
-// N-sized temporaries, four of them N*m tuples) by three launches:
+// N-sized temporaries, four of them N*m tuples) by five launches:
 //
 //   seg_plan_spans  per segment: its length.  Segments longer than one tile
 //                   (P elements) are "large" and are cut into runs of up to
 //                   RUN_TILES tiles; the other ("small") segments are grouped
-//                   by the tile their first element falls in (a group spans
-//                   at most 2P elements).  Block-local scans of the run and
-//                   group counts; the last CTA scans the block totals and
-//                   records the counts, the largest number of runs of one
-//                   segment (the lag below) and a new look-back epoch, and
-//                   resets the persistent kernel's ticket.
+//                   (consecutive small segments starting in one window of
+//                   3P/8 elements, at most kGroupSegs of them).  Block-local
+//                   scans of the run and group counts; the last CTA scans the
+//                   block totals, records the counts and resets the tickets.
 //   seg_plan_emit   writes the run entries {segment, [p0, p1), last run of
 //                   the segment} and the group heads, in element order.
-//   seg_main        one persistent launch.  CTAs take tickets in order, a
-//                   ticket only when the CTA is ready to work on it:
-//                     * batches of small-segment groups: each group's range is
-//                       read into shared memory by one bulk copy (the next
-//                       group's copy overlaps the current group's work), warps
-//                       partition one segment each (lanes own odd-stride
-//                       contiguous sub-ranges: per-lane 16-bit class counters,
-//                       a warp scan, a second pass places the elements) into a
-//                       shared output image, and the CTA writes the range back
-//                       with 16-byte stores -- one HBM read and one write per
-//                       element;
-//                     * then, per run j of a large segment, a count item C(j)
-//                       (class counts of the run with 16-byte loads, published
-//                       to epoch-tagged per-class status words; decoupled
-//                       look-back over the segment's earlier runs gives the
-//                       run's exclusive prefix, the last run gives the
-//                       segment's class totals) and a scatter item S(j) (the
-//                       run's tiles through a TMA ring and tile_scatter).
-//                       S(j) is issued D tickets after C(j), D = the most runs
-//                       of one segment, so it waits only on earlier tickets (no
-//                       deadlock) and re-reads its run from L2.
+//   seg_main        persistent; CTAs take tickets in order:
+//                     * batches of groups: each group's range is read into
+//                       shared memory by one bulk copy (the next group's copy
+//                       overlaps the current group's work) and partitioned by
+//                       the whole CTA (seg_group_cta: every thread owns ~L/256
+//                       consecutive elements whatever the segment lengths; a
+//                       segmented scan of per-thread class counts, the
+//                       segments' class bases in shared memory) into a shared
+//                       output image written back with 16-byte stores -- one
+//                       HBM read and one write per element;
+//                     * then the class counts of every run (16-byte loads).
+//   seg_run_scan    per large segment (a warp, lanes over its runs): the
+//                   runs' exclusive class prefixes, the segment's sizes and
+//                   head flags, and every run's output position per class.
+//   seg_run_scatter persistent; the runs in reverse order through a TMA ring
+//                   and tile_scatter (as the plain scatter), from those
+//                   positions.
 //
-// Every wait is bounded (kWaitLimitNs); a wait that runs out latches
-// kErrTimeout and publishes what it has so no other CTA waits forever.
+// The partition kernels wait on no other CTA, only on their own bulk copies;
+// the head-flag converter below waits on earlier tiles (decoupled look-back).
+// Every wait is bounded by kWaitLimitNs; one that runs out latches
+// kErrTimeout and publishes what it has, so no other CTA waits forever.
 //
 // Output per segment equals seqMdiscr (SeqMdiscr.h:10-57) applied to the
 // segment, which is exactly what MdiscrSegmTest.cu:8-41 validates; sizes are
@@ -60,7 +56,7 @@ namespace mdx {
 // Defaults of the run-time knobs (the autotuner may choose others):
 constexpr int kRunTiles = 8;     // tiles per run of a large segment
 constexpr int kGroupBatch = 8;   // small-segment groups per work item (pipelined)
-constexpr int kLagSlackPct = 50; // extra lag of scatter items, in % of the grid
+constexpr int kLagSlackPct = 50; // accepted in the tuning table, no longer used
 
 // status word: [63:34] epoch (30 bits), [33:32] state, [31:0] count
 constexpr uint64_t kStAgg = 1ull;
@@ -77,15 +73,16 @@ struct SegHeader {      // lives at the start of the segmented workspace
     uint32_t error;     // latched error bits
     uint32_t epoch;     // look-back epoch of the current call (1 .. 2^30-1)
     uint32_t num_runs;  // large-segment runs this call
-    uint32_t lag;       // most runs of one segment (max over the planner's blocks)
+    uint32_t lag;       // unused
     uint32_t plan_done; // planner CTA ticket
     uint64_t num_segs;  // S (written by the flags converter for the head-flag form)
-    uint32_t lag_cur;   // lag of the current call (snapshot taken by the planner)
+    uint32_t lag_cur;   // unused
     uint32_t flags_ticket;  // tile ticket of the flags converter
     uint32_t flags_done;    // finished tiles of the flags converter
     uint32_t flags_epoch;   // look-back epoch of the flags converter
     uint32_t num_groups;    // small-segment groups this call
-    uint32_t pad[3];
+    uint32_t ticket2;       // run-scatter ticket counter (reset by the planner)
+    uint32_t pad[2];
 };
 
 struct RunEntry {       // a run of up to run_tiles tiles of one large segment
@@ -113,8 +110,8 @@ struct SegArgs {
     uint32_t* groups;          // [max_groups] first segment of each group
     uint32_t* groups_end;      // [max_groups] one past its last segment (0xffffffff: none
                                // marked, the group runs to S; reset every call)
-    uint64_t* status;          // [max_runs][M]
-    uint32_t* excl;            // [max_runs][M] exclusive prefix of each run
+    uint32_t* run_cnt;         // [max_runs][M] class counts of each run
+    uint32_t* run_base;        // [max_runs][M] output position of each run's first element per class
     uint32_t plan_blocks;
     uint32_t max_runs;         // capacity (enough for segments that tile [0, n))
     uint32_t max_groups;
@@ -124,7 +121,6 @@ struct SegArgs {
     uint32_t m_bound;          // classes of any segment are < m_bound (per-segment m clamped)
     uint32_t run_tiles;        // tiles per run of a large segment
     uint32_t group_batch;      // small-segment groups per work item
-    uint32_t lag_slack_pct;    // extra lag of scatter items, in % of the grid
 };
 
 // The discriminator of segment s: the launch's, or -- when the call carries
@@ -142,6 +138,20 @@ __device__ __forceinline__ D seg_discr(const SegArgs& a, const D& d, uint64_t s)
 
 constexpr uint64_t kSegsOnDevice = ~0ull;
 
+// Small segments are grouped: a group is a run of consecutive small segments
+// whose first elements lie in one window of 3P/8 elements, cut after at most
+// kGroupSegs segments, so a group spans < 3P/8 + P elements.
+constexpr uint32_t kGroupSegs = 128;
+template <int P>
+__host__ __device__ constexpr uint64_t group_window() {
+    return 3ull * P / 8ull;
+}
+template <int P>
+__device__ __forceinline__ bool group_head(const SegArgs& a, uint64_t s, uint64_t a0) {
+    constexpr uint64_t GW = group_window<P>();
+    return s == 0 || a.offsets[s - 1] / GW != a0 / GW || (s % kGroupSegs) == 0;
+}
+
 __device__ __forceinline__ uint64_t seg_count(const SegArgs& a) {
     return a.num_segs == kSegsOnDevice ? a.hdr->num_segs : a.num_segs;
 }
@@ -158,7 +168,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
     const uint64_t G = gridDim.x;
     const uint64_t R = (S + G - 1) / G;
     const uint64_t s0 = blockIdx.x * R, s1 = min(s0 + R, S);
-    uint32_t carry_r = 0, carry_g = 0, maxruns = 0;
+    uint32_t carry_r = 0, carry_g = 0;
     for (uint64_t base = s0; base < s1; base += THREADS) {
         const uint64_t s = base + tid;
         uint32_t runs = 0, head = 0;
@@ -170,7 +180,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
                 const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
                 runs = (span + a.run_tiles - 1) / a.run_tiles;
             } else {
-                head = (s == 0 || a.offsets[s - 1] / (P / 2) != a0 / (P / 2)) ? 1u : 0u;
+                head = group_head<P>(a, s, a0) ? 1u : 0u;
             }
             if (a.in_flags != nullptr && a1 > a0 && a1 <= a.n &&
                 static_cast<uint64_t>(a.in_flags[a0]) != a1 - a0)
@@ -178,7 +188,6 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
             if (a.seg_m != nullptr && (a.seg_m[s] < 1u || a.seg_m[s] > a.m_bound))
                 atomicOr(&a.hdr->error, kErrSegments);
         }
-        maxruns = max(maxruns, runs);
         const uint32_t ir = warp_incl_scan(runs);
         const uint32_t ig = warp_incl_scan(head);
         if (lane == 31) {
@@ -202,8 +211,6 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         carry_g += tg;
         __syncthreads();
     }
-    for (int d = 16; d > 0; d >>= 1) maxruns = max(maxruns, __shfl_xor_sync(0xffffffffu, maxruns, d));
-    if (lane == 0 && maxruns > 0) atomicMax(&a.hdr->lag, maxruns);
     if (tid == 0) {
         a.blk_runs[blockIdx.x] = carry_r;
         a.blk_grps[blockIdx.x] = carry_g;
@@ -228,8 +235,6 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         if (lane == 0) {
             if (warp == 0) {
                 a.hdr->num_runs = run <= a.max_runs ? run : 0u;  // over capacity: malformed
-                a.hdr->lag_cur = a.hdr->lag;  // every block's atomicMax preceded its ticket
-                a.hdr->lag = 0u;
             } else {
                 a.hdr->num_groups = run <= a.max_groups ? run : 0u;
             }
@@ -241,6 +246,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         if (e >= (1u << 30) || e == 0u) e = 1u;
         a.hdr->epoch = e;
         a.hdr->ticket = 0u;
+        a.hdr->ticket2 = 0u;
         a.hdr->plan_done = 0u;
         // head-flag converter state for its next call
         a.hdr->flags_ticket = 0u;
@@ -292,7 +298,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
                         list_pos[q] = pos;
                         list_runs[q] = nr;
                     }
-                } else if (s == 0 || a.offsets[s - 1] / (P / 2) != a0 / (P / 2)) {
+                } else if (group_head<P>(a, s, a0)) {
                     const uint32_t g = goff + a.grp_loc[s];
                     if (g < num_groups) a.groups[g] = static_cast<uint32_t>(s);
                 }
@@ -300,7 +306,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
             // the group before segment s ends at s at the latest when s starts
             // a group, is large or is malformed
             const bool small_ok = (a1 >= a0 && a1 <= a.n && a1 - a0 <= static_cast<uint64_t>(P));
-            const bool is_head = small_ok && (s == 0 || a.offsets[s - 1] / (P / 2) != a0 / (P / 2));
+            const bool is_head = small_ok && group_head<P>(a, s, a0);
             const uint32_t before = goff + a.grp_loc[s];  // groups starting before s
             if ((is_head || !small_ok) && before >= 1u && before - 1u < num_groups)
                 atomicMin(&a.groups_end[before - 1u], static_cast<uint32_t>(s));
@@ -332,15 +338,19 @@ struct SegSmem {
     using G = TileGeom<V, THREADS, M>;
     static constexpr int kTile = G::kTile;  // == P
     static constexpr uint32_t kAU = G::kAU;
-    // small groups (segments starting in one half-tile window, each <= P):
-    // two input buffers (one being filled by TMA) and an output image, each
-    // for a range of <= P/2 + P elements plus 16-byte alignment slack
-    static constexpr int kGroupElems = kTile / 2 + kTile + 2 * static_cast<int>(kAU);
+    // small groups (segments starting in one window of 3P/8, each <= P): two
+    // input buffers (one being filled by a bulk copy) and an output image, each
+    // for a range of < 3P/8 + P elements plus 16-byte alignment slack
+    static constexpr int kGroupElems =
+        static_cast<int>(group_window<kTile>()) + kTile + 2 * static_cast<int>(kAU);
     static constexpr size_t kGroupBytes = 3ull * kGroupElems * sizeof(V);
-    // runs: TMA ring + tile stage + count matrix
+    static constexpr size_t kBytes = 128 + kGroupBytes;  // seg_main
+    // elements per thread in a group (odd: the threads' strided shared-memory
+    // reads fall in different banks)
+    static constexpr int kGroupItems = ((kGroupElems + 255) / 256) | 1;
+    // seg_run_scatter: TMA ring + tile stage + count matrix
     static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
-    static constexpr size_t kRunBytes = kRingBytes + G::kStageBytes + G::kCntBytes;
-    static constexpr size_t kBytes = 1024 + (kGroupBytes > kRunBytes ? kGroupBytes : kRunBytes);
+    static constexpr size_t kRunBytes = 1024 + kRingBytes + G::kStageBytes + G::kCntBytes;
 };
 
 // Bounded spin on a status word until it carries this epoch with state >=
@@ -380,91 +390,253 @@ struct HalfCounts {
     }
 };
 
-// One warp partitions one segment held in shared memory (element e at
-// src[e], 0 <= e < L <= 2P) into the shared output image dst[0 .. L) and
-// writes the segment's sizes.  Lane l owns the contiguous elements
-// [l*k, (l+1)*k) with k odd (so the 32 lanes read 32 different banks):
-// pass 1 counts them, a warp scan of the counters gives every lane its
-// per-class prefix (stable: lane order = input order) and the segment's
-// class offsets, pass 2 places them.
-template <class V, class D, int M>
-__device__ void seg_small_warp(const SegArgs& a, const D& d, uint64_t s, uint64_t a0, uint32_t L,
-                               const V* src, V* dst) {
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t k = (L + 31u) >> 5;
-    k |= 1u;  // odd stride
-    const uint32_t b = min(lane * k, L), e1 = min(b + k, L);
-    HalfCounts<M> cnt;
-    cnt.zero();
-    for (uint32_t e = b; e < e1; e++) cnt.inc(d(src[e]));
-    // warp inclusive scan of the packed counters
-    HalfCounts<M> incl = cnt;
+// Shared state of one group partition (at most kGroupSegs non-empty
+// segments).
+template <int M, int THREADS>
+struct GroupScratch {
+    static constexpr int NW = HalfCounts<M>::NW;
+    uint32_t base[kGroupSegs][NW];  // class bases of each non-empty segment (u16 pairs)
+    uint32_t wagg[THREADS / 32][NW + 1];
+    uint16_t hpos[kGroupSegs + 1];  // head of each non-empty segment in the group; [nseg] = L
+    uint16_t sidx[kGroupSegs];      // its index - h
+    uint8_t msz[kGroupSegs];        // its class count (per-segment m)
+    uint8_t start_ord[THREADS];     // the non-empty segment holding each thread's first element
+};
+
+// The discriminator of a group's segment with class count m: per-segment
+// remainders use the precomputed constants cmod[m] (DiscrMod::make).
+template <class D>
+__device__ __forceinline__ D group_discr(const SegArgs& a, const D& d, const uint64_t* cmod,
+                                         uint32_t m) {
+    if constexpr (std::is_same<D, DiscrMod>::value) {
+        if (a.seg_m != nullptr) {
+            DiscrMod x;
+            x.c = cmod[m];
+            x.m = m;
+            return x;
+        }
+    }
+    return d;
+}
+
+// One CTA partitions one group of small segments held in shared memory
+// (element x of the group at src[x], 0 <= x < L) into the output image
+// dst[0 .. L) and writes the segments' sizes.  Every thread owns k <= ITEMS
+// consecutive elements whatever the segment lengths:
+//   P0  one thread per segment: ordinals of the non-empty segments, their
+//       heads, and the segment holding each thread's first element;
+//   P1  classes (kept as nibbles) and the class counts of the fragment after
+//       the thread's last segment head;
+//   P2  a segmented exclusive scan of those counts over the threads gives the
+//       counts of the thread's first segment before its first element;
+//   P3  the thread in which a segment ends has its class totals: it writes the
+//       segment's class bases (shared) and sizes / head flags (global);
+//   P4  every element goes to head + base[class] + its rank in the segment.
+template <class V, class D, int M, int THREADS, int ITEMS>
+__device__ void seg_group_cta(const SegArgs& a, const D& d, const uint64_t* cmod, uint32_t h,
+                              uint32_t he, uint64_t r0, uint32_t L, const V* src, V* dst,
+                              GroupScratch<M, THREADS>& gs) {
+    using HC = HalfCounts<M>;
+    constexpr int NW = HC::NW;
+    constexpr int W = THREADS / 32;
+    constexpr int CW = (ITEMS + 7) / 8;  // nibble words
+    static_assert(static_cast<int>(kGroupSegs) <= THREADS, "one thread per segment");
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t k = ((L + THREADS - 1) / THREADS) | 1u;  // <= ITEMS
+    const uint32_t lo = min(tid * k, L), hi = min(lo + k, L);
+
+    // ---- P0
+    const uint64_t sg = static_cast<uint64_t>(h) + tid;
+    uint32_t ne = 0, x0 = 0, x1 = 0, ms = a.m;
+    if (sg < he && tid < static_cast<int>(kGroupSegs)) {
+        const uint64_t o0 = a.offsets[sg], o1 = a.offsets[sg + 1];
+        x0 = static_cast<uint32_t>(o0 - r0);
+        x1 = static_cast<uint32_t>(o1 - r0);
+        ne = (o1 > o0 && o0 >= r0 && x1 <= L) ? 1u : 0u;
+        if (a.seg_m != nullptr) ms = min(max(a.seg_m[sg], 1u), a.m_bound);
+        if (o1 == o0 && a.seg_sizes != nullptr)
+            for (uint32_t c = 0; c < a.m; c++) a.seg_sizes[sg * a.m + c] = 0u;
+    }
+    const uint32_t incl = warp_incl_scan(ne);
+    if (lane == 31) gs.wagg[warp][0] = incl;
+    __syncthreads();
+    uint32_t before = 0, nseg = 0;
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+        const uint32_t x = gs.wagg[w][0];
+        before += w < warp ? x : 0u;
+        nseg += x;
+    }
+    if (ne) {
+        const uint32_t q = before + incl - 1u;
+        gs.hpos[q] = static_cast<uint16_t>(x0);
+        gs.sidx[q] = static_cast<uint16_t>(tid);
+        gs.msz[q] = static_cast<uint8_t>(ms);
+        for (uint32_t t = (x0 + k - 1u) / k; t * k < x1 && t < static_cast<uint32_t>(THREADS); t++)
+            gs.start_ord[t] = static_cast<uint8_t>(q);
+    }
+    if (tid == 0) gs.hpos[nseg] = static_cast<uint16_t>(L);
+    __syncthreads();
+
+    // ---- P1
+    const bool active = lo < hi && nseg > 0;
+    const uint32_t q0 = active ? min(static_cast<uint32_t>(gs.start_ord[tid]), nseg - 1u) : 0u;
+    const bool head_at_lo = active && gs.hpos[q0] == lo;
+    uint32_t cls[CW];
+#pragma unroll
+    for (int w = 0; w < CW; w++) cls[w] = 0;
+    HC tail;
+    tail.zero();
+    bool inner = false;  // a segment head in (lo, hi)
+    if (active) {
+        uint32_t q = q0, nxt = gs.hpos[q0 + 1];
+        D dc = group_discr(a, d, cmod, gs.msz[q0]);
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t x = lo + i;
+            if (x < hi) {
+                if (x == nxt) {
+                    inner = true;
+                    tail.zero();
+                    q++;
+                    nxt = gs.hpos[q + 1];
+                    dc = group_discr(a, d, cmod, gs.msz[q]);
+                }
+                const uint32_t c = dc(src[x]);
+                cls[i >> 3] |= c << (4 * (i & 7));
+                tail.inc(c);
+            }
+        }
+    }
+
+    // ---- P2: segmented exclusive scan of (reset, counts) over the threads
+    uint32_t f = (head_at_lo || inner) ? 1u : 0u;
+    HC v = tail;
 #pragma unroll
     for (int dd = 1; dd < 32; dd <<= 1) {
+        const uint32_t fu = __shfl_up_sync(0xffffffffu, f, dd);
+        HC vu;
 #pragma unroll
-        for (int q = 0; q < HalfCounts<M>::NW; q++) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl.w[q], dd);
-            if (lane >= static_cast<uint32_t>(dd)) incl.w[q] += y;
+        for (int w = 0; w < NW; w++) vu.w[w] = __shfl_up_sync(0xffffffffu, v.w[w], dd);
+        if (lane >= dd) {
+            if (!f) {
+#pragma unroll
+                for (int w = 0; w < NW; w++) v.w[w] += vu.w[w];
+            }
+            f |= fu;
         }
     }
-    // segment totals (lane 31's inclusive) -> class offsets
-    HalfCounts<M> tot;
+    if (lane == 31) {
+        gs.wagg[warp][0] = f;
 #pragma unroll
-    for (int q = 0; q < HalfCounts<M>::NW; q++) tot.w[q] = __shfl_sync(0xffffffffu, incl.w[q], 31);
-    HalfCounts<M> base;  // class offset + this lane's exclusive prefix, per class
-    base.zero();
-    uint32_t off = 0;
-#pragma unroll
-    for (int c = 0; c < M; c++) {
-        const uint32_t t = tot.get(c);
-        const uint32_t mine = incl.get(c) - cnt.get(c) + off;
-        base.w[c >> 1] |= mine << ((c & 1) << 4);
-        if (static_cast<uint32_t>(c) == lane) {
-            if (a.seg_sizes != nullptr && static_cast<uint32_t>(c) < a.m) a.seg_sizes[s * a.m + c] = t;
-            if (a.headflags != nullptr && t > 0) a.headflags[a0 + off] = t;
-        }
-        off += t;
+        for (int w = 0; w < NW; w++) gs.wagg[warp][1 + w] = v.w[w];
     }
-    for (uint32_t e = b; e < e1; e++) {
-        const V v = src[e];
-        const uint32_t c = d(v);
-        dst[base.get(c)] = v;
-        base.inc(c);
+    const uint32_t fe = __shfl_up_sync(0xffffffffu, f, 1);
+    HC ve;
+#pragma unroll
+    for (int w = 0; w < NW; w++) ve.w[w] = __shfl_up_sync(0xffffffffu, v.w[w], 1);
+    __syncthreads();
+    HC carry;
+    carry.zero();
+    for (int w = 0; w < warp; w++) {
+        const bool fw = gs.wagg[w][0] != 0u;
+#pragma unroll
+        for (int q = 0; q < NW; q++) carry.w[q] = (fw ? 0u : carry.w[q]) + gs.wagg[w][1 + q];
+    }
+    if (lane > 0) {
+#pragma unroll
+        for (int q = 0; q < NW; q++) carry.w[q] = (fe ? 0u : carry.w[q]) + ve.w[q];
+    }
+    if (head_at_lo) carry.zero();
+
+    // ---- P3
+    if (active) {
+        uint32_t q = q0, nxt = gs.hpos[q0 + 1];
+        HC run = carry;
+        auto close = [&](uint32_t qq) {  // segment qq ends here; `run` holds its totals
+            const uint64_t s = static_cast<uint64_t>(h) + gs.sidx[qq];
+            const uint64_t xh = r0 + gs.hpos[qq];
+            uint32_t off = 0;
+            uint32_t bw[NW];
+#pragma unroll
+            for (int w = 0; w < NW; w++) bw[w] = 0;
+#pragma unroll
+            for (int c = 0; c < M; c++) {
+                const uint32_t t = run.get(c);
+                bw[c >> 1] |= off << (16 * (c & 1));
+                if (a.seg_sizes != nullptr && static_cast<uint32_t>(c) < a.m)
+                    a.seg_sizes[s * a.m + c] = t;
+                if (a.headflags != nullptr && t > 0) a.headflags[xh + off] = t;
+                off += t;
+            }
+#pragma unroll
+            for (int w = 0; w < NW; w++) gs.base[qq][w] = bw[w];
+        };
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t x = lo + i;
+            if (x < hi) {
+                if (x == nxt) {
+                    close(q);
+                    run.zero();
+                    q++;
+                    nxt = gs.hpos[q + 1];
+                }
+                run.inc((cls[i >> 3] >> (4 * (i & 7))) & 15u);
+            }
+        }
+        if (hi == nxt) close(q);
+    }
+    __syncthreads();
+
+    // ---- P4
+    if (active) {
+        uint32_t q = q0, nxt = gs.hpos[q0 + 1], xh = gs.hpos[q0];
+        HC bs, run = carry;
+#pragma unroll
+        for (int w = 0; w < NW; w++) bs.w[w] = gs.base[q0][w];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const uint32_t x = lo + i;
+            if (x < hi) {
+                if (x == nxt) {
+                    q++;
+                    xh = x;
+                    nxt = gs.hpos[q + 1];
+#pragma unroll
+                    for (int w = 0; w < NW; w++) bs.w[w] = gs.base[q][w];
+                    run.zero();
+                }
+                const uint32_t c = (cls[i >> 3] >> (4 * (i & 7))) & 15u;
+                const uint32_t pos = xh + bs.get(c) + run.get(c);
+                run.inc(c);
+                if (pos < L) dst[pos] = src[x];
+            }
+        }
     }
 }
 
 template <class V, class D, int M, int THREADS, int STAGES>
 __global__ void __launch_bounds__(THREADS, 3)
-    seg_main(SegArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
+    seg_main(SegArgs a, D d) {
     using L = SegSmem<V, M, THREADS, STAGES>;
-    using TG = typename L::G;
-    constexpr int ITEMS = TG::kItems;
-    constexpr int P = L::kTile;
-    constexpr int ROWS = TG::kRows;
     constexpr uint32_t AU = L::kAU;
     constexpr int W = THREADS / 32;
     static_assert(M <= 16 && M >= 2, "class bound");
-    static_assert(ROWS <= 256, "TMA box height");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const uint32_t raw = smem_addr(smem_raw);
-    unsigned char* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    // small groups
+    unsigned char* base = smem_raw + (((raw + 127u) & ~127u) - raw);
     V* g_in0 = reinterpret_cast<V*>(base);
     V* g_out = g_in0 + 2 * L::kGroupElems;
-    // runs (aliases the group buffers)
-    V* ring = reinterpret_cast<V*>(base);
-    V* stage = reinterpret_cast<V*>(base + L::kRingBytes);
-    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(base + L::kRingBytes + TG::kStageBytes);
 
-    __shared__ __align__(8) uint64_t bars[STAGES];
     __shared__ __align__(8) uint64_t gbars[2];
-    __shared__ TileShared<M> sh;
     __shared__ uint32_t ticket_sh[2];
-    __shared__ uint32_t gi_h[2], gi_he[2], gi_next[2];  // group pipeline slots
+    __shared__ uint32_t gi_h[2], gi_he[2];  // group pipeline slots
     __shared__ uint64_t gi_r0[2], gi_r1[2], gi_as[2], gi_tail[2];
     __shared__ uint32_t red[W][M];
-    __shared__ int fail_sh;
+    __shared__ GroupScratch<M, THREADS> gs;
+    __shared__ uint64_t cmod[17];  // DiscrMod constants for m = 1 .. 16
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const V* in = static_cast<const V*>(a.in);
@@ -473,32 +645,22 @@ __global__ void __launch_bounds__(THREADS, 3)
         static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
     const bool in_vec = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
     const bool out_vec = (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
-    const bool tma_ok = a.use_tma != 0;
     const uint64_t S = seg_count(a);
-    const uint32_t epoch = a.hdr->epoch;
     const uint32_t num_runs = a.hdr->num_runs;
     const uint32_t num_groups = a.hdr->num_groups;
-    // S(j) trails C(j) by the most runs of one segment (so it only waits on
-    // earlier tickets) plus half a grid of slack (so those are mostly done)
-    const uint32_t lag =
-        min(max(a.hdr->lag_cur, 1u) + gridDim.x * a.lag_slack_pct / 100u, max(num_runs, 1u));
     const uint32_t num_batches = (num_groups + a.group_batch - 1) / a.group_batch;
-    const uint32_t total = num_batches + 2u * num_runs;
-    uint32_t ring_uses = 0;   // mbarrier phase bookkeeping across items
+    const uint32_t total = num_batches + num_runs;
     uint32_t group_uses = 0;
 
     if (tid == 0) {
-#pragma unroll
-        for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
         mbar_init(&gbars[0], 1);
         mbar_init(&gbars[1], 1);
         mbar_fence_init();
     }
+    if (tid >= 1 && tid <= 16) cmod[tid] = DiscrMod::make(static_cast<uint32_t>(tid)).c;
+    if (tid == 0) cmod[0] = 0;
     __syncthreads();
 
-    // A ticket is taken only when the CTA is ready to work on it: a ticket held
-    // while its CTA waits on another item would delay every item that waits on
-    // it in turn.
     for (uint32_t it = 0;; it++) {
         if (tid == 0) ticket_sh[it & 1u] = atomicAdd(&a.hdr->ticket, 1u);
         __syncthreads();
@@ -523,7 +685,6 @@ __global__ void __launch_bounds__(THREADS, 3)
                 if (!in_vec || ve < as) ve = as;
                 gi_h[slot] = h;
                 gi_he[slot] = he;
-                gi_next[slot] = h;
                 gi_r0[slot] = r0;
                 gi_r1[slot] = r1;
                 gi_as[slot] = as;
@@ -556,16 +717,9 @@ __global__ void __launch_bounds__(THREADS, 3)
                     break;
                 }
                 if (tid == 0 && i + 1 < gcnt) issue_group(i + 1);  // the other buffer is free
-                const uint32_t he = gi_he[slot];
-                for (;;) {
-                    uint32_t s = 0;
-                    if (lane == 0) s = atomicAdd(&gi_next[slot], 1u);
-                    s = __shfl_sync(0xffffffffu, s, 0);
-                    if (s >= he) break;
-                    const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
-                    seg_small_warp<V, D, M>(a, seg_discr(a, d, s), s, a0, static_cast<uint32_t>(a1 - a0),
-                                            gin + (a0 - as), g_out + (a0 - as));
-                }
+                seg_group_cta<V, D, M, THREADS, L::kGroupItems>(
+                    a, d, cmod, gi_h[slot], gi_he[slot], r0, static_cast<uint32_t>(r1 - r0),
+                    gin + (r0 - as), g_out + (r0 - as), gs);
                 __syncthreads();
                 // write the range back from the output image
                 if (out_vec && out_phase == 0u) {
@@ -593,33 +747,11 @@ __global__ void __launch_bounds__(THREADS, 3)
             continue;
         }
 
-        // ---------------- runs of large segments ----------------
-        const uint32_t u = t - num_batches;
-        uint32_t j;
-        bool is_count;
-        if (u < lag) {
-            j = u;
-            is_count = true;
-        } else {
-            const uint32_t v = u - lag;
-            const uint32_t pairs = num_runs - lag;
-            if (v < 2u * pairs) {
-                is_count = (v & 1u) != 0u;
-                j = is_count ? lag + (v >> 1) : (v >> 1);
-            } else {
-                is_count = false;
-                j = pairs + (v - 2u * pairs);
-                if (lag >= num_runs) j = num_runs - 1u - j;  // all counts first: walk back (L2)
-            }
-        }
+        // ---------------- class counts of run j of a large segment ----------
+        const uint32_t j = t - num_batches;
         const RunEntry ent = a.runs[j];
-        const uint64_t seg_start = a.offsets[ent.seg];
         const D dj = seg_discr(a, d, ent.seg);
-        const bool first_run = (ent.p0 == static_cast<uint32_t>(seg_start));
-        const bool last_run = (j == ent.jlast);
-
-        if (is_count) {
-            // ---------------- C(j): class counts of the run + look-back ----
+        {
             PackedCounts<M> pc;
             pc.init();
             const uint64_t p0 = ent.p0, p1 = ent.p1;
@@ -671,79 +803,139 @@ __global__ void __launch_bounds__(THREADS, 3)
                 if (lane == 0) red[warp][c] = x;
             }
             __syncthreads();
-            if (warp == 0) {
-                const uint32_t c = lane;
-                const bool cls = c < static_cast<uint32_t>(M);
+            if (tid < M) {
                 uint32_t agg = 0;
-                if (cls)
-                    for (int w = 0; w < W; w++) agg += red[w][c];
-                uint64_t* st = a.status + static_cast<uint64_t>(j) * M;
-                uint32_t prefix = 0;
-                bool ok = true;
-                if (cls) {
-                    if (first_run) {
-                        a.excl[static_cast<uint64_t>(j) * M + c] = 0u;
-                        __threadfence();
-                        st_release_u64(st + c, st_pack(epoch, kStInc, agg));
-                    } else {
-                        st_release_u64(st + c, st_pack(epoch, kStAgg, agg));
-                        // decoupled look-back over this segment's earlier runs
-                        for (uint32_t jj = j - 1u;; jj--) {
-                            uint64_t w;
-                            if (!wait_status(a.status + static_cast<uint64_t>(jj) * M + c, epoch,
-                                             kStAgg, w)) {
-                                ok = false;
-                                break;
-                            }
-                            prefix += static_cast<uint32_t>(w);
-                            if (st_state(w) == kStInc) break;
-                        }
-                        a.excl[static_cast<uint64_t>(j) * M + c] = prefix;
-                        __threadfence();
-                        st_release_u64(st + c, st_pack(epoch, kStInc, prefix + agg));
-                    }
-                }
-                if (__any_sync(0xffffffffu, !ok) && lane == 0) atomicOr(&a.hdr->error, kErrTimeout);
-                if (last_run) {
-                    // segment totals -> sizes (tuple and head-flag forms)
-                    const uint32_t tot = cls ? prefix + agg : 0u;
-                    const uint32_t incl = warp_incl_scan(tot);
-                    if (cls) {
-                        if (a.seg_sizes != nullptr && c < a.m)
-                            a.seg_sizes[static_cast<uint64_t>(ent.seg) * a.m + c] = tot;
-                        if (a.headflags != nullptr && tot > 0)
-                            a.headflags[seg_start + incl - tot] = tot;
-                    }
-                }
+                for (int w = 0; w < W; w++) agg += red[w][tid];
+                a.run_cnt[static_cast<uint64_t>(j) * M + tid] = agg;
             }
-            __syncthreads();
-            continue;
         }
+    }
+}
 
-        // ---------------- S(j): scatter the run ----------------
-        if (warp == 0) {
-            const uint32_t c = lane;
-            bool ok = true;
-            uint32_t tot = 0, pre = 0;
-            if (c < static_cast<uint32_t>(M)) {
-                uint64_t w;
-                ok = wait_status(a.status + static_cast<uint64_t>(ent.jlast) * M + c, epoch, kStInc, w);
-                tot = static_cast<uint32_t>(w);
-                uint64_t w2;
-                ok = wait_status(a.status + static_cast<uint64_t>(j) * M + c, epoch, kStInc, w2) && ok;
-                pre = __ldcg(a.excl + static_cast<uint64_t>(j) * M + c);
-            }
-            const uint32_t incl = warp_incl_scan(tot);
-            if (c < static_cast<uint32_t>(M))
-                sh.cursor[0][c] = static_cast<uint32_t>(seg_start) + (incl - tot) + pre;
-            const bool bad = __any_sync(0xffffffffu, !ok);
-            if (lane == 0) {
-                fail_sh = bad ? 1 : 0;
-                if (bad) atomicOr(&a.hdr->error, kErrTimeout);
-            }
+// One large segment's runs [j, jl]: lane l takes a contiguous share of the
+// runs, class counts in registers; warp scans per class give each run's
+// output position per class, the segment's sizes and head flags.
+template <int M>
+__device__ __forceinline__ void scan_segment_runs(const SegArgs& a, uint32_t j, uint32_t jl,
+                                                  uint32_t seg, uint32_t seg_start) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t R = jl - j + 1u;
+    const uint32_t per = (R + 31u) >> 5;
+    const uint32_t rb = j + min(lane * per, R), re = j + min(lane * per + per, R);
+    uint32_t acc[M];
+#pragma unroll
+    for (int c = 0; c < M; c++) acc[c] = 0;
+    for (uint32_t r = rb; r < re; r++) {
+        const uint32_t* row = a.run_cnt + static_cast<uint64_t>(r) * M;
+#pragma unroll
+        for (int c = 0; c < M; c++) acc[c] += __ldcg(row + c);
+    }
+    uint32_t cur[M];
+    uint32_t off = seg_start;
+#pragma unroll
+    for (int c = 0; c < M; c++) {
+        const uint32_t incl = warp_incl_scan(acc[c]);
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        cur[c] = off + incl - acc[c];
+        if (lane == static_cast<uint32_t>(c)) {
+            if (a.seg_sizes != nullptr && static_cast<uint32_t>(c) < a.m)
+                a.seg_sizes[static_cast<uint64_t>(seg) * a.m + c] = tot;
+            if (a.headflags != nullptr && tot > 0) a.headflags[off] = tot;
         }
+        off += tot;
+    }
+    for (uint32_t r = rb; r < re; r++) {
+        const uint32_t* row = a.run_cnt + static_cast<uint64_t>(r) * M;
+        uint32_t* dst = a.run_base + static_cast<uint64_t>(r) * M;
+#pragma unroll
+        for (int c = 0; c < M; c++) {
+            const uint32_t x = __ldcg(row + c);
+            dst[c] = cur[c];
+            cur[c] += x;
+        }
+    }
+}
+
+// Every warp looks at 32 consecutive runs at a time and scans the segments
+// whose first run is among them.
+template <int M>
+__global__ void __launch_bounds__(256) seg_run_scan(SegArgs a) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t num_runs = a.hdr->num_runs;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t j0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32u; j0 < num_runs;
+         j0 += warps * 32u) {
+        const uint32_t j = j0 + lane;
+        RunEntry e{};
+        bool first = false;
+        if (j < num_runs) {
+            e = a.runs[j];
+            first = e.p0 == static_cast<uint32_t>(a.offsets[e.seg]);
+        }
+        uint32_t firsts = __ballot_sync(0xffffffffu, first);
+        while (firsts != 0u) {
+            const int l = __ffs(firsts) - 1;
+            firsts &= firsts - 1u;
+            const uint32_t jl = __shfl_sync(0xffffffffu, e.jlast, l);
+            const uint32_t seg = __shfl_sync(0xffffffffu, e.seg, l);
+            const uint32_t p0 = __shfl_sync(0xffffffffu, e.p0, l);
+            scan_segment_runs<M>(a, j0 + l, min(jl, num_runs - 1u), seg, p0);
+        }
+    }
+}
+
+// Every run of a large segment through the TMA ring and tile_scatter, from
+// the run_base positions.  Runs are taken in reverse order of the counts, so
+// the first re-reads find the runs counted last still in L2.
+template <class V, class D, int M, int THREADS, int STAGES>
+__global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 64 registers
+    seg_run_scatter(SegArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
+    using L = SegSmem<V, M, THREADS, STAGES>;
+    using TG = typename L::G;
+    constexpr int ITEMS = TG::kItems;
+    constexpr int P = L::kTile;
+    constexpr int ROWS = TG::kRows;
+    constexpr uint32_t AU = L::kAU;
+    static_assert(M <= 16 && M >= 2, "class bound");
+    static_assert(ROWS <= 256, "TMA box height");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    unsigned char* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    V* ring = reinterpret_cast<V*>(base);
+    V* stage = reinterpret_cast<V*>(base + L::kRingBytes);
+    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(base + L::kRingBytes + TG::kStageBytes);
+
+    __shared__ __align__(8) uint64_t bars[STAGES];
+    __shared__ TileShared<M> sh;
+    __shared__ uint32_t ticket_sh[2];
+
+    const int tid = threadIdx.x;
+    const V* in = static_cast<const V*>(a.in);
+    V* out = static_cast<V*>(a.out);
+    const uint32_t out_phase =
+        static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
+    const bool tma_ok = a.use_tma != 0;
+    const uint32_t num_runs = a.hdr->num_runs;
+    uint32_t ring_uses = 0;  // mbarrier phase bookkeeping across runs
+
+    if (tid == 0) {
+#pragma unroll
+        for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    for (uint32_t it = 0;; it++) {
+        if (tid == 0) ticket_sh[it & 1u] = atomicAdd(&a.hdr->ticket2, 1u);
         __syncthreads();
-        if (fail_sh) continue;  // uniform: nothing was issued
+        const uint32_t t = ticket_sh[it & 1u];
+        if (t >= num_runs) break;
+        const uint32_t j = num_runs - 1u - t;
+        const RunEntry ent = a.runs[j];
+        const D dj = seg_discr(a, d, ent.seg);
+        if (tid < M) sh.cursor[0][tid] = __ldcg(a.run_base + static_cast<uint64_t>(j) * M + tid);
+        __syncthreads();
         const uint32_t wf = ent.p0 / P, wl = (ent.p1 - 1u) / P;
         const uint32_t ntiles = wl - wf + 1u;
         auto issue = [&](uint32_t i) {  // tile wf+i into ring slot (ring_uses+i) % STAGES
@@ -794,10 +986,6 @@ __global__ void __launch_bounds__(THREADS, 3)
             }
         }
         ring_uses += ntiles;
-        // the ring and the stage alias the group buffers: the bulk stores must
-        // have read the stage before a group item may overwrite it
-        if (tid < M) bulk_wait_read<0>();
-        __syncthreads();
         if (failed) break;
     }
     if (tid < M) bulk_wait_all();

@@ -97,6 +97,22 @@ def test_empty_and_tiny_segments(cuda_ready):
         check(cuda_ready, x, offs, m)
 
 
+@pytest.mark.parametrize("m", [3, 16])
+def test_group_partition_edges(cuda_ready, m):
+    """Small segments are partitioned by a whole CTA per group, each thread
+    owning k consecutive elements (k odd, at most 23 for u32): lengths at and
+    around those per-thread spans, around the group window (1536 elements)
+    and the small-segment bound (4096), runs of empty segments, and groups cut
+    after 128 segments."""
+    rng = np.random.default_rng(40 + m)
+    pool = [0, 0, 0, 1, 2, 21, 22, 23, 24, 25, 45, 46, 47, 69, 1535, 1536, 1537, 3000, 4095, 4096]
+    lengths = rng.choice(pool, size=6000)
+    lengths[1000:1400] = 1  # 400 one-element segments in a row
+    offs = offsets_from_lengths(lengths)
+    x = oracle.fill_uniform_u32(int(offs[-1]), 41 + m)
+    check(cuda_ready, x, offs, m)
+
+
 def test_single_huge_segment_equals_plain(cuda_ready):
     n = (1 << 22) + 123
     x = oracle.fill_uniform_u32(n, 9)
@@ -218,13 +234,15 @@ def test_one_workspace_serves_plain_and_segmented_calls(cuda_ready):
 
 
 @pytest.mark.parametrize("m_max", [4, 16])
-def test_per_segment_class_counts(cuda_ready, m_max):
+@pytest.mark.parametrize("short", [False, True])
+def test_per_segment_class_counts(cuda_ready, m_max, short):
     """One launch, a class count per segment (class = v % m_s): each segment
-    equals the oracle run with its own m."""
+    equals the oracle run with its own m.  ``short``: segments of 0..59
+    elements, so one thread's elements span segments of different m."""
     import mdiscriminator_b200 as mdx
     torch = cuda_ready
     rng = np.random.default_rng(90 + m_max)
-    lengths = lognormal_lengths(1200, 91 + m_max)
+    lengths = rng.integers(0, 60, size=3000) if short else lognormal_lengths(1200, 91 + m_max)
     offs = offsets_from_lengths(lengths)
     seg_m = rng.integers(1, m_max + 1, size=len(lengths)).astype(np.int32)
     x = oracle.fill_uniform_u32(int(offs[-1]), 92)
