@@ -5,9 +5,9 @@ Keys: element layout (4-byte values / 8-byte records), class bound (the
 smallest power of two >= m) and a range of ceil(log2 n).  Knobs:
 
 * plain path: CTAs per SM of the chunk grid (`plain_ctas_per_sm`);
-* segmented path: tiles per run of a large segment (`run_tiles`),
-  small-segment groups per work item (`group_batch`), and the extra lag of
-  scatter items behind their counts (`lag_slack_pct`).
+* segmented path: tiles per run of a large segment (`run_tiles`) and
+  small-segment groups per work item (`group_batch`).  (`lag_slack_pct` is
+  still accepted in the table but no longer used by the kernels.)
 
 The reference picked its block shapes by recompiling with -D macros and
 timing them (cuda_code/run.py:12-96); here the choice is made at run time.
@@ -104,7 +104,7 @@ def main(argv=None):
             out = torch.empty_like(d)
             do = torch.from_numpy(offs).to(dev)
             ws = mdx.new_workspace(mdx.segmented_workspace_size(n, S, elem, 16), dev)
-            cands = list(itertools.product((4, 8, 16), (4, 8, 16), (25, 50, 100)))
+            cands = list(itertools.product((2, 4, 8, 16), (2, 4, 8, 16), (50,)))
             if args.quick:
                 cands = list(itertools.product((4, 8, 16), (8,), (50,)))
             for M in seg_bounds:
