@@ -471,6 +471,7 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         const Tuning tun = tuning_for(sizeof(V) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_U32, M, n);
         a.run_tiles = tun.run_tiles >= 1 ? tun.run_tiles : kRunTiles;
         a.group_batch = tun.group_batch >= 1 ? tun.group_batch : kGroupBatch;
+        if (a.group_batch > static_cast<uint32_t>(kMaxGroupBatch)) a.group_batch = kMaxGroupBatch;
     }
     CUtensorMap map;
     a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::G::kRows) ? 1 : 0;

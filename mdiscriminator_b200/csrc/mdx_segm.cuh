@@ -56,6 +56,7 @@ namespace mdx {
 // Defaults of the run-time knobs (the autotuner may choose others):
 constexpr int kRunTiles = 8;     // tiles per run of a large segment
 constexpr int kGroupBatch = 8;   // small-segment groups per work item (pipelined)
+constexpr int kMaxGroupBatch = 32;
 constexpr int kLagSlackPct = 50; // accepted in the tuning table, no longer used
 
 // status word: [63:34] epoch (30 bits), [33:32] state, [31:0] count
@@ -345,9 +346,6 @@ struct SegSmem {
         static_cast<int>(group_window<kTile>()) + kTile + 2 * static_cast<int>(kAU);
     static constexpr size_t kGroupBytes = 3ull * kGroupElems * sizeof(V);
     static constexpr size_t kBytes = 128 + kGroupBytes;  // seg_main
-    // elements per thread in a group (odd: the threads' strided shared-memory
-    // reads fall in different banks)
-    static constexpr int kGroupItems = ((kGroupElems + 255) / 256) | 1;
     // seg_run_scatter: TMA ring + tile stage + count matrix
     static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
     static constexpr size_t kRunBytes = 1024 + kRingBytes + G::kStageBytes + G::kCntBytes;
@@ -400,7 +398,14 @@ struct GroupScratch {
     uint16_t hpos[kGroupSegs + 1];  // head of each non-empty segment in the group; [nseg] = L
     uint16_t sidx[kGroupSegs];      // its index - h
     uint8_t msz[kGroupSegs];        // its class count (per-segment m)
-    uint8_t start_ord[THREADS];     // the non-empty segment holding each thread's first element
+};
+
+// Offsets (and class count) of segment h + threadIdx.x of the next group,
+// loaded by each thread while the current group is partitioned.
+struct GroupPrefetch {
+    uint64_t o0, o1;
+    uint32_t m;
+    bool valid;
 };
 
 // The discriminator of a group's segment with class count m: per-segment
@@ -411,8 +416,8 @@ __device__ __forceinline__ D group_discr(const SegArgs& a, const D& d, const uin
     if constexpr (std::is_same<D, DiscrMod>::value) {
         if (a.seg_m != nullptr) {
             DiscrMod x;
-            x.c = cmod[m];
-            x.m = m;
+            x.m = min(m, 16u);
+            x.c = cmod[x.m];
             return x;
         }
     }
@@ -421,45 +426,68 @@ __device__ __forceinline__ D group_discr(const SegArgs& a, const D& d, const uin
 
 // One CTA partitions one group of small segments held in shared memory
 // (element x of the group at src[x], 0 <= x < L) into the output image
-// dst[0 .. L) and writes the segments' sizes.  Every thread owns k <= ITEMS
-// consecutive elements whatever the segment lengths:
-//   P0  one thread per segment: ordinals of the non-empty segments, their
-//       heads, and the segment holding each thread's first element;
-//   P1  classes (kept as nibbles) and the class counts of the fragment after
-//       the thread's last segment head;
+// dst[0 .. L) and writes the segments' sizes.  Every thread owns k = ~L/256
+// consecutive elements whatever the segment lengths (k odd: the threads'
+// strided shared-memory reads fall in different banks):
+//   P0  one thread per segment: ordinals of the non-empty segments and their
+//       heads; each thread finds the segment holding its first element by a
+//       binary search over the heads;
+//   P1  the class counts of the fragment after the thread's last segment
+//       head; a segment that begins and ends inside the thread's range is
+//       closed here (its class bases to shared memory, its sizes and head
+//       flags to global memory);
 //   P2  a segmented exclusive scan of those counts over the threads gives the
 //       counts of the thread's first segment before its first element;
-//   P3  the thread in which a segment ends has its class totals: it writes the
-//       segment's class bases (shared) and sizes / head flags (global);
+//   P3  the thread's first segment, if it ends in the thread's range, is
+//       closed with the scanned counts plus its part in the range;
 //   P4  every element goes to head + base[class] + its rank in the segment.
-template <class V, class D, int M, int THREADS, int ITEMS>
+template <class V, class D, int M, int THREADS>
 __device__ void seg_group_cta(const SegArgs& a, const D& d, const uint64_t* cmod, uint32_t h,
                               uint32_t he, uint64_t r0, uint32_t L, const V* src, V* dst,
-                              GroupScratch<M, THREADS>& gs) {
+                              GroupScratch<M, THREADS>& gs, GroupPrefetch& pf,
+                              const uint32_t* next_h, const uint32_t* next_he) {
     using HC = HalfCounts<M>;
     constexpr int NW = HC::NW;
     constexpr int W = THREADS / 32;
-    constexpr int CW = (ITEMS + 7) / 8;  // nibble words
     static_assert(static_cast<int>(kGroupSegs) <= THREADS, "one thread per segment");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t k = ((L + THREADS - 1) / THREADS) | 1u;  // <= ITEMS
+    const uint32_t k = ((L + THREADS - 1) / THREADS) | 1u;
     const uint32_t lo = min(tid * k, L), hi = min(lo + k, L);
 
     // ---- P0
     const uint64_t sg = static_cast<uint64_t>(h) + tid;
     uint32_t ne = 0, x0 = 0, x1 = 0, ms = a.m;
     if (sg < he && tid < static_cast<int>(kGroupSegs)) {
-        const uint64_t o0 = a.offsets[sg], o1 = a.offsets[sg + 1];
+        uint64_t o0, o1;
+        if (pf.valid) {
+            o0 = pf.o0;
+            o1 = pf.o1;
+            ms = pf.m;
+        } else {
+            o0 = a.offsets[sg];
+            o1 = a.offsets[sg + 1];
+            if (a.seg_m != nullptr) ms = min(max(a.seg_m[sg], 1u), a.m_bound);
+        }
         x0 = static_cast<uint32_t>(o0 - r0);
         x1 = static_cast<uint32_t>(o1 - r0);
         ne = (o1 > o0 && o0 >= r0 && x1 <= L) ? 1u : 0u;
-        if (a.seg_m != nullptr) ms = min(max(a.seg_m[sg], 1u), a.m_bound);
         if (o1 == o0 && a.seg_sizes != nullptr)
             for (uint32_t c = 0; c < a.m; c++) a.seg_sizes[sg * a.m + c] = 0u;
     }
     const uint32_t incl = warp_incl_scan(ne);
     if (lane == 31) gs.wagg[warp][0] = incl;
     __syncthreads();
+    // the next group's head and end are visible now: start its loads
+    pf.valid = next_h != nullptr;
+    if (pf.valid) {
+        const uint64_t ns = static_cast<uint64_t>(*next_h) + tid;
+        pf.m = a.m;
+        if (ns < *next_he && tid < static_cast<int>(kGroupSegs)) {
+            pf.o0 = a.offsets[ns];
+            pf.o1 = a.offsets[ns + 1];
+            if (a.seg_m != nullptr) pf.m = min(max(a.seg_m[ns], 1u), a.m_bound);
+        }
+    }
     uint32_t before = 0, nseg = 0;
 #pragma unroll
     for (int w = 0; w < W; w++) {
@@ -472,41 +500,66 @@ __device__ void seg_group_cta(const SegArgs& a, const D& d, const uint64_t* cmod
         gs.hpos[q] = static_cast<uint16_t>(x0);
         gs.sidx[q] = static_cast<uint16_t>(tid);
         gs.msz[q] = static_cast<uint8_t>(ms);
-        for (uint32_t t = (x0 + k - 1u) / k; t * k < x1 && t < static_cast<uint32_t>(THREADS); t++)
-            gs.start_ord[t] = static_cast<uint8_t>(q);
     }
     if (tid == 0) gs.hpos[nseg] = static_cast<uint16_t>(L);
     __syncthreads();
 
     // ---- P1
     const bool active = lo < hi && nseg > 0;
-    const uint32_t q0 = active ? min(static_cast<uint32_t>(gs.start_ord[tid]), nseg - 1u) : 0u;
+    uint32_t q0 = 0;  // the last non-empty segment with head <= lo (hpos[nseg] = L > lo)
+    if (active) {
+        uint32_t qb = nseg;
+        while (qb - q0 > 1u) {
+            const uint32_t mid = (q0 + qb) >> 1;
+            if (gs.hpos[mid] <= lo) q0 = mid; else qb = mid;
+        }
+    }
     const bool head_at_lo = active && gs.hpos[q0] == lo;
-    uint32_t cls[CW];
+    const D d0 = active ? group_discr(a, d, cmod, gs.msz[q0]) : d;
+    // segment qq ends here with class totals `tot`: its class bases (shared),
+    // sizes and head flags (global)
+    auto close = [&](uint32_t qq, const HC& tot) {
+        const uint64_t s = static_cast<uint64_t>(h) + gs.sidx[qq];
+        const uint64_t xh = r0 + gs.hpos[qq];
+        uint32_t off = 0;
+        uint32_t bw[NW];
 #pragma unroll
-    for (int w = 0; w < CW; w++) cls[w] = 0;
-    HC tail;
+        for (int w = 0; w < NW; w++) bw[w] = 0;
+#pragma unroll
+        for (int c = 0; c < M; c++) {
+            const uint32_t t = tot.get(c);
+            bw[c >> 1] |= off << (16 * (c & 1));
+            if (a.seg_sizes != nullptr && static_cast<uint32_t>(c) < a.m) a.seg_sizes[s * a.m + c] = t;
+            if (a.headflags != nullptr && t > 0) a.headflags[xh + off] = t;
+            off += t;
+        }
+#pragma unroll
+        for (int w = 0; w < NW; w++) gs.base[qq][w] = bw[w];
+    };
+    // the counts of the fragment after the last head in (lo, hi) (all of the
+    // range without one); segments that begin and end inside the range are
+    // closed on the way, the first segment's part is kept for after the scan
+    HC tail, pre;
     tail.zero();
+    pre.zero();
     bool inner = false;  // a segment head in (lo, hi)
     if (active) {
         uint32_t q = q0, nxt = gs.hpos[q0 + 1];
-        D dc = group_discr(a, d, cmod, gs.msz[q0]);
-#pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t x = lo + i;
-            if (x < hi) {
-                if (x == nxt) {
-                    inner = true;
-                    tail.zero();
-                    q++;
-                    nxt = gs.hpos[q + 1];
-                    dc = group_discr(a, d, cmod, gs.msz[q]);
-                }
-                const uint32_t c = dc(src[x]);
-                cls[i >> 3] |= c << (4 * (i & 7));
-                tail.inc(c);
+        D dc = d0;
+        for (uint32_t x = lo; x < hi; x++) {
+            if (x == nxt) {
+                if (inner) close(q, tail);
+                else pre = tail;
+                inner = true;
+                tail.zero();
+                q++;
+                nxt = gs.hpos[q + 1];
+                dc = group_discr(a, d, cmod, gs.msz[q]);
             }
+            tail.inc(dc(src[x]));
         }
+        if (inner && hi == nxt) close(q, tail);
+        if (!inner) pre = tail;
     }
 
     // ---- P2: segmented exclusive scan of (reset, counts) over the threads
@@ -549,69 +602,39 @@ __device__ void seg_group_cta(const SegArgs& a, const D& d, const uint64_t* cmod
     }
     if (head_at_lo) carry.zero();
 
-    // ---- P3
+    // ---- P3: the first segment ends at the first head inside, or exactly at hi
     if (active) {
-        uint32_t q = q0, nxt = gs.hpos[q0 + 1];
-        HC run = carry;
-        auto close = [&](uint32_t qq) {  // segment qq ends here; `run` holds its totals
-            const uint64_t s = static_cast<uint64_t>(h) + gs.sidx[qq];
-            const uint64_t xh = r0 + gs.hpos[qq];
-            uint32_t off = 0;
-            uint32_t bw[NW];
+        const bool ends = inner || hi == gs.hpos[q0 + 1];
+        if (ends) {
+            HC t;
 #pragma unroll
-            for (int w = 0; w < NW; w++) bw[w] = 0;
-#pragma unroll
-            for (int c = 0; c < M; c++) {
-                const uint32_t t = run.get(c);
-                bw[c >> 1] |= off << (16 * (c & 1));
-                if (a.seg_sizes != nullptr && static_cast<uint32_t>(c) < a.m)
-                    a.seg_sizes[s * a.m + c] = t;
-                if (a.headflags != nullptr && t > 0) a.headflags[xh + off] = t;
-                off += t;
-            }
-#pragma unroll
-            for (int w = 0; w < NW; w++) gs.base[qq][w] = bw[w];
-        };
-#pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t x = lo + i;
-            if (x < hi) {
-                if (x == nxt) {
-                    close(q);
-                    run.zero();
-                    q++;
-                    nxt = gs.hpos[q + 1];
-                }
-                run.inc((cls[i >> 3] >> (4 * (i & 7))) & 15u);
-            }
+            for (int w = 0; w < NW; w++) t.w[w] = carry.w[w] + pre.w[w];
+            close(q0, t);
         }
-        if (hi == nxt) close(q);
     }
     __syncthreads();
 
-    // ---- P4
+    // ---- P4: positions = head + class base + rank in the segment (packed per class)
     if (active) {
         uint32_t q = q0, nxt = gs.hpos[q0 + 1], xh = gs.hpos[q0];
-        HC bs, run = carry;
+        HC cur;
 #pragma unroll
-        for (int w = 0; w < NW; w++) bs.w[w] = gs.base[q0][w];
+        for (int w = 0; w < NW; w++) cur.w[w] = gs.base[q0][w] + carry.w[w];
+        D dc = d0;
+        for (uint32_t x = lo; x < hi; x++) {
+            if (x == nxt) {
+                q++;
+                xh = x;
+                nxt = gs.hpos[q + 1];
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++) {
-            const uint32_t x = lo + i;
-            if (x < hi) {
-                if (x == nxt) {
-                    q++;
-                    xh = x;
-                    nxt = gs.hpos[q + 1];
-#pragma unroll
-                    for (int w = 0; w < NW; w++) bs.w[w] = gs.base[q][w];
-                    run.zero();
-                }
-                const uint32_t c = (cls[i >> 3] >> (4 * (i & 7))) & 15u;
-                const uint32_t pos = xh + bs.get(c) + run.get(c);
-                run.inc(c);
-                if (pos < L) dst[pos] = src[x];
+                for (int w = 0; w < NW; w++) cur.w[w] = gs.base[q][w];
+                dc = group_discr(a, d, cmod, gs.msz[q]);
             }
+            const V v = src[x];
+            const uint32_t c = dc(v);
+            const uint32_t pos = xh + cur.get(c);
+            cur.inc(c);
+            if (pos < L) dst[pos] = v;
         }
     }
 }
@@ -636,6 +659,8 @@ __global__ void __launch_bounds__(THREADS, 3)
     __shared__ uint64_t gi_r0[2], gi_r1[2], gi_as[2], gi_tail[2];
     __shared__ uint32_t red[W][M];
     __shared__ GroupScratch<M, THREADS> gs;
+    __shared__ uint32_t gb_h[kMaxGroupBatch], gb_he[kMaxGroupBatch];  // the batch's groups
+    __shared__ uint64_t gb_r0[kMaxGroupBatch], gb_r1[kMaxGroupBatch];
     __shared__ uint64_t cmod[17];  // DiscrMod constants for m = 1 .. 16
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -674,11 +699,21 @@ __global__ void __launch_bounds__(THREADS, 3)
             // partitioned
             const uint32_t g0 = t * a.group_batch;
             const uint32_t gcnt = min(a.group_batch, num_groups - g0);
+            // the batch's group heads, ends and element ranges, loaded once
+            if (tid < static_cast<int>(gcnt)) {
+                const uint32_t h = a.groups[g0 + tid];
+                const uint32_t he =
+                    static_cast<uint32_t>(min(static_cast<uint64_t>(a.groups_end[g0 + tid]), S));
+                gb_h[tid] = h;
+                gb_he[tid] = he;
+                gb_r0[tid] = a.offsets[h];
+                gb_r1[tid] = a.offsets[he];
+            }
+            __syncthreads();
             auto issue_group = [&](uint32_t i) {  // thread 0 only
                 const uint32_t slot = (group_uses + i) & 1u;
-                const uint32_t h = a.groups[g0 + i];
-                const uint32_t he = static_cast<uint32_t>(min(static_cast<uint64_t>(a.groups_end[g0 + i]), S));
-                const uint64_t r0 = a.offsets[h], r1 = a.offsets[he];
+                const uint32_t h = gb_h[i], he = gb_he[i];
+                const uint64_t r0 = gb_r0[i], r1 = gb_r1[i];
                 const uint64_t as = r0 & ~static_cast<uint64_t>(AU - 1u);
                 uint64_t ve = min((r1 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u),
                                   a.n & ~static_cast<uint64_t>(AU - 1u));
@@ -700,6 +735,8 @@ __global__ void __launch_bounds__(THREADS, 3)
             };
             if (tid == 0) issue_group(0);
             bool failed = false;
+            GroupPrefetch pf;
+            pf.valid = false;
             for (uint32_t i = 0; i < gcnt; i++) {
                 const uint32_t use = group_uses + i;
                 const uint32_t slot = use & 1u;
@@ -717,9 +754,11 @@ __global__ void __launch_bounds__(THREADS, 3)
                     break;
                 }
                 if (tid == 0 && i + 1 < gcnt) issue_group(i + 1);  // the other buffer is free
-                seg_group_cta<V, D, M, THREADS, L::kGroupItems>(
+                const bool more = i + 1 < gcnt;
+                seg_group_cta<V, D, M, THREADS>(
                     a, d, cmod, gi_h[slot], gi_he[slot], r0, static_cast<uint32_t>(r1 - r0),
-                    gin + (r0 - as), g_out + (r0 - as), gs);
+                    gin + (r0 - as), g_out + (r0 - as), gs, pf, more ? &gi_h[slot ^ 1u] : nullptr,
+                    more ? &gi_he[slot ^ 1u] : nullptr);
                 __syncthreads();
                 // write the range back from the output image
                 if (out_vec && out_phase == 0u) {
