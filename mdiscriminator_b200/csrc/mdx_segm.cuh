@@ -955,6 +955,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     const uint32_t out_phase =
         static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
     const bool tma_ok = a.use_tma != 0;
+    const uint64_t map_elems = (a.n * sizeof(V) / 128u) * (128u / sizeof(V));
     const uint32_t num_runs = a.hdr->num_runs;
     uint32_t ring_uses = 0;  // mbarrier phase bookkeeping across runs
 
@@ -977,12 +978,16 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         __syncthreads();
         const uint32_t wf = ent.p0 / P, wl = (ent.p1 - 1u) / P;
         const uint32_t ntiles = wl - wf + 1u;
+        // a tile (partial ones too) comes by TMA when the run's part of it lies
+        // inside the tensor map (the input's whole 128-byte rows; rows past the
+        // map read as zeros and lie outside the run)
+        auto via_tma = [&](uint32_t w) {
+            return tma_ok && min(static_cast<uint64_t>(ent.p1), static_cast<uint64_t>(w + 1) * P) <= map_elems;
+        };
         auto issue = [&](uint32_t i) {  // tile wf+i into ring slot (ring_uses+i) % STAGES
             const uint32_t w = wf + i;
             const uint32_t slot = (ring_uses + i) % STAGES;
-            const bool whole = static_cast<uint64_t>(w) * P >= ent.p0 &&
-                               static_cast<uint64_t>(w + 1) * P <= ent.p1;
-            if (tma_ok && whole) {
+            if (via_tma(w)) {
                 mbar_arrive_expect_tx(&bars[slot], P * sizeof(V));
                 tma_load_2d(ring + slot * P, &tmap, 0, static_cast<int32_t>(w * ROWS), &bars[slot]);
             } else {
@@ -1002,7 +1007,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
             const uint32_t use = ring_uses + i;
             const bool ok = mbar_wait_bounded(&bars[use % STAGES], (use / STAGES) & 1u);
             V v[ITEMS];
-            if (tma_ok && full) {
+            if (via_tma(w)) {
                 take_swizzled<V, ITEMS>(ring + (use % STAGES) * P, v);
             } else {
 #pragma unroll
