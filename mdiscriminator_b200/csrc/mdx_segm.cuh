@@ -895,8 +895,43 @@ __device__ __forceinline__ void scan_segment_runs(const SegArgs& a, uint32_t j, 
     }
 }
 
-// Every warp looks at 32 consecutive runs at a time and scans the segments
-// whose first run is among them.
+// One large segment with few runs [j, jl], by one lane alone.
+template <int M>
+__device__ __forceinline__ void scan_segment_runs_lane(const SegArgs& a, uint32_t j, uint32_t jl,
+                                                       uint32_t seg, uint32_t seg_start) {
+    uint32_t tot[M];
+#pragma unroll
+    for (int c = 0; c < M; c++) tot[c] = 0;
+    for (uint32_t r = j; r <= jl; r++) {
+        const uint32_t* row = a.run_cnt + static_cast<uint64_t>(r) * M;
+#pragma unroll
+        for (int c = 0; c < M; c++) tot[c] += __ldcg(row + c);
+    }
+    uint32_t cur[M];
+    uint32_t off = seg_start;
+#pragma unroll
+    for (int c = 0; c < M; c++) {
+        cur[c] = off;
+        if (a.seg_sizes != nullptr && static_cast<uint32_t>(c) < a.m)
+            a.seg_sizes[static_cast<uint64_t>(seg) * a.m + c] = tot[c];
+        if (a.headflags != nullptr && tot[c] > 0) a.headflags[off] = tot[c];
+        off += tot[c];
+    }
+    for (uint32_t r = j; r <= jl; r++) {
+        const uint32_t* row = a.run_cnt + static_cast<uint64_t>(r) * M;
+        uint32_t* dst = a.run_base + static_cast<uint64_t>(r) * M;
+#pragma unroll
+        for (int c = 0; c < M; c++) {
+            const uint32_t x = __ldcg(row + c);
+            dst[c] = cur[c];
+            cur[c] += x;
+        }
+    }
+}
+
+// Every warp looks at 32 consecutive runs at a time: the lane holding a
+// segment's first run scans a segment of at most 4 runs by itself, the whole
+// warp takes the longer ones in turn.
 template <int M>
 __global__ void __launch_bounds__(256) seg_run_scan(SegArgs a) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -911,14 +946,17 @@ __global__ void __launch_bounds__(256) seg_run_scan(SegArgs a) {
             e = a.runs[j];
             first = e.p0 == static_cast<uint32_t>(a.offsets[e.seg]);
         }
-        uint32_t firsts = __ballot_sync(0xffffffffu, first);
-        while (firsts != 0u) {
-            const int l = __ffs(firsts) - 1;
-            firsts &= firsts - 1u;
-            const uint32_t jl = __shfl_sync(0xffffffffu, e.jlast, l);
+        const uint32_t jl = min(e.jlast, num_runs - 1u);
+        const bool shortseg = first && jl >= j && jl - j < 4u;
+        if (shortseg) scan_segment_runs_lane<M>(a, j, jl, e.seg, e.p0);
+        uint32_t longs = __ballot_sync(0xffffffffu, first && !shortseg);
+        while (longs != 0u) {
+            const int l = __ffs(longs) - 1;
+            longs &= longs - 1u;
+            const uint32_t jll = __shfl_sync(0xffffffffu, jl, l);
             const uint32_t seg = __shfl_sync(0xffffffffu, e.seg, l);
             const uint32_t p0 = __shfl_sync(0xffffffffu, e.p0, l);
-            scan_segment_runs<M>(a, j0 + l, min(jl, num_runs - 1u), seg, p0);
+            if (jll >= j0 + l) scan_segment_runs<M>(a, j0 + l, jll, seg, p0);
         }
     }
 }
