@@ -399,8 +399,8 @@ inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool
     const uint64_t NW = (n + P - 1) / P;
     SegLayout L;
     L.max_runs = 2 * NW + 2;    // runs of segments that tile [0, n): far fewer
-    // a group starts at a new window of 3P/8 elements or after kGroupSegs segments
-    const uint64_t GW = 3 * P / 8;  // group_window<P>()
+    // a group starts at a new window of P elements or after kGroupSegs segments
+    const uint64_t GW = P;  // group_window<P>()
     L.max_groups = (n + GW - 1) / GW + S / kGroupSegs + 2;
     L.run_loc = kHeaderBytes;
     L.grp_loc = align_up(L.run_loc + 4 * (S + 1), kAlign);

@@ -9,7 +9,7 @@
 //                   (P elements) are "large" and are cut into runs of up to
 //                   RUN_TILES tiles; the other ("small") segments are grouped
 //                   (consecutive small segments starting in one window of
-//                   3P/8 elements, at most kGroupSegs of them).  Block-local
+//                   P elements, at most kGroupSegs of them).  Block-local
 //                   scans of the run and group counts; the last CTA scans the
 //                   block totals, records the counts and resets the tickets.
 //   seg_plan_emit   writes the run entries {segment, [p0, p1), last run of
@@ -140,12 +140,12 @@ __device__ __forceinline__ D seg_discr(const SegArgs& a, const D& d, uint64_t s)
 constexpr uint64_t kSegsOnDevice = ~0ull;
 
 // Small segments are grouped: a group is a run of consecutive small segments
-// whose first elements lie in one window of 3P/8 elements, cut after at most
-// kGroupSegs segments, so a group spans < 3P/8 + P elements.
+// whose first elements lie in one window of P elements, cut after at most
+// kGroupSegs segments, so a group spans < 2P elements.
 constexpr uint32_t kGroupSegs = 128;
 template <int P>
 __host__ __device__ constexpr uint64_t group_window() {
-    return 3ull * P / 8ull;
+    return static_cast<uint64_t>(P);
 }
 template <int P>
 __device__ __forceinline__ bool group_head(const SegArgs& a, uint64_t s, uint64_t a0) {
@@ -339,12 +339,13 @@ struct SegSmem {
     using G = TileGeom<V, THREADS, M>;
     static constexpr int kTile = G::kTile;  // == P
     static constexpr uint32_t kAU = G::kAU;
-    // small groups (segments starting in one window of 3P/8, each <= P): two
-    // input buffers (one being filled by a bulk copy) and an output image, each
-    // for a range of < 3P/8 + P elements plus 16-byte alignment slack
+    // small groups (segments starting in one window of P, each <= P): an
+    // input buffer and an output image, each for a range of < 2P elements plus
+    // 16-byte alignment slack (the next group's copy overlaps the current
+    // group's write-out; the other resident CTAs cover the rest of its latency)
     static constexpr int kGroupElems =
         static_cast<int>(group_window<kTile>()) + kTile + 2 * static_cast<int>(kAU);
-    static constexpr size_t kGroupBytes = 3ull * kGroupElems * sizeof(V);
+    static constexpr size_t kGroupBytes = 2ull * kGroupElems * sizeof(V);
     static constexpr size_t kBytes = 128 + kGroupBytes;  // seg_main
     // seg_run_scatter: TMA ring + tile stage + count matrix
     static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
@@ -651,7 +652,7 @@ __global__ void __launch_bounds__(THREADS, 3)
     const uint32_t raw = smem_addr(smem_raw);
     unsigned char* base = smem_raw + (((raw + 127u) & ~127u) - raw);
     V* g_in0 = reinterpret_cast<V*>(base);
-    V* g_out = g_in0 + 2 * L::kGroupElems;
+    V* g_out = g_in0 + L::kGroupElems;
 
     __shared__ __align__(8) uint64_t gbars[2];
     __shared__ uint32_t ticket_sh[2];
@@ -724,7 +725,7 @@ __global__ void __launch_bounds__(THREADS, 3)
                 gi_r1[slot] = r1;
                 gi_as[slot] = as;
                 gi_tail[slot] = max(ve, r0);
-                V* dst = g_in0 + slot * L::kGroupElems;
+                V* dst = g_in0;
                 const uint32_t bytes = static_cast<uint32_t>((ve - as) * sizeof(V));
                 if (bytes > 0) {
                     mbar_arrive_expect_tx(&gbars[slot], bytes);
@@ -742,7 +743,7 @@ __global__ void __launch_bounds__(THREADS, 3)
                 const uint32_t slot = use & 1u;
                 const bool ok = mbar_wait_bounded(&gbars[slot], (use >> 1) & 1u);
                 __syncthreads();  // slot info visible
-                V* gin = g_in0 + slot * L::kGroupElems;
+                V* gin = g_in0;
                 const uint64_t as = gi_as[slot], r0 = gi_r0[slot], r1 = gi_r1[slot];
                 for (uint64_t e = gi_tail[slot] + tid; e < r1; e += THREADS) gin[e - as] = in[e];
                 if (__syncthreads_or(!ok)) {
@@ -753,13 +754,15 @@ __global__ void __launch_bounds__(THREADS, 3)
                     }
                     break;
                 }
-                if (tid == 0 && i + 1 < gcnt) issue_group(i + 1);  // the other buffer is free
                 const bool more = i + 1 < gcnt;
                 seg_group_cta<V, D, M, THREADS>(
                     a, d, cmod, gi_h[slot], gi_he[slot], r0, static_cast<uint32_t>(r1 - r0),
-                    gin + (r0 - as), g_out + (r0 - as), gs, pf, more ? &gi_h[slot ^ 1u] : nullptr,
-                    more ? &gi_he[slot ^ 1u] : nullptr);
+                    gin + (r0 - as), g_out + (r0 - as), gs, pf, more ? &gb_h[i + 1] : nullptr,
+                    more ? &gb_he[i + 1] : nullptr);
+                // every read of the input buffer precedes the next group's copy
+                fence_proxy_async_smem();
                 __syncthreads();
+                if (tid == 0 && more) issue_group(i + 1);
                 // write the range back from the output image
                 if (out_vec && out_phase == 0u) {
                     const uint64_t vs = (r0 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u);

@@ -100,12 +100,13 @@ def test_empty_and_tiny_segments(cuda_ready):
 @pytest.mark.parametrize("m", [3, 16])
 def test_group_partition_edges(cuda_ready, m):
     """Small segments are partitioned by a whole CTA per group, each thread
-    owning k consecutive elements (k odd, at most 23 for u32): lengths at and
-    around those per-thread spans, around the group window (1536 elements)
-    and the small-segment bound (4096), runs of empty segments, and groups cut
+    owning k consecutive elements (k odd, at most 33 for u32): lengths at and
+    around those per-thread spans, around the group window and the
+    small-segment bound (both 4096), runs of empty segments, and groups cut
     after 128 segments."""
     rng = np.random.default_rng(40 + m)
-    pool = [0, 0, 0, 1, 2, 21, 22, 23, 24, 25, 45, 46, 47, 69, 1535, 1536, 1537, 3000, 4095, 4096]
+    pool = [0, 0, 0, 1, 2, 7, 9, 21, 23, 31, 32, 33, 34, 65, 66, 67, 99, 1535, 2048, 3000, 4095,
+            4096]
     lengths = rng.choice(pool, size=6000)
     lengths[1000:1400] = 1  # 400 one-element segments in a row
     offs = offsets_from_lengths(lengths)
