@@ -483,6 +483,13 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     seg_plan_spans<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
     seg_plan_emit<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
     main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d);
+    {
+        auto count_fn = seg_run_count<V, D, M, kThreads>;
+        int cblocks = 0;
+        if (occupancy(reinterpret_cast<const void*>(count_fn), 0, &cblocks, &sms) != cudaSuccess)
+            return MDX_ERR_CUDA;
+        count_fn<<<static_cast<uint32_t>(cblocks) * sms, kThreads, 0, st>>>(a, d);
+    }
     // a warp per 32 runs (the run count is on the device: enough for the capacity)
     const uint64_t scan_blocks = std::min<uint64_t>((L.max_runs + 255) / 256, 4096);
     seg_run_scan<M><<<static_cast<uint32_t>(scan_blocks), 256, 0, st>>>(a);

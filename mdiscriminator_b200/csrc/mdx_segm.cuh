@@ -3,7 +3,7 @@
 // Replaces mdiscrSegm<DISCR> (cuda_code/MdiscrSegmHost.cu.h:36-230: a chain
 // of ~12 kernels -- segmented scans of head flags and of N one-hot m-tuples,
 // per-element reductions, class offsets, indices, permute, sizes -- with nine
-// N-sized temporaries, four of them N*m tuples) by five launches:
+// N-sized temporaries, four of them N*m tuples) by six launches:
 //
 //   seg_plan_spans  per segment: its length.  Segments longer than one tile
 //                   (P elements) are "large" and are cut into runs of up to
@@ -14,20 +14,19 @@
 //                   block totals, records the counts and resets the tickets.
 //   seg_plan_emit   writes the run entries {segment, [p0, p1), last run of
 //                   the segment} and the group heads, in element order.
-//   seg_main        persistent; CTAs take tickets in order:
-//                     * batches of groups: each group's range is read into
-//                       shared memory by one bulk copy (the next group's copy
-//                       overlaps the current group's work) and partitioned by
-//                       the whole CTA (seg_group_cta: every thread owns ~L/256
-//                       consecutive elements whatever the segment lengths; a
-//                       segmented scan of per-thread class counts, the
-//                       segments' class bases in shared memory) into a shared
-//                       output image written back with 16-byte stores -- one
-//                       HBM read and one write per element;
-//                     * then the class counts of every run (16-byte loads).
-//   seg_run_scan    per large segment (a warp, lanes over its runs): the
-//                   runs' exclusive class prefixes, the segment's sizes and
-//                   head flags, and every run's output position per class.
+//   seg_main        persistent; CTAs take tickets for batches of groups.
+//                   Each group's range is read into shared memory by one bulk
+//                   copy and partitioned by the whole CTA (seg_group_cta:
+//                   every thread owns ~L/256 consecutive elements whatever the
+//                   segment lengths; a segmented scan of per-thread class
+//                   counts, the segments' class bases in shared memory) into
+//                   a shared output image written back with 16-byte stores --
+//                   one HBM read and one write per element;
+//   seg_run_count   the class counts of every run of the large segments,
+//                   one CTA per run (16-byte loads, warp reductions).
+//   seg_run_scan    per large segment (a lane, or a warp for many runs):
+//                   the runs' exclusive class prefixes, the segment's sizes
+//                   and head flags, and every run's output position per class.
 //   seg_run_scatter persistent; the runs in reverse order through a TMA ring
 //                   and tile_scatter (as the plain scatter), from those
 //                   positions.
@@ -83,7 +82,8 @@ struct SegHeader {      // lives at the start of the segmented workspace
     uint32_t flags_epoch;   // look-back epoch of the flags converter
     uint32_t num_groups;    // small-segment groups this call
     uint32_t ticket2;       // run-scatter ticket counter (reset by the planner)
-    uint32_t pad[2];
+    uint32_t ticket3;       // run-count ticket counter (reset by the planner)
+    uint32_t pad[1];
 };
 
 struct RunEntry {       // a run of up to run_tiles tiles of one large segment
@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         a.hdr->epoch = e;
         a.hdr->ticket = 0u;
         a.hdr->ticket2 = 0u;
+        a.hdr->ticket3 = 0u;
         a.hdr->plan_done = 0u;
         // head-flag converter state for its next call
         a.hdr->flags_ticket = 0u;
@@ -645,7 +646,6 @@ __global__ void __launch_bounds__(THREADS, 3)
     seg_main(SegArgs a, D d) {
     using L = SegSmem<V, M, THREADS, STAGES>;
     constexpr uint32_t AU = L::kAU;
-    constexpr int W = THREADS / 32;
     static_assert(M <= 16 && M >= 2, "class bound");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -658,13 +658,12 @@ __global__ void __launch_bounds__(THREADS, 3)
     __shared__ uint32_t ticket_sh[2];
     __shared__ uint32_t gi_h[2], gi_he[2];  // group pipeline slots
     __shared__ uint64_t gi_r0[2], gi_r1[2], gi_as[2], gi_tail[2];
-    __shared__ uint32_t red[W][M];
     __shared__ GroupScratch<M, THREADS> gs;
     __shared__ uint32_t gb_h[kMaxGroupBatch], gb_he[kMaxGroupBatch];  // the batch's groups
     __shared__ uint64_t gb_r0[kMaxGroupBatch], gb_r1[kMaxGroupBatch];
     __shared__ uint64_t cmod[17];  // DiscrMod constants for m = 1 .. 16
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const V* in = static_cast<const V*>(a.in);
     V* out = static_cast<V*>(a.out);
     const uint32_t out_phase =
@@ -672,10 +671,13 @@ __global__ void __launch_bounds__(THREADS, 3)
     const bool in_vec = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
     const bool out_vec = (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
     const uint64_t S = seg_count(a);
-    const uint32_t num_runs = a.hdr->num_runs;
     const uint32_t num_groups = a.hdr->num_groups;
-    const uint32_t num_batches = (num_groups + a.group_batch - 1) / a.group_batch;
-    const uint32_t total = num_batches + num_runs;
+    // groups per ticket: the tuned batch, but no more than spreads the groups
+    // over every CTA (a few groups must not queue up on one CTA)
+    const uint32_t batch =
+        max(1u, min(a.group_batch, (num_groups + gridDim.x - 1) / gridDim.x));
+    const uint32_t num_batches = (num_groups + batch - 1) / batch;
+    const uint32_t total = num_batches;
     uint32_t group_uses = 0;
 
     if (tid == 0) {
@@ -698,8 +700,8 @@ __global__ void __launch_bounds__(THREADS, 3)
             // group i of the batch: segments [h, he), elements [r0, r1); its
             // range is fetched by one bulk copy while the previous group is
             // partitioned
-            const uint32_t g0 = t * a.group_batch;
-            const uint32_t gcnt = min(a.group_batch, num_groups - g0);
+            const uint32_t g0 = t * batch;
+            const uint32_t gcnt = min(batch, num_groups - g0);
             // the batch's group heads, ends and element ranges, loaded once
             if (tid < static_cast<int>(gcnt)) {
                 const uint32_t h = a.groups[g0 + tid];
@@ -788,68 +790,86 @@ __global__ void __launch_bounds__(THREADS, 3)
             if (failed) break;
             continue;
         }
+    }
+}
 
-        // ---------------- class counts of run j of a large segment ----------
-        const uint32_t j = t - num_batches;
+// Class counts of every run of the large segments: one CTA per run (run
+// tickets), 16-byte loads four deep per thread, per-thread packed counters,
+// warp reductions and one barrier per run.  A few hundred bytes of shared
+// memory, so more CTAs per SM than the group kernel keep loads in flight.
+template <class V, class D, int M, int THREADS>
+__global__ void __launch_bounds__(THREADS, 4) seg_run_count(SegArgs a, D d) {
+    constexpr uint32_t AU = 16 / sizeof(V);
+    constexpr int W = THREADS / 32;
+    __shared__ uint32_t red[W][M];
+    __shared__ uint32_t ticket_sh[2];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const V* in = static_cast<const V*>(a.in);
+    const bool in_vec = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
+    const uint32_t num_runs = a.hdr->num_runs;
+    for (uint32_t it = 0;; it++) {
+        if (tid == 0) ticket_sh[it & 1u] = atomicAdd(&a.hdr->ticket3, 1u);
+        __syncthreads();
+        const uint32_t j = ticket_sh[it & 1u];
+        if (j >= num_runs) break;
         const RunEntry ent = a.runs[j];
         const D dj = seg_discr(a, d, ent.seg);
+        PackedCounts<M> pc;
+        pc.init();
+        const uint64_t p0 = ent.p0, p1 = ent.p1;
+        const uint64_t vs = in_vec ? ((p0 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u)) : p1;
+        const uint64_t ve = in_vec ? max(vs, p1 & ~static_cast<uint64_t>(AU - 1u)) : p1;
         {
-            PackedCounts<M> pc;
-            pc.init();
-            const uint64_t p0 = ent.p0, p1 = ent.p1;
-            const uint64_t vs = in_vec ? ((p0 + AU - 1u) & ~static_cast<uint64_t>(AU - 1u)) : p1;
-            const uint64_t ve = in_vec ? max(vs, p1 & ~static_cast<uint64_t>(AU - 1u)) : p1;
-            {
-                uint32_t k = 0;
-                for (uint64_t e = p0 + tid; e < min(vs, p1); e += THREADS) {
-                    pc.add(dj(in[e]));
-                    if (++k == 8u) {
-                        pc.fold();
-                        k = 0;
-                    }
-                }
-                for (uint64_t e = ve + tid; e < p1 && vs < p1; e += THREADS) {
-                    pc.add(dj(in[e]));
-                    if (++k == 8u) {
-                        pc.fold();
-                        k = 0;
-                    }
-                }
-                pc.fold();
-            }
-            {
-                const uint4* vp = reinterpret_cast<const uint4*>(in + vs);
-                const uint32_t nv = static_cast<uint32_t>((ve - vs) / AU);
-                constexpr int UNROLL = 4;
-                for (uint32_t q = tid; q < nv; q += THREADS * UNROLL) {
-                    uint4 r[UNROLL];
-#pragma unroll
-                    for (int uu = 0; uu < UNROLL; uu++)
-                        if (q + uu * THREADS < nv) r[uu] = __ldg(vp + q + uu * THREADS);
-#pragma unroll
-                    for (int uu = 0; uu < UNROLL; uu++) {
-                        if (q + uu * THREADS < nv) {
-                            V e[AU];
-                            unpack16_to<V>(r[uu], e);
-#pragma unroll
-                            for (uint32_t z = 0; z < AU; z++) pc.add(dj(e[z]));
-                        }
-                        if (uu & 1) pc.fold();  // every two vectors: <= 8 increments
-                    }
+            uint32_t k = 0;
+            for (uint64_t e = p0 + tid; e < min(vs, p1); e += THREADS) {
+                pc.add(dj(in[e]));
+                if (++k == 8u) {
+                    pc.fold();
+                    k = 0;
                 }
             }
-            pc.finish();
+            for (uint64_t e = ve + tid; e < p1 && vs < p1; e += THREADS) {
+                pc.add(dj(in[e]));
+                if (++k == 8u) {
+                    pc.fold();
+                    k = 0;
+                }
+            }
+            pc.fold();
+        }
+        {
+            const uint4* vp = reinterpret_cast<const uint4*>(in + vs);
+            const uint32_t nv = static_cast<uint32_t>((ve - vs) / AU);
+            constexpr int UNROLL = 4;
+            for (uint32_t q = tid; q < nv; q += THREADS * UNROLL) {
+                uint4 r[UNROLL];
 #pragma unroll
-            for (int c = 0; c < M; c++) {
-                const uint32_t x = warp_sum(pc.acc[c]);
-                if (lane == 0) red[warp][c] = x;
+                for (int uu = 0; uu < UNROLL; uu++)
+                    if (q + uu * THREADS < nv) r[uu] = __ldg(vp + q + uu * THREADS);
+#pragma unroll
+                for (int uu = 0; uu < UNROLL; uu++) {
+                    if (q + uu * THREADS < nv) {
+                        V e[AU];
+                        unpack16_to<V>(r[uu], e);
+#pragma unroll
+                        for (uint32_t z = 0; z < AU; z++) pc.add(dj(e[z]));
+                    }
+                    if (uu & 1) pc.fold();  // every two vectors: <= 8 increments
+                }
             }
-            __syncthreads();
-            if (tid < M) {
-                uint32_t agg = 0;
-                for (int w = 0; w < W; w++) agg += red[w][tid];
-                a.run_cnt[static_cast<uint64_t>(j) * M + tid] = agg;
-            }
+        }
+        pc.finish();
+#pragma unroll
+        for (int c = 0; c < M; c++) {
+            const uint32_t x = warp_sum(pc.acc[c]);
+            if (lane == 0) red[warp][c] = x;
+        }
+        __syncthreads();
+        if (tid < static_cast<uint32_t>(M)) {
+            uint32_t agg = 0;
+#pragma unroll
+            for (int w = 0; w < W; w++) agg += red[w][tid];
+            a.run_cnt[static_cast<uint64_t>(j) * M + tid] = agg;
         }
     }
 }
