@@ -69,14 +69,14 @@ __device__ __forceinline__ uint32_t st_epoch(uint64_t w) { return static_cast<ui
 __device__ __forceinline__ uint64_t st_state(uint64_t w) { return (w >> 32) & 3ull; }
 
 struct SegHeader {      // lives at the start of the segmented workspace
-    uint32_t ticket;    // persistent-kernel ticket counter (reset by the planner)
+    uint32_t ticket;    // seg_main's group-batch tickets (reset by the planner)
     uint32_t error;     // latched error bits
-    uint32_t epoch;     // look-back epoch of the current call (1 .. 2^30-1)
+    uint32_t reserved0;
     uint32_t num_runs;  // large-segment runs this call
-    uint32_t lag;       // unused
+    uint32_t reserved1;
     uint32_t plan_done; // planner CTA ticket
     uint64_t num_segs;  // S (written by the flags converter for the head-flag form)
-    uint32_t lag_cur;   // unused
+    uint32_t reserved2;
     uint32_t flags_ticket;  // tile ticket of the flags converter
     uint32_t flags_done;    // finished tiles of the flags converter
     uint32_t flags_epoch;   // look-back epoch of the flags converter
@@ -116,7 +116,7 @@ struct SegArgs {
     uint32_t plan_blocks;
     uint32_t max_runs;         // capacity (enough for segments that tile [0, n))
     uint32_t max_groups;
-    int use_tma;               // the tensor map passed to seg_main is valid
+    int use_tma;               // the tensor map passed to seg_run_scatter is valid
     const uint32_t* seg_m;     // per-segment class counts (remainder discriminator), or null:
                                // every segment uses the launch's discriminator
     uint32_t m_bound;          // classes of any segment are < m_bound (per-segment m clamped)
@@ -243,9 +243,6 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
     }
     __syncthreads();
     if (tid == 0) {
-        uint32_t e = a.hdr->epoch + 1u;
-        if (e >= (1u << 30) || e == 0u) e = 1u;
-        a.hdr->epoch = e;
         a.hdr->ticket = 0u;
         a.hdr->ticket2 = 0u;
         a.hdr->ticket3 = 0u;
