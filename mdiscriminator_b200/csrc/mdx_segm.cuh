@@ -1013,7 +1013,8 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     const uint32_t out_phase =
         static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
     const bool tma_ok = a.use_tma != 0;
-    const uint64_t map_elems = (a.n * sizeof(V) / 128u) * (128u / sizeof(V));
+    constexpr uint32_t kPerRow = 128u / sizeof(V);  // elements per 128-byte row
+    const uint64_t map_elems = (a.n * sizeof(V) / 128u) * kPerRow;
     const uint32_t num_runs = a.hdr->num_runs;
     uint32_t ring_uses = 0;  // mbarrier phase bookkeeping across runs
 
@@ -1034,20 +1035,22 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         const D dj = seg_discr(a, d, ent.seg);
         if (tid < M) sh.cursor[0][tid] = __ldcg(a.run_base + static_cast<uint64_t>(j) * M + tid);
         __syncthreads();
-        const uint32_t wf = ent.p0 / P, wl = (ent.p1 - 1u) / P;
-        const uint32_t ntiles = wl - wf + 1u;
-        // a tile (partial ones too) comes by TMA when the run's part of it lies
-        // inside the tensor map (the input's whole 128-byte rows; rows past the
-        // map read as zeros and lie outside the run)
-        auto via_tma = [&](uint32_t w) {
-            return tma_ok && min(static_cast<uint64_t>(ent.p1), static_cast<uint64_t>(w + 1) * P) <= map_elems;
+        // the run's tiles start at the 128-byte row holding its first element
+        // (not at multiples of P), so only its last tile is short
+        const uint64_t rb = ent.p0 & ~static_cast<uint64_t>(kPerRow - 1u);
+        const uint32_t ntiles = static_cast<uint32_t>((ent.p1 - rb + P - 1u) / P);
+        // a tile comes by TMA when the run's part of it lies inside the tensor
+        // map (the input's whole 128-byte rows; rows past the map read as zeros
+        // and lie outside the run)
+        auto via_tma = [&](uint32_t i) {
+            return tma_ok && min(static_cast<uint64_t>(ent.p1), rb + static_cast<uint64_t>(i + 1) * P) <= map_elems;
         };
-        auto issue = [&](uint32_t i) {  // tile wf+i into ring slot (ring_uses+i) % STAGES
-            const uint32_t w = wf + i;
+        auto issue = [&](uint32_t i) {  // tile i of the run into ring slot (ring_uses+i) % STAGES
             const uint32_t slot = (ring_uses + i) % STAGES;
-            if (via_tma(w)) {
+            if (via_tma(i)) {
                 mbar_arrive_expect_tx(&bars[slot], P * sizeof(V));
-                tma_load_2d(ring + slot * P, &tmap, 0, static_cast<int32_t>(w * ROWS), &bars[slot]);
+                tma_load_2d(ring + slot * P, &tmap, 0,
+                            static_cast<int32_t>(rb / kPerRow + static_cast<uint64_t>(i) * ROWS), &bars[slot]);
             } else {
                 mbar_arrive(&bars[slot]);
             }
@@ -1057,15 +1060,14 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         const uint32_t e0 = tid * ITEMS;
         bool failed = false;
         for (uint32_t i = 0; i < ntiles; i++) {
-            const uint32_t w = wf + i;
-            const uint64_t ts = static_cast<uint64_t>(w) * P;
+            const uint64_t ts = rb + static_cast<uint64_t>(i) * P;
             const uint32_t lo = static_cast<uint32_t>(max(static_cast<uint64_t>(ent.p0), ts) - ts);
             const uint32_t hi = static_cast<uint32_t>(min(static_cast<uint64_t>(ent.p1), ts + P) - ts);
             const bool full = lo == 0u && hi == static_cast<uint32_t>(P);
             const uint32_t use = ring_uses + i;
             const bool ok = mbar_wait_bounded(&bars[use % STAGES], (use / STAGES) & 1u);
             V v[ITEMS];
-            if (via_tma(w)) {
+            if (via_tma(i)) {
                 take_swizzled<V, ITEMS>(ring + (use % STAGES) * P, v);
             } else {
 #pragma unroll
