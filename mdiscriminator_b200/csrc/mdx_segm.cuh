@@ -54,11 +54,12 @@ namespace mdx {
 
 // Defaults of the run-time knobs (the autotuner may choose others):
 constexpr int kRunTiles = 8;     // tiles per run of a large segment
-constexpr int kGroupBatch = 8;   // small-segment groups per work item (pipelined)
+constexpr int kGroupBatch = 8;   // small-segment groups per ticket of seg_main
 constexpr int kMaxGroupBatch = 32;
 constexpr int kLagSlackPct = 50; // accepted in the tuning table, no longer used
 
-// status word: [63:34] epoch (30 bits), [33:32] state, [31:0] count
+// look-back status word of the head-flag converter: [63:34] epoch (30 bits),
+// [33:32] state, [31:0] count
 constexpr uint64_t kStAgg = 1ull;
 constexpr uint64_t kStInc = 2ull;
 
@@ -364,8 +365,8 @@ __device__ __forceinline__ bool wait_status(const uint64_t* p, uint32_t epoch, u
     }
 }
 
-// Per-lane class counters in 16-bit fields (M <= 16: (M+1)/2 words), wide
-// enough for a whole segment's totals after a warp scan (<= 2P < 2^16).
+// Per-thread class counters in 16-bit fields (M <= 16: (M+1)/2 words), wide
+// enough for any count within one group (< 2P < 2^16 elements).
 template <int M>
 struct HalfCounts {
     static constexpr int NW = (M + 1) / 2;
