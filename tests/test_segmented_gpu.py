@@ -114,6 +114,33 @@ def test_group_partition_edges(cuda_ready, m):
     check(cuda_ready, x, offs, m)
 
 
+@pytest.mark.parametrize("m", [4, 16])
+def test_unaligned_buffers(cuda_ready, m):
+    """Input and output views off their 16-byte alignment: the group copies,
+    run counts and run scatter fall back from bulk copies, 16-byte loads and
+    TMA to element loads and stores; the result must not change."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    lengths = np.concatenate([lognormal_lengths(400, 60 + m), [20000, 3, 70000, 1, 4097]])
+    offs = offsets_from_lengths(lengths)
+    n = int(offs[-1])
+    x = oracle.fill_uniform_u32(n, 61 + m)
+    eo, es, ef = oracle.partition_segmented(x, offs, m, kind=oracle.DISCR_MOD, headflags=True)
+    for din, dout in ((1, 0), (0, 3), (3, 1)):
+        base_in = torch.zeros(n + 4, dtype=torch.int32, device="cuda")
+        base_in[din:din + n] = torch.from_numpy(x.view(np.int32)).cuda()
+        base_out = torch.zeros(n + 4, dtype=torch.int32, device="cuda")
+        d_in, d_out = base_in[din:din + n], base_out[dout:dout + n]
+        out, seg_sizes, hf = mdx.partition_segmented(
+            d_in, torch.from_numpy(offs.view(np.int64)).cuda(), ("mod", m), out=d_out,
+            headflags=True)
+        torch.cuda.synchronize()
+        assert mdx.workspace(0).error() == mdx.MDX_OK
+        assert np.array_equal(d_out.cpu().numpy().view(np.uint32), eo), (din, dout)
+        assert np.array_equal(seg_sizes.cpu().numpy(), es)
+        assert np.array_equal(hf.cpu().numpy(), ef)
+
+
 def test_single_huge_segment_equals_plain(cuda_ready):
     n = (1 << 22) + 123
     x = oracle.fill_uniform_u32(n, 9)
