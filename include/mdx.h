@@ -351,8 +351,8 @@ mdx_status mdx_server_destroy(mdx_server server);
 typedef struct {
     uint32_t plain_ctas_per_sm;  /* plain path: CTAs per SM of the chunk grid (0: as many as fit) */
     uint32_t run_tiles;          /* segmented: tiles per run of a large segment (default 8) */
-    uint32_t group_batch;        /* segmented: small-segment groups per work item (default 8) */
-    uint32_t lag_slack_pct;      /* segmented: extra lag of scatter items, % of the grid (default 50) */
+    uint32_t group_batch;        /* segmented: small-segment groups per work item (default 8, at most 32) */
+    uint32_t lag_slack_pct;      /* accepted and stored (default 50); no kernel reads it any more */
 } mdx_tuning;
 
 mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,
