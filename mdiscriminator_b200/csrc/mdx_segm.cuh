@@ -376,15 +376,27 @@ struct HalfCounts {
         for (int q = 0; q < NW; q++) w[q] = 0;
     }
     __device__ __forceinline__ uint32_t get(uint32_t c) const {
-        uint32_t x = w[0];
+        if constexpr (NW == 2) {  // four fields: one 64-bit shift
+            const uint64_t x = (static_cast<uint64_t>(w[1]) << 32) | w[0];
+            return static_cast<uint32_t>(x >> (c << 4)) & 0xffffu;
+        } else {
+            uint32_t x = w[0];
 #pragma unroll
-        for (int q = 1; q < NW; q++) x = (c >> 1) == static_cast<uint32_t>(q) ? w[q] : x;
-        return (x >> ((c & 1u) << 4)) & 0xffffu;
+            for (int q = 1; q < NW; q++) x = (c >> 1) == static_cast<uint32_t>(q) ? w[q] : x;
+            return (x >> ((c & 1u) << 4)) & 0xffffu;
+        }
     }
     __device__ __forceinline__ void inc(uint32_t c) {
-        const uint32_t one = 1u << ((c & 1u) << 4);
+        if constexpr (NW == 2) {
+            uint64_t x = (static_cast<uint64_t>(w[1]) << 32) | w[0];
+            x += 1ull << (c << 4);
+            w[0] = static_cast<uint32_t>(x);
+            w[1] = static_cast<uint32_t>(x >> 32);
+        } else {
+            const uint32_t one = 1u << ((c & 1u) << 4);
 #pragma unroll
-        for (int q = 0; q < NW; q++) w[q] += (c >> 1) == static_cast<uint32_t>(q) ? one : 0u;
+            for (int q = 0; q < NW; q++) w[q] += (c >> 1) == static_cast<uint32_t>(q) ? one : 0u;
+        }
     }
 };
 
