@@ -379,6 +379,10 @@ struct HalfCounts {
         if constexpr (NW == 2) {  // four fields: one 64-bit shift
             const uint64_t x = (static_cast<uint64_t>(w[1]) << 32) | w[0];
             return static_cast<uint32_t>(x >> (c << 4)) & 0xffffu;
+        } else if constexpr (NW == 4) {  // eight fields: two 64-bit halves
+            const uint64_t lo = (static_cast<uint64_t>(w[1]) << 32) | w[0];
+            const uint64_t hi = (static_cast<uint64_t>(w[3]) << 32) | w[2];
+            return static_cast<uint32_t>(((c & 4u) ? hi : lo) >> ((c & 3u) << 4)) & 0xffffu;
         } else {
             uint32_t x = w[0];
 #pragma unroll
@@ -392,6 +396,15 @@ struct HalfCounts {
             x += 1ull << (c << 4);
             w[0] = static_cast<uint32_t>(x);
             w[1] = static_cast<uint32_t>(x >> 32);
+        } else if constexpr (NW == 4) {
+            uint64_t lo = (static_cast<uint64_t>(w[1]) << 32) | w[0];
+            uint64_t hi = (static_cast<uint64_t>(w[3]) << 32) | w[2];
+            const uint64_t one = 1ull << ((c & 3u) << 4);
+            if (c & 4u) hi += one; else lo += one;
+            w[0] = static_cast<uint32_t>(lo);
+            w[1] = static_cast<uint32_t>(lo >> 32);
+            w[2] = static_cast<uint32_t>(hi);
+            w[3] = static_cast<uint32_t>(hi >> 32);
         } else {
             const uint32_t one = 1u << ((c & 1u) << 4);
 #pragma unroll
