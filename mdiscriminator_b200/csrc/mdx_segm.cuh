@@ -383,6 +383,14 @@ struct HalfCounts {
             const uint64_t lo = (static_cast<uint64_t>(w[1]) << 32) | w[0];
             const uint64_t hi = (static_cast<uint64_t>(w[3]) << 32) | w[2];
             return static_cast<uint32_t>(((c & 4u) ? hi : lo) >> ((c & 3u) << 4)) & 0xffffu;
+        } else if constexpr (NW == 8) {  // sixteen fields: four 64-bit quarters
+            uint64_t x = (static_cast<uint64_t>(w[1]) << 32) | w[0];
+#pragma unroll
+            for (int q = 1; q < 4; q++)
+                x = (c >> 2) == static_cast<uint32_t>(q)
+                        ? (static_cast<uint64_t>(w[2 * q + 1]) << 32) | w[2 * q]
+                        : x;
+            return static_cast<uint32_t>(x >> ((c & 3u) << 4)) & 0xffffu;
         } else {
             uint32_t x = w[0];
 #pragma unroll
@@ -405,6 +413,15 @@ struct HalfCounts {
             w[1] = static_cast<uint32_t>(lo >> 32);
             w[2] = static_cast<uint32_t>(hi);
             w[3] = static_cast<uint32_t>(hi >> 32);
+        } else if constexpr (NW == 8) {
+            const uint64_t one = 1ull << ((c & 3u) << 4);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                uint64_t x = (static_cast<uint64_t>(w[2 * q + 1]) << 32) | w[2 * q];
+                if ((c >> 2) == static_cast<uint32_t>(q)) x += one;
+                w[2 * q] = static_cast<uint32_t>(x);
+                w[2 * q + 1] = static_cast<uint32_t>(x >> 32);
+            }
         } else {
             const uint32_t one = 1u << ((c & 1u) << 4);
 #pragma unroll
