@@ -36,16 +36,19 @@ struct NibbleCounts {
     __device__ __forceinline__ uint32_t get(uint32_t c) const {
         if constexpr (NW == 1) {
             return (w[0] >> (c << 2)) & 15u;
-        } else {
-            return (((c < 8u) ? w[0] : w[1]) >> ((c & 7u) << 2)) & 15u;
+        } else {  // sixteen nibbles: one 64-bit shift
+            const uint64_t x = (static_cast<uint64_t>(w[1]) << 32) | w[0];
+            return static_cast<uint32_t>(x >> (c << 2)) & 15u;
         }
     }
     __device__ __forceinline__ void inc(uint32_t c) {
         if constexpr (NW == 1) {
             w[0] += 1u << (c << 2);
         } else {
-            const uint32_t one = 1u << ((c & 7u) << 2);
-            if (c < 8u) w[0] += one; else w[1] += one;
+            uint64_t x = (static_cast<uint64_t>(w[1]) << 32) | w[0];
+            x += 1ull << (c << 2);
+            w[0] = static_cast<uint32_t>(x);
+            w[1] = static_cast<uint32_t>(x >> 32);
         }
     }
 };
