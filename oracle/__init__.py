@@ -36,9 +36,25 @@ _lib = None
 _ref = None
 
 
+def reference_sources() -> str | None:
+    """The reference checkout's ``cuda_code/`` directory, or None.
+
+    ``MDX_REF_SRC`` names it; otherwise a checkout named ``reference`` beside
+    the repository directory is used when it holds ``SeqMdiscr.h``."""
+    env = os.environ.get("MDX_REF_SRC")
+    if env:
+        return env
+    beside = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "cuda_code")
+    return beside if os.path.exists(os.path.join(beside, "SeqMdiscr.h")) else None
+
+
 def build(quiet: bool = True) -> None:
     """Compile the oracle (and, where the reference sources exist, _ref)."""
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    cmd = ["make", "-C", HERE]
+    src = reference_sources()
+    if src:
+        cmd.append(f"REF_SRC={src}")
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
