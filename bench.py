@@ -2,9 +2,10 @@
 
 Workload (one "step" = one partition of one synthetic batch resident in HBM):
 plain mdiscr, N = 2^28 int32 values uniform over [0, 2^31) from a seeded
-generator, m = 8, class = value mod 8 (Mod8: value & 7), stable; outputs the
-permuted array and the 8 class sizes.  Inputs (1 GiB) and outputs (1 GiB) are
-larger than the 126 MB L2, so no flush is needed between steps.
+generator (mdiscriminator_b200.workloads, seed "c2a"), m = 8, class = value
+mod 8 (Mod8: value & 7), stable; outputs the permuted array and the 8 class
+sizes.  Inputs (1 GiB) and outputs (1 GiB) are larger than the 126 MB L2, so
+no flush is needed between steps.
 
 Printed JSON (rank 0, one line):
   value      elements/s over all ranks, kernels only, inputs resident in HBM
@@ -14,16 +15,24 @@ Printed JSON (rank 0, one line):
   roofline   the partition call against the HBM roofline of reading and
              writing each element once (2*N*4 + 4*m bytes), and each of its
              two kernels against its own algorithmic bytes
+  configs    every other plain configuration of the benchmark list, each on
+             its own seeded input: N=2^20 m=4 (L2 flushed between reps), the
+             Zipf-skewed N=2^28 m=8, and N=2^27 8-byte records at m in
+             {2,4,16,32,64}, random and pre-sorted by class
+  batched    100,000 log-normal segments, offsets form and head-flag form
+  served     Poisson request arrivals through the serving loop
   cpu_baseline  the reference's OpenmpMdiscr (compiled from its sources,
-             oracle/_ref) on a bounded sample, on this host's cores
+             oracle/_ref) on the same input as the GPU (the whole array when
+             host memory allows), on this host's cores; its seqMdiscr on one
+             core on a prefix of that input
 
 --impl reference runs the reference's own CPU implementation (OpenmpMdiscr)
-instead, on rank 0 only, with every host thread, on bounded samples of the
-same workload.
+instead, on rank 0 only, with every host thread, on the same seeded input.
 
 Multi-GPU (torchrun, one process per GPU): every rank partitions its own
 N = 2^28 array (independent units, no data-path collective; weak scaling);
-the step time is the max over ranks.
+the step time is the max over ranks.  --distributed instead partitions one
+array spread over the ranks (count all-gather + scatter into peer chunks).
 """
 from __future__ import annotations
 
@@ -134,31 +143,28 @@ class ClockSampler:
 
 
 def make_input(torch, n, seed, device):
-    g = torch.Generator(device=device).manual_seed(seed)
-    return torch.randint(0, 1 << 31, (n,), device=device, dtype=torch.int64,
-                         generator=g).to(torch.int32)
-
-
-def lognormal_lengths(S: int, seed: int, mu: float, sigma: float, hi: int):
-    import numpy as np
-    rng = np.random.default_rng(seed)
-    return np.clip(np.rint(rng.lognormal(mu, sigma, size=S)), 1, hi).astype(np.int64)
+    """n int32 values uniform over [0, 2^31): the splitmix64 stream of
+    mdiscriminator_b200.workloads, generated on the device."""
+    from mdiscriminator_b200 import workloads as W
+    return W.uniform_u32_torch(torch, n, seed, device)
 
 
 def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segments=2000,
-                        num_segments=100_000, keep="all", with_plain=True):
+                        num_segments=100_000, keep="all", with_plain=True, with_flags=True):
     """Batched segmented partition: 100,000 segments, lengths
     LogNormal(ln 1024, 1.5) clamped to [1, 2^22] (~3e8 int32), m = 4,
     class = v mod 4, as one segmented call replayed from a CUDA graph, against
     one plain partition per segment (a CUDA graph of per-segment calls over a
-    sample of consecutive segments).  ``keep`` = "large" / "small" keeps only
-    the segments longer than / at most one 4096-element tile (for profiling the
-    two halves of the kernel)."""
-    import math
-
+    sample of consecutive segments).  The same segments are also given in the
+    reference's head-flag form (mdiscrSegm: i32 length at every segment start,
+    head-flag class sizes out), timed the same way.  ``keep`` = "large" /
+    "small" keeps only the segments longer than / at most one 4096-element
+    tile (for profiling the two halves of the kernel)."""
     import numpy as np
+
+    from mdiscriminator_b200 import workloads as W
     m = 4
-    lengths = lognormal_lengths(num_segments, 2024, math.log(1024), 1.5, 1 << 22)
+    lengths = W.lognormal_lengths(num_segments, W.SEEDS["c4"])
     if keep == "large":
         lengths = lengths[lengths > 4096]
     elif keep == "small":
@@ -166,30 +172,36 @@ def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segmen
     S = len(lengths)
     offs = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)
     n = int(offs[-1])
-    d_in = make_input(torch, n, 99, dev)
+    d_in = make_input(torch, n, W.SEEDS["c4"], dev)
     d_out = torch.empty_like(d_in)
     d_offs = torch.from_numpy(offs).to(dev)
     seg_sizes = torch.empty((S, m), dtype=torch.uint32, device=dev)
     ws = mdx.new_workspace(mdx.segmented_workspace_size(n, S, mdx.ELEM_U32, m), dev)
     stream = torch.cuda.Stream(device=dev)
-    with torch.cuda.stream(stream):
-        for _ in range(warmup):
-            mdx.partition_segmented(d_in, d_offs, ("mod", m), out=d_out, seg_sizes=seg_sizes, ws=ws)
-        stream.synchronize()
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=stream):
-            mdx.partition_segmented(d_in, d_offs, ("mod", m), out=d_out, seg_sizes=seg_sizes, ws=ws)
-        g.replay()
-        stream.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def graph_time(issue, reps):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                issue()
+            stream.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=stream):
+                issue()
             g.replay()
-        e1.record(stream)
-        stream.synchronize()
+            stream.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                g.replay()
+            e1.record(stream)
+            stream.synchronize()
+        del g
+        return e0.elapsed_time(e1) * 1e-3 / reps
+
+    t_b = graph_time(lambda: mdx.partition_segmented(d_in, d_offs, ("mod", m), out=d_out,
+                                                     seg_sizes=seg_sizes, ws=ws), steps)
     if ws.error() != mdx.MDX_OK:
         raise SystemExit("device error in the batched measurement")
-    t_b = e0.elapsed_time(e1) * 1e-3 / steps
     alg = 2 * n * 4 + 8 * (S + 1) + 4 * m * S
     workload = (f"{S:,} segments, LogNormal(ln 1024, 1.5) clamped [1, 2^22]"
                 + ("" if keep == "all" else f" (only the {keep} ones of {num_segments:,})")
@@ -199,8 +211,28 @@ def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segmen
            "ms": t_b * 1e3,
            "roofline": {"bound": "hbm", "achieved": alg / t_b / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": alg / t_b / 1e9 / peak, "alg_bytes": "2*N*4 + 8*(S+1) + 4*m*S"}}
+    if with_flags:
+        # the reference's own form: head-flag segment sizes in, head-flag class
+        # sizes out (mdiscrSegm, MdiscrSegmHost.cu.h:36-42)
+        flags = torch.zeros(n, dtype=torch.int32, device=dev)
+        flags[d_offs[:-1]] = torch.from_numpy(lengths.astype(np.int32)).to(dev)
+        new_sizes = torch.empty(n, dtype=torch.int32, device=dev)
+        fws = mdx.new_workspace(int(mdx.lib().mdx_mdiscr_segm_workspace_size(n, mdx.ELEM_U32, m)),
+                                dev)
+        t_f = graph_time(lambda: mdx.mdiscr_segm(d_in, flags, ("mod", m), d_out=d_out,
+                                                 d_new_sizes=new_sizes, ws=fws), steps)
+        if fws.error() != mdx.MDX_OK:
+            raise SystemExit("device error in the head-flag batched measurement")
+        alg_f = 2 * n * 4 + 4 * n + 4 * n
+        res["head_flag_form"] = {
+            "value": n / t_f / 1e9, "unit": "Gelem/s", "ms": t_f * 1e3,
+            "roofline": {"achieved": alg_f / t_f / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg_f / t_f / 1e9 / peak,
+                         "alg_bytes": "2*N*4 + 4*N (flags in) + 4*N (head-flag sizes out)"},
+            "what": "mdx_mdiscr_segm: i32 segment lengths at segment starts in, i32 head-flag "
+                    "class sizes per segment out, one CUDA graph replay per step"}
+        del flags, new_sizes, fws
     if not with_plain:
-        del g
         return res
     # one plain launch per segment, on a sample of consecutive segments
     s0 = S // 2
@@ -209,25 +241,12 @@ def batched_measurement(torch, mdx, dev, peak, steps=10, warmup=3, sample_segmen
     pws = mdx.new_workspace(max(mdx.workspace_size(int(lengths[s0:s1].max()), mdx.ELEM_U32, m), 1 << 20), dev)
     sizes = torch.empty(m, dtype=torch.uint32, device=dev)
     views = [(int(offs[s]), int(offs[s + 1])) for s in range(s0, s1)]
-    with torch.cuda.stream(stream):
-        for a, b in views[:8]:
+
+    def per_segment():
+        for a, b in views:
             mdx.partition(d_in[a:b], ("mod", m), out=d_out[a:b], sizes=sizes, ws=pws)
-        stream.synchronize()
-        gp = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(gp, stream=stream):
-            for a, b in views:
-                mdx.partition(d_in[a:b], ("mod", m), out=d_out[a:b], sizes=sizes, ws=pws)
-        gp.replay()
-        stream.synchronize()
-        e0.record(stream)
-        reps = 3
-        for _ in range(reps):
-            gp.replay()
-        e1.record(stream)
-        stream.synchronize()
-    t_p = e0.elapsed_time(e1) * 1e-3 / reps
+    t_p = graph_time(per_segment, 3)
     v_p = (a1 - a0) / t_p / 1e9
-    del g, gp
     res["per_segment_plain"] = {"value": v_p, "unit": "Gelem/s",
                                 "sample": f"segments {s0}..{s1 - 1} ({a1 - a0} elements), one "
                                           "mdx_partition per segment, CUDA graph of the calls"}
@@ -274,7 +293,8 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
     import numpy as np
     rng = np.random.default_rng(17)
     src_n = 1 << 28
-    src = make_input(torch, src_n, 5, dev)
+    from mdiscriminator_b200 import workloads as W
+    src = make_input(torch, src_n, W.SEEDS["c5"], dev)
     out_pool = torch.empty(1 << 30, dtype=torch.int32, device=dev)
     sizes_pool = torch.empty((1 << 16, 16), dtype=torch.int32, device=dev)
     res = []
@@ -357,26 +377,131 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
                                             "back to back on one stream (host wall clock)"}}
 
 
-def cpu_baseline(n_sample: int, m: int, reps: int):
-    """The reference's openmpMdiscr on a bounded sample (rank 0, N=1 only)."""
-    import numpy as np
+def time_calls(torch, fn, reps, warmup, flush=None):
+    """Median and mean device time (ms) of ``fn`` over ``reps`` calls, CUDA
+    events around each call on the current stream; ``flush`` (a tensor larger
+    than L2) is rewritten before every call."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(reps)]
+    for a, b in evs:
+        if flush is not None:
+            flush.fill_(7)
+        a.record()
+        fn()
+        b.record()
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    return statistics.median(ms), statistics.mean(ms)
 
+
+def configs_measurement(torch, mdx, dev, peak, reps=10, warmup=3):
+    """The plain configurations of the benchmark list other than the headline,
+    each on its own seeded input generated on the device
+    (mdiscriminator_b200.workloads), timed call by call with CUDA events."""
+    from mdiscriminator_b200 import workloads as W
+    out = []
+
+    def entry(name, d_in, m, what, flush=None):
+        n = d_in.numel()
+        w = d_in.element_size()
+        d_out = torch.empty_like(d_in)
+        sizes = torch.empty(m, dtype=torch.uint32, device=dev)
+        ws = mdx.new_workspace(mdx.workspace_size(n, mdx.ELEM_U32 if w == 4 else mdx.ELEM_REC8, m),
+                               dev)
+        discr = ("mask", m) if (m & (m - 1)) == 0 else ("mod", m)
+        med, mean = time_calls(torch, lambda: mdx.partition(d_in, discr, out=d_out, sizes=sizes,
+                                                            ws=ws), reps, warmup, flush)
+        if ws.error() != mdx.MDX_OK:
+            raise SystemExit(f"device error in config {name}")
+        t = med * 1e-3
+        alg = 2 * n * w + 4 * m
+        out.append({"config": name, "what": what, "n": n, "elem_bytes": w, "m": m,
+                    "ms": med, "ms_mean": mean, "gelem_per_s": n / t / 1e9,
+                    "roofline_frac": alg / t / 1e9 / peak,
+                    "frac_of_two_pass_bound": (3 * n * w + 4 * m) / t / 1e9 / peak})
+        del d_out, sizes, ws
+
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    d = make_input(torch, 1 << 20, W.SEEDS["c1"], dev)
+    entry("c1", d, 4, "N=2^20 int32 uniform, m=4 (class = v mod 4); L2 flushed (512 MB write) "
+                      "before every call", flush)
+    del d, flush
+    d = W.zipf8_torch(torch, 1 << 28, W.SEEDS["c2b"], dev)
+    entry("c2b", d, 8, "N=2^28 int32, class ~ Zipf(1.1) over 8 classes, v = 8*U[0,2^28) + class, "
+                       "m=8 (v & 7)")
+    del d
+    for presorted in (False, True):
+        for m in (2, 4, 16, 32, 64):
+            d = W.records_torch(torch, 1 << 27, W.SEEDS["c3"], m, presorted, dev)
+            entry(f"c3_m{m}" + ("_presorted" if presorted else ""), d, m,
+                  f"N=2^27 8-byte records {{key uniform [0,2^31), payload = index}}, class = "
+                  f"key & {m - 1}" + (", keys pre-sorted by class" if presorted else ""))
+            del d
+    torch.cuda.empty_cache()
+    return out
+
+
+def host_mem_available() -> int:
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def openmp_sample_size(n: int, m: int) -> int:
+    """Largest prefix of the n-element input (n itself when it fits) whose
+    openmpMdiscr run fits in ~60% of the available host memory: input,
+    output, head flags, the per-element classes and two N x m tuple arrays
+    (cuda_code/OpenmpMdiscr.h:18-22)."""
+    per_elem = 4 + 4 + 4 + 4 + 2 * 4 * m
+    fit = int(0.6 * host_mem_available()) // per_elem
+    k = n
+    while k > fit and k > (1 << 20):
+        k //= 2
+    return k
+
+
+def cpu_baseline(x, m: int, reps: int, seq_sample: int = 1 << 25):
+    """The reference's openmpMdiscr on the GPU arm's own input ``x`` (the
+    whole array, or its largest prefix that host memory allows), every host
+    thread; and its seqMdiscr (Mod8 / Mod4 for m = 8 / 4, else Mod<m>) on one
+    core on a prefix of the same input.  Rank 0, N = 1 only."""
     import oracle
     if not oracle.ref_available():
         return None, "oracle/_ref not built"
-    x = oracle.fill_uniform_u32(n_sample, 7)
+    n = x.shape[0]
+    k = openmp_sample_size(n, m)
+    xs = x[:k]
     threads = os.cpu_count() or 1
     best = None
     for _ in range(reps):
-        _, _, us = oracle.ref_openmp(x, m, threads=threads)
+        _, _, us = oracle.ref_openmp(xs, m, threads=threads)
         if us > 0 and (best is None or us < best):
             best = us
     if best is None:
         return None, "reference run failed"
-    return {"value": n_sample / (best * 1e-6) / 1e9, "unit": "Gelem/s", "cores": threads,
-            "kind": "reference",
-            "sample": f"openmpMdiscr (cuda_code/OpenmpMdiscr.h) on {n_sample} uniform int32, m={m}, "
-                      f"best of {reps}, its own gettimeofday timer, OMP threads={threads}"}, None
+    ks = min(seq_sample, n)
+    _, _, seq_us = oracle.ref_seq(x[:ks], m, specialized=m in (4, 8), measure=True)
+    res = {"value": k / (best * 1e-6) / 1e9, "unit": "Gelem/s", "cores": threads,
+           "kind": "reference", "same_input": True,
+           "sample": (f"openmpMdiscr (cuda_code/OpenmpMdiscr.h) on the GPU arm's own input "
+                      + ("(the whole array)" if k == n else
+                         f"(its first {k} elements: the whole array needs more host memory)")
+                      + f", m={m}, best of {reps}, its own gettimeofday timer, OMP threads={threads}")}
+    if seq_us and seq_us > 0:
+        res["seq_single_core"] = {
+            "value": ks / (seq_us * 1e-6) / 1e9, "unit": "Gelem/s", "cores": 1,
+            "sample": f"seqMdiscr<{'Mod%d' % m if m in (4, 8) else 'Mod<%d>' % m}, true> "
+                      f"(cuda_code/SeqMdiscr.h:10-57) on the first {ks} elements of the same "
+                      "input, its own timer, one run"}
+    return res, None
 
 
 def distributed_main(args, torch, dist, mdx, dev, world, rank):
@@ -397,7 +522,8 @@ def distributed_main(args, torch, dist, mdx, dev, world, rank):
                                 world_size=1, device_id=dev)
     n, m = args.n, args.m
     discr = ("mask", m) if (m & (m - 1)) == 0 else ("mod", m)
-    x = make_input(torch, n, 1234 + rank, dev)
+    from mdiscriminator_b200 import workloads as W
+    x = make_input(torch, n, W.SEEDS["c2a"] + rank, dev)
     out = None
     for _ in range(args.warmup):
         out, _ = D.partition_distributed(x, discr, out=out)
@@ -429,35 +555,56 @@ def distributed_main(args, torch, dist, mdx, dev, world, rank):
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU implementation, rank 0 only."""
+    """--impl reference: the reference's CPU implementation (openmpMdiscr,
+    compiled from its sources into oracle/_ref) on rank 0 only, every host
+    thread, on the GPU arm's own seeded input: the whole array when host
+    memory and the run's time allow, else its largest prefix that does."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import oracle
+    from mdiscriminator_b200 import workloads as W
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's "
                           "OpenmpMdiscr build) is missing"}))
         return 0
-    n_sample = args.ref_sample
-    x = oracle.fill_uniform_u32(n_sample, 7)
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        oracle.ref_openmp(x, args.m, threads=threads)
+    x = W.uniform_u32(args.n, W.SEEDS["c2a"])
+    k = openmp_sample_size(args.n, args.m)
+    # keep the whole run within a few minutes: probe one step, halve the
+    # prefix while (warm-up + timed steps) would take longer than budget_s
+    budget_s = 150.0
+    while True:
+        _, _, us = oracle.ref_openmp(x[:k], args.m, threads=threads)
+        if us <= 0:
+            print(json.dumps({"impl": "reference", "unavailable": "openmpMdiscr run failed"}))
+            return 0
+        if (args.steps + args.warmup) * us * 1e-6 <= budget_s or k <= (1 << 20):
+            break
+        k //= 2
+    xs = x[:k]
+    for _ in range(max(args.warmup - 1, 0)):
+        oracle.ref_openmp(xs, args.m, threads=threads)
     times = []
     for _ in range(args.steps):
-        _, _, us = oracle.ref_openmp(x, args.m, threads=threads)
+        _, _, us = oracle.ref_openmp(xs, args.m, threads=threads)
         times.append(us * 1e-6)
     t = statistics.mean(times)
-    value = n_sample / t / 1e9
+    value = k / t / 1e9
+    sample = ("the whole input" if k == args.n else
+              f"the first {k} elements of the same input (the whole array would need more host "
+              "memory or time)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gelem/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": args.n, "m": args.m,
-                   "sample_per_step": n_sample, "parallelism": "host threads"},
+                   "seed": W.SEEDS["c2a"], "sample_per_step": k, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "Gelem/s", "cores": threads, "kind": "reference",
-                         "sample": f"openmpMdiscr on {n_sample} of the workload's elements per step"},
+                         "same_input": True,
+                         "sample": f"openmpMdiscr (cuda_code/OpenmpMdiscr.h) on {sample}, its own "
+                                   "gettimeofday timer"},
         "e2e": {"value": value, "unit": "Gelem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -473,8 +620,9 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--m", type=int, default=M_DEFAULT)
     ap.add_argument("--e2e-steps", type=int, default=6)
-    ap.add_argument("--ref-sample", type=int, default=1 << 25)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other plain configurations")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched segmented measurement")
     ap.add_argument("--no-served", action="store_true",
@@ -520,7 +668,8 @@ def main():
 
     n, m = args.n, args.m
     discr = ("mask", m) if (m & (m - 1)) == 0 else ("mod", m)
-    d_in = make_input(torch, n, 1234 + rank, dev)
+    from mdiscriminator_b200 import workloads as W
+    d_in = make_input(torch, n, W.SEEDS["c2a"] + rank, dev)
     d_out = torch.empty_like(d_in)
     sizes = torch.empty(m, dtype=torch.uint32, device=dev)
     ws = mdx.new_workspace(mdx.workspace_size(n, mdx.ELEM_U32, m), dev)
@@ -663,6 +812,9 @@ def main():
                             "traffic": tr.get("scatter_kernel_bytes")},
             },
         }
+        configs = None
+        if world == 1 and not args.no_configs:
+            configs = configs_measurement(torch, mdx, dev, peak)
         batched = None
         if world == 1 and not args.no_batched:
             batched = batched_measurement(torch, mdx, dev, peak)
@@ -674,7 +826,12 @@ def main():
             served = served_measurement(torch, mdx, dev, peak)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu, why = cpu_baseline(args.ref_sample, m, reps=3)
+            import numpy as np
+            x_host = d_in.cpu().numpy().view(np.uint32)
+            del d_in, d_out
+            torch.cuda.empty_cache()
+            cpu, why = cpu_baseline(x_host, m, reps=2)
+            del x_host
             if cpu is None:
                 cpu = {"value": None, "unavailable": why}
         line = {
@@ -683,6 +840,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": n, "m": m, "discr": f"{discr[0]} {m}",
+                       "seed": W.SEEDS["c2a"],
                        "l2": "inputs and outputs (1 GiB each) larger than L2; no flush",
                        "parallelism": f"independent arrays per rank x{world}" if world > 1
                        else "single GPU"},
@@ -694,6 +852,7 @@ def main():
                             "on the same streams, no partition (CUDA events)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "configs": configs,
             "batched": batched,
             "served": served,
             "sort_baseline": sort_ref,
