@@ -212,13 +212,22 @@ mdx_status mdx_graph_destroy(mdx_graph graph);
  *     its stream.  Calls that may overlap on the GPU race: keep them in one
  *     stream or order them.
  *   - A device-side wait that runs out (a tile copy that never lands within a
- *     second) is not reported by this entry point; use mdx_partition with a
- *     workspace and mdx_workspace_error where that report is needed.
+ *     second) leaves that call's output incomplete and latches a bit in the
+ *     array's error word, which later calls keep; mdx_partition_noalloc_error
+ *     reports it.
  * Allocates nothing: no cudaMalloc, no cudaFree, no allocating library call.
  */
 mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
                                  mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
                                  mdx_stream_t stream);
+
+/*
+ * Device-side errors latched by mdx_partition_noalloc calls on the current
+ * device since the last query (no counterpart in the reference): MDX_OK, or
+ * MDX_ERR_TIMEOUT when a wait ran out.  Reads and clears the built-in array's
+ * error word on `stream` and synchronizes that stream; allocates nothing.
+ */
+mdx_status mdx_partition_noalloc_error(mdx_stream_t stream);
 
 /*
  * Wide elements.  Records of record_bytes (a multiple of 4) whose class comes

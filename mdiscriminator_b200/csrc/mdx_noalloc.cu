@@ -25,9 +25,13 @@
 //
 // Sharing: every call uses the same array, which keeps whatever the last call
 // left in it.  Each call first clears, on its stream, the part that must start
-// at zero (the chunk ticket and the error word).  Calls whose kernels can
-// overlap on the GPU -- different streams without ordering between them --
-// race on the array: issue them in one stream or order them.
+// at zero (the chunk ticket).  Calls whose kernels can overlap on the GPU --
+// different streams without ordering between them -- race on the array: issue
+// them in one stream or order them.
+//
+// Errors: a device-side wait that runs out (a tile copy that never lands
+// within a second) latches a bit in the array's error word, which no call
+// clears; mdx_partition_noalloc_error reads it, clears it and reports it.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -69,41 +73,39 @@ cudaError_t scratch_address(void** out) {
     return cudaSuccess;
 }
 
-struct Occ {
-    int device;
-    const void* fn;
-    int blocks, sms;
-};
-Occ g_occ[128];
-int g_occ_n = 0;
-
+// Resident CTAs per SM and SM count, looked up once per device for each
+// kernel instantiation (K tags the instantiation: one pair of statics each).
+template <class K>
 cudaError_t occupancy_n(const void* fn, size_t smem, int* blocks, int* sms) {
+    static int s_blocks[kMaxDevices];
+    static int s_sms[kMaxDevices];
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(g_mu);
-    for (int i = 0; i < g_occ_n; i++)
-        if (g_occ[i].device == dev && g_occ[i].fn == fn) {
-            *blocks = g_occ[i].blocks;
-            *sms = g_occ[i].sms;
-            return cudaSuccess;
+    if (s_blocks[dev] == 0) {
+        if (smem > 48 * 1024) {
+            err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+            if (err != cudaSuccess) return err;
         }
-    if (smem > 48 * 1024) {
-        err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(smem));
-        if (err != cudaSuccess) return err;
+        int b = 0, s = 0;
+        if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreadsN, smem)) !=
+            cudaSuccess)
+            return err;
+        if ((err = cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+            return err;
+        s_sms[dev] = s;
+        s_blocks[dev] = b < 1 ? 1 : b;
     }
-    int b = 0, s = 0;
-    if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreadsN, smem)) != cudaSuccess)
-        return err;
-    if ((err = cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-        return err;
-    if (b < 1) b = 1;
-    if (g_occ_n < 128) g_occ[g_occ_n++] = Occ{dev, fn, b, s};
-    *blocks = b;
-    *sms = s;
+    *blocks = s_blocks[dev];
+    *sms = s_sms[dev];
     return cudaSuccess;
 }
+
+template <class V, class D, int M>
+struct KernelTag {};
 
 typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
@@ -142,7 +144,7 @@ inline uint32_t bound_of(uint32_t m) {
 }
 
 // Offsets inside the scratch (same roles as the caller workspace of
-// mdx_partition): header {done, error}, class bases, class totals, [M][G]
+// mdx_partition): header {ticket, error}, class bases, class totals, [M][G]
 // chunk counts and prefixes.
 struct Layout {
     size_t class_base, class_tot, chunk_cnt, chunk_pre, total;
@@ -168,7 +170,8 @@ mdx_status run(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint3
     void* scratch = nullptr;
     if (scratch_address(&scratch) != cudaSuccess) return MDX_ERR_CUDA;
     int blocks = 0, sms = 0;
-    if (occupancy_n(reinterpret_cast<const void*>(scatter), SL::kBytes, &blocks, &sms) != cudaSuccess)
+    if (occupancy_n<KernelTag<V, D, M>>(reinterpret_cast<const void*>(scatter), SL::kBytes,
+                                        &blocks, &sms) != cudaSuccess)
         return MDX_ERR_CUDA;
     const uint32_t nt = static_cast<uint32_t>((n + TILE - 1) / TILE);
     uint32_t G = static_cast<uint32_t>(blocks) * static_cast<uint32_t>(sms);
@@ -177,8 +180,9 @@ mdx_status run(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint3
     const Layout L = layout_for(M, G);
     if (L.total > kNoAllocScratchBytes) return MDX_ERR_WORKSPACE;
     unsigned char* ws = static_cast<unsigned char*>(scratch);
-    // the chunk ticket and the error word must start at zero
-    if (cudaMemsetAsync(ws, 0, kHeaderN, st) != cudaSuccess) return MDX_ERR_CUDA;
+    // the chunk ticket must start at zero (the error word keeps its bits
+    // until mdx_partition_noalloc_error reads them)
+    if (cudaMemsetAsync(ws, 0, sizeof(uint32_t), st) != cudaSuccess) return MDX_ERR_CUDA;
     if (d_headflags != nullptr &&
         cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), st) != cudaSuccess)
         return MDX_ERR_CUDA;
@@ -259,4 +263,19 @@ extern "C" mdx_status mdx_partition_noalloc(const void* d_in, void* d_out, uint6
     if (elem == MDX_ELEM_U32)
         return by_discr<uint32_t>(d_in, d_out, n, discr, d_sizes, d_headflags, st);
     return by_discr<uint64_t>(d_in, d_out, n, discr, d_sizes, d_headflags, st);
+}
+
+extern "C" mdx_status mdx_partition_noalloc_error(mdx_stream_t stream) {
+    using namespace mdx::noalloc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    void* scratch = nullptr;
+    if (scratch_address(&scratch) != cudaSuccess) return MDX_ERR_CUDA;
+    uint32_t* word = static_cast<uint32_t*>(scratch) + 1;
+    uint32_t bits = 0;  // pageable: the copy completes before cudaMemcpyAsync returns
+    if (cudaMemcpyAsync(&bits, word, sizeof(bits), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemsetAsync(word, 0, sizeof(uint32_t), st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return MDX_ERR_CUDA;
+    if (bits & mdx::kErrTimeout) return MDX_ERR_TIMEOUT;
+    return bits ? MDX_ERR_INVALID : MDX_OK;
 }
