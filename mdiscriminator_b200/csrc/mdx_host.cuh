@@ -11,6 +11,7 @@
 #include <mutex>
 
 #include "../../include/mdx.h"
+#include "mdx_fused.cuh"
 #include "mdx_plain.cuh"
 #include "mdx_segm.cuh"
 #include "mdx_tile.cuh"
@@ -78,7 +79,8 @@ struct PlainLayout {
 
 inline PlainLayout plain_layout(uint64_t n, mdx_elem e, uint32_t m) {
     const uint32_t M = class_bound(m);
-    const size_t G = max_chunks_of(n, e);
+    // rows of the [class][chunk] tables padded to 4 chunks (16-byte loads)
+    const size_t G = (max_chunks_of(n, e) + 3u) & ~size_t{3};
     PlainLayout L;
     L.class_base = kHeaderBytes;
     L.class_tot = L.class_base + kMaxClasses * 4;
@@ -245,6 +247,10 @@ struct DistOut {
 constexpr size_t kDistSkipOffset = 196;
 static_assert(kDistSkipOffset >= kPlainDoneOffset + 4 && kDistSkipOffset + 4 <= kHeaderBytes,
               "skip word inside the header, clear of the plain ticket");
+// Grid barrier of the one-kernel plain path: arrival counter and generation.
+constexpr size_t kFusedBarOffset = 200;
+static_assert(kFusedBarOffset >= kDistSkipOffset + 4 && kFusedBarOffset + 8 <= kHeaderBytes,
+              "barrier words inside the header");
 
 template <class V, class D, int M>
 mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
@@ -299,6 +305,47 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
                                                          d_headflags);
         if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
         return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+    }
+    if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr) {
+        // one cooperative kernel: count, grid barrier, scatter (mdx_fused.cuh)
+        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
+        CUtensorMap map;
+        if (make_row_map(&map, d_in, n, sizeof(V), SL::kRows)) {
+            auto fused = plain_fused_kernel<V, D, M, kThreads, kStages>;
+            int fb = 0, fs = 0;
+            if (occupancy(reinterpret_cast<const void*>(fused), smem, &fb, &fs) != cudaSuccess)
+                return MDX_ERR_CUDA;
+            if (tun.plain_ctas_per_sm > 0 && static_cast<int>(tun.plain_ctas_per_sm) < fb)
+                fb = static_cast<int>(tun.plain_ctas_per_sm);
+            uint32_t FG = static_cast<uint32_t>(fb) * static_cast<uint32_t>(fs);
+            if (FG > nt) FG = nt;
+            if (FG > kMaxChunks) FG = kMaxChunks;
+            if (d_headflags != nullptr &&
+                cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess)
+                return MDX_ERR_CUDA;
+            FusedArgs fa;
+            fa.p = a;
+            fa.p.num_chunks = FG;
+            fa.p.use_tma = 1;
+            fa.chunk_stride = (FG + 3u) & ~3u;
+            fa.bar_count = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset);
+            fa.bar_gen = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 4);
+            const OutFlat<V> o{static_cast<V*>(d_out),
+                               static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
+                                                     (16u / sizeof(V) - 1u))};
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(FG);
+            cfg.blockDim = dim3(kThreads);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            if (cudaLaunchKernelEx(&cfg, fused, fa, d, map, o) != cudaSuccess) return MDX_ERR_CUDA;
+            return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+        }
     }
     if (step != PlainStep::kScatter) {
         // head flags: all zero but for count_c at offset_c, which the last
