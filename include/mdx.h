@@ -34,7 +34,8 @@ typedef enum {
     MDX_ERR_CUDA = 3,        /* a CUDA runtime call failed (launch, copy, attribute query) */
     MDX_ERR_TIMEOUT = 4,     /* a device-side bounded wait ran out (latched in the workspace) */
     MDX_ERR_UNSUPPORTED = 5, /* valid request this build does not handle */
-    MDX_ERR_SEGMENTS = 6     /* malformed segment description */
+    MDX_ERR_SEGMENTS = 6,    /* malformed segment description */
+    MDX_ERR_CANCELLED = 7    /* a served request withdrawn before launch (mdx_server_cancel) */
 } mdx_status;
 
 /* Element layouts.  U32: one unsigned 32-bit value, class from the value
@@ -315,6 +316,10 @@ mdx_status mdx_ipc_close(void* d_ptr, uint64_t offset);
  * latency from submit to completion.  Long requests in device memory
  * (direct_min_elems) still take their place in the pool but are partitioned
  * in place by the plain kernels, one launch each, without the pool's copies.
+ * Batched (short) requests run on streams of the device's highest priority,
+ * in-place (long) ones on its lowest, so short requests are not parked behind
+ * long ones on the GPU.  A batch's stream is free again as soon as that batch
+ * is done.
  */
 typedef struct mdx_server_st* mdx_server;
 
@@ -343,8 +348,13 @@ mdx_status mdx_server_create(mdx_server* server, const mdx_server_config* config
 /* in: n values; out: n values; sizes: m class sizes.  Returns immediately. */
 mdx_status mdx_server_submit(mdx_server server, const uint32_t* in, uint32_t* out, uint32_t* sizes,
                              uint64_t n, uint32_t m, uint64_t* ticket);
-/* Block until the request is done; its latency in seconds. */
+/* Block until the request is done; its latency in seconds.  MDX_ERR_CANCELLED
+ * for a request withdrawn by mdx_server_cancel (its outputs are untouched). */
 mdx_status mdx_server_wait(mdx_server server, uint64_t ticket, double* latency_s);
+/* Withdraw a request that has not been launched yet (still queued or
+ * admitted): MDX_OK, and its wait returns MDX_ERR_CANCELLED; MDX_ERR_INVALID
+ * when the ticket is unknown or the request is already on the GPU or done. */
+mdx_status mdx_server_cancel(mdx_server server, uint64_t ticket);
 mdx_status mdx_server_get_stats(mdx_server server, mdx_server_stats* stats);
 mdx_status mdx_server_reset_stats(mdx_server server);
 /* Finishes the work already submitted, then frees everything. */
@@ -361,7 +371,8 @@ typedef struct {
     uint32_t plain_ctas_per_sm;  /* plain path: CTAs per SM of the chunk grid (0: as many as fit) */
     uint32_t run_tiles;          /* segmented: tiles per run of a large segment (default 8) */
     uint32_t group_batch;        /* segmented: small-segment groups per work item (default 8, at most 32) */
-    uint32_t lag_slack_pct;      /* accepted and stored (default 50); no kernel reads it any more */
+    uint32_t plain_two_kernel;   /* plain path: 1 = count and scatter as two kernels; 0 (default) =
+                                    one cooperative kernel where the input allows TMA */
 } mdx_tuning;
 
 mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,
@@ -370,6 +381,16 @@ mdx_status mdx_get_tuning(mdx_elem elem, uint32_t m, uint64_t n, mdx_tuning* tun
 
 /* Human-readable text of a status. */
 const char* mdx_strerror(mdx_status s);
+
+/*
+ * Fault injection for tests (no reference counterpart; the reference exits on
+ * any CUDA error, HelpersHost.cu.h:11-19): the `nth` device or page-locked
+ * host allocation that the serving loop's set-up (mdx_server_create) makes
+ * from now on fails as if memory were exhausted; 0 turns it off.  Lets a test
+ * check that every failing allocation is reported (MDX_ERR_CUDA) and that
+ * what was already allocated is freed.  Host-side only: no GPU fault.
+ */
+void mdx_test_inject_alloc_failure(uint32_t nth);
 
 /* Library version string, e.g. "mdx 0.1.0 sm_100a". */
 const char* mdx_version(void);

@@ -56,6 +56,7 @@ inline const char* status_text(mdx_status s) {
         case MDX_ERR_TIMEOUT: return "device-side bounded wait timed out";
         case MDX_ERR_UNSUPPORTED: return "unsupported request";
         case MDX_ERR_SEGMENTS: return "malformed segment description";
+        case MDX_ERR_CANCELLED: return "request cancelled before launch";
     }
     return "unknown status";
 }

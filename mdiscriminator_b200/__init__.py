@@ -39,6 +39,7 @@ MDX_ERR_CUDA = 3
 MDX_ERR_TIMEOUT = 4
 MDX_ERR_UNSUPPORTED = 5
 MDX_ERR_SEGMENTS = 6
+MDX_ERR_CANCELLED = 7
 
 ELEM_U32 = 0
 ELEM_REC8 = 1
@@ -64,7 +65,7 @@ class Column(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("plain_ctas_per_sm", ctypes.c_uint32), ("run_tiles", ctypes.c_uint32),
-                ("group_batch", ctypes.c_uint32), ("lag_slack_pct", ctypes.c_uint32)]
+                ("group_batch", ctypes.c_uint32), ("plain_two_kernel", ctypes.c_uint32)]
 
 
 TUNING_PATH = os.path.join(HERE, "tuning.json")
@@ -96,7 +97,7 @@ def load_tuning(path: str, missing_ok: bool = False) -> int:
         elem = ELEM_REC8 if e["elem"] == "rec8" else ELEM_U32
         lo, hi = e["log2_n"]
         set_tuning(elem, e["m"], lo, hi, **{x: e[x] for x in ("plain_ctas_per_sm", "run_tiles",
-                                                             "group_batch", "lag_slack_pct") if x in e})
+                                                             "group_batch", "plain_two_kernel") if x in e})
         k += 1
     return k
 
@@ -670,6 +671,10 @@ def _bind_server(L):
     L.mdx_server_reset_stats.restype = ctypes.c_int
     L.mdx_server_destroy.argtypes = [vp]
     L.mdx_server_destroy.restype = ctypes.c_int
+    L.mdx_server_cancel.argtypes = [vp, ctypes.c_uint64]
+    L.mdx_server_cancel.restype = ctypes.c_int
+    L.mdx_test_inject_alloc_failure.argtypes = [ctypes.c_uint32]
+    L.mdx_test_inject_alloc_failure.restype = None
     L._server_bound = True
     return L
 
@@ -712,6 +717,12 @@ class Server:
         self._keep.pop(ticket, None)
         _check(st, "mdx_server_wait")
         return lat.value
+
+    def cancel(self, ticket: int) -> bool:
+        """Withdraw a request not yet launched; True if it was withdrawn (its
+        wait() then raises MdxError with MDX_ERR_CANCELLED), False if it is
+        already on the GPU or done."""
+        return self._L.mdx_server_cancel(self._h, ticket) == MDX_OK
 
     def stats(self) -> dict:
         s = ServerStats()

@@ -4,10 +4,11 @@ table mdiscriminator_b200 loads at import (tuning.json).
 Keys: element layout (4-byte values / 8-byte records), class bound (the
 smallest power of two >= m) and a range of ceil(log2 n).  Knobs:
 
-* plain path: CTAs per SM of the chunk grid (`plain_ctas_per_sm`);
+* plain path: CTAs per SM of the chunk grid (`plain_ctas_per_sm`), and one
+  cooperative kernel against count and scatter as two kernels
+  (`plain_two_kernel`);
 * segmented path: tiles per run of a large segment (`run_tiles`) and
-  small-segment groups per work item (`group_batch`).  (`lag_slack_pct` is
-  still accepted in the table but no longer used by the kernels.)
+  small-segment groups per work item (`group_batch`).
 
 The reference picked its block shapes by recompiling with -D macros and
 timing them (cuda_code/run.py:12-96); here the choice is made at run time.
@@ -85,15 +86,17 @@ def main(argv=None):
             for M in bounds:
                 sizes = torch.empty(M, dtype=torch.uint32, device=dev)
                 best = None
-                for k in (2, 3, 4, 0):
-                    mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=k)
+                for k, two in itertools.product((2, 3, 4, 0), (0, 1)):
+                    mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=k, plain_two_kernel=two)
                     ms = timeit(lambda: mdx.partition(d, ("mask", M), out=out, sizes=sizes, ws=ws),
                                 torch)
                     if best is None or ms < best[0]:
-                        best = (ms, k)
+                        best = (ms, k, two)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "plain",
-                                "plain_ctas_per_sm": best[1], "ms": best[0]})
-                mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=best[1])
+                                "plain_ctas_per_sm": best[1], "plain_two_kernel": best[2],
+                                "ms": best[0]})
+                mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=best[1],
+                               plain_two_kernel=best[2])
             del d, out, ws
         seg_bounds = [2, 4, 8, 16]
         for n_target, (lo, hi) in buckets:
@@ -104,27 +107,28 @@ def main(argv=None):
             out = torch.empty_like(d)
             do = torch.from_numpy(offs).to(dev)
             ws = mdx.new_workspace(mdx.segmented_workspace_size(n, S, elem, 16), dev)
-            cands = list(itertools.product((2, 4, 8, 16), (2, 4, 8, 16), (50,)))
+            cands = list(itertools.product((2, 4, 8, 16), (2, 4, 8, 16)))
             if args.quick:
-                cands = list(itertools.product((4, 8, 16), (8,), (50,)))
+                cands = list(itertools.product((4, 8, 16), (8,)))
             for M in seg_bounds:
                 ss = torch.empty((S, M), dtype=torch.uint32, device=dev)
-                plain_k = next(e["plain_ctas_per_sm"] for e in entries
-                               if e["elem"] == ename and e["m"] == M and e["path"] == "plain"
-                               and e["log2_n"] == [lo, hi])
+                pe = next(e for e in entries
+                          if e["elem"] == ename and e["m"] == M and e["path"] == "plain"
+                          and e["log2_n"] == [lo, hi])
+                plain_k, plain_two = pe["plain_ctas_per_sm"], pe["plain_two_kernel"]
                 best = None
-                for rt, gb, lag in cands:
-                    mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k, run_tiles=rt,
-                                   group_batch=gb, lag_slack_pct=lag)
+                for rt, gb in cands:
+                    mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
+                                   plain_two_kernel=plain_two, run_tiles=rt, group_batch=gb)
                     ms = timeit(lambda: mdx.partition_segmented(d, do, ("mask", M), out=out,
                                                                 seg_sizes=ss, ws=ws), torch, reps=5)
                     if best is None or ms < best[0]:
-                        best = (ms, rt, gb, lag)
+                        best = (ms, rt, gb)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "segmented",
-                                "plain_ctas_per_sm": plain_k, "run_tiles": best[1],
-                                "group_batch": best[2], "lag_slack_pct": best[3], "ms": best[0]})
-                mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k, run_tiles=best[1],
-                               group_batch=best[2], lag_slack_pct=best[3])
+                                "plain_ctas_per_sm": plain_k, "plain_two_kernel": plain_two,
+                                "run_tiles": best[1], "group_batch": best[2], "ms": best[0]})
+                mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
+                               plain_two_kernel=plain_two, run_tiles=best[1], group_batch=best[2])
             del d, out, ws
     # one entry per key: the segmented entry (it carries the plain knob too)
     merged = {}

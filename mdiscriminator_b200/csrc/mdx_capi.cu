@@ -422,7 +422,7 @@ mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_
     if (check_elem(elem) != MDX_OK || t == nullptr || m < 1 || m > MDX_MAX_CLASSES ||
         log2_n_lo > log2_n_hi || log2_n_hi > 33)
         return MDX_ERR_INVALID;
-    if (t->run_tiles > 64 || t->group_batch > 1024 || t->lag_slack_pct > 400) return MDX_ERR_INVALID;
+    if (t->run_tiles > 64 || t->group_batch > 1024 || t->plain_two_kernel > 1) return MDX_ERR_INVALID;
     TuningTable& tt = tuning_table();
     std::lock_guard<std::mutex> lk(tt.mu);
     for (uint32_t b = log2_n_lo; b <= log2_n_hi; b++) {
@@ -430,7 +430,7 @@ mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_
         x.plain_ctas_per_sm = t->plain_ctas_per_sm;
         x.run_tiles = t->run_tiles ? t->run_tiles : kRunTiles;
         x.group_batch = t->group_batch ? t->group_batch : kGroupBatch;
-        x.lag_slack_pct = t->lag_slack_pct ? t->lag_slack_pct : kLagSlackPct;
+        x.plain_two_kernel = t->plain_two_kernel;
     }
     return MDX_OK;
 }
@@ -442,7 +442,7 @@ mdx_status mdx_get_tuning(mdx_elem elem, uint32_t m, uint64_t n, mdx_tuning* t) 
     t->plain_ctas_per_sm = x.plain_ctas_per_sm;
     t->run_tiles = x.run_tiles;
     t->group_batch = x.group_batch;
-    t->lag_slack_pct = x.lag_slack_pct;
+    t->plain_two_kernel = x.plain_two_kernel;
     return MDX_OK;
 }
 
@@ -455,6 +455,7 @@ const char* mdx_strerror(mdx_status s) {
         case MDX_ERR_TIMEOUT: return "device-side bounded wait timed out";
         case MDX_ERR_UNSUPPORTED: return "unsupported request";
         case MDX_ERR_SEGMENTS: return "malformed segment description";
+        case MDX_ERR_CANCELLED: return "request cancelled before launch";
     }
     return "unknown status";
 }

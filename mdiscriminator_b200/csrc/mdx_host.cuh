@@ -205,7 +205,7 @@ struct Tuning {
     uint32_t plain_ctas_per_sm = 0;  // 0: as many as fit
     uint32_t run_tiles = kRunTiles;
     uint32_t group_batch = kGroupBatch;
-    uint32_t lag_slack_pct = kLagSlackPct;
+    uint32_t plain_two_kernel = 0;  // 1: count and scatter as two kernels
 };
 struct TuningTable {
     std::mutex mu;
@@ -306,7 +306,7 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
         return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     }
-    if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr) {
+    if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr && tun.plain_two_kernel == 0) {
         // one cooperative kernel: count, grid barrier, scatter (mdx_fused.cuh)
         using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
         CUtensorMap map;

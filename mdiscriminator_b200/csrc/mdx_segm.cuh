@@ -56,7 +56,6 @@ namespace mdx {
 constexpr int kRunTiles = 8;     // tiles per run of a large segment
 constexpr int kGroupBatch = 8;   // small-segment groups per ticket of seg_main
 constexpr int kMaxGroupBatch = 32;
-constexpr int kLagSlackPct = 50; // accepted in the tuning table, no longer used
 
 // look-back status word of the head-flag converter: [63:34] epoch (30 bits),
 // [33:32] state, [31:0] count

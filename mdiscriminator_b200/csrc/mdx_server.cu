@@ -26,12 +26,21 @@
 //    requests in stream order on each), so
 //    the long requests that carry most elements skip the pool's two copies
 //    and do not cut the runs of short requests that share a batch.
-//  * Completion: ring space is released in admission order when a batch
-//    finishes; waiters are woken; the latency of every request (submit to
-//    completion stamp) goes into the p50 / p99 statistics.
+//  * Priorities: the batch streams (short requests) are created with the
+//    device's highest stream priority and the in-place lanes with its lowest,
+//    so the GPU schedules the blocks of a short request's kernels ahead of
+//    the queued blocks of long ones instead of parking them behind.
+//  * Completion: a batch slot is free again as soon as its own batch is
+//    done; ring space is released in admission order (every allocation
+//    carries a done mark, the ring's tail advances over finished ones);
+//    waiters are woken; the latency of every request (submit to completion
+//    stamp) goes into the p50 / p99 statistics.
+//  * Cancellation: a request that has not been launched yet can be
+//    withdrawn (mdx_server_cancel); its wait then returns MDX_ERR_CANCELLED.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -123,6 +132,28 @@ T* device_view(T* p) {
     return static_cast<T*>(attr.devicePointer);
 }
 
+// Test fault injection (mdx_test_inject_alloc_failure): counts down the
+// set-up's allocations; the one that brings the count to zero fails.
+std::atomic<uint32_t> g_fail_countdown{0};
+inline bool injected_failure() {
+    uint32_t c = g_fail_countdown.load();
+    while (c > 0)
+        if (g_fail_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+    return false;
+}
+template <class T>
+cudaError_t dev_alloc(T** p, size_t bytes) {
+    *p = nullptr;
+    if (injected_failure()) return cudaErrorMemoryAllocation;
+    return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+template <class T>
+cudaError_t pinned_alloc(T** p, size_t bytes) {
+    *p = nullptr;
+    if (injected_failure()) return cudaErrorMemoryAllocation;
+    return cudaMallocHost(reinterpret_cast<void**>(p), bytes);
+}
+
 using Clock = std::chrono::steady_clock;
 inline double now_s() {
     return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
@@ -138,7 +169,17 @@ struct Req {
     uint64_t off = 0;  // ring slot
     double t_submit = 0, t_launch = 0, t_done = 0;
     bool done = false;
+    bool launched = false;
     bool direct = false;  // partitioned in place (long, device-resident): no ring copies
+    mdx_status status = MDX_OK;  // MDX_ERR_CANCELLED when withdrawn before launch
+    struct LiveEntry* ring = nullptr;  // its ring allocation (ring requests)
+};
+
+// One admitted ring allocation; `done` once its request finished or was
+// cancelled.  The ring's tail advances over done entries in admission order.
+struct LiveEntry {
+    uint64_t off, n;
+    bool done;
 };
 
 struct Batch;
@@ -204,7 +245,7 @@ struct Server {
     uint32_t* d_out = nullptr;
     uint64_t cap = 0;        // elements per ring
     uint64_t head = 0;       // next allocation
-    std::deque<std::pair<uint64_t, uint64_t>> live;  // admitted allocations (off, n), in order
+    std::deque<LiveEntry> live;  // admitted allocations, in order (references stay valid)
     std::vector<Slot> slots;
 
     std::mutex mu;
@@ -215,7 +256,7 @@ struct Server {
     std::vector<Lane> lanes;
     std::vector<cudaEvent_t> free_events;
     std::unordered_map<uint64_t, Req*> reqs;  // every request not yet collected
-    std::deque<Batch*> inflight;  // launch order
+    uint32_t inflight_batches = 0;
     uint64_t next_id = 1;
     bool stop = false;
     std::thread sched;
@@ -229,25 +270,31 @@ struct Server {
     // ring: [off, off + n) for a new request, or false if it does not fit now.
     // Live allocations are consecutive in admission order; when the head wraps
     // to 0 the unused end [head, cap) is skipped until the tail passes it.
-    bool ring_alloc(uint64_t n, uint64_t* off) {
-        if (n == 0 || n > cap) return false;
+    LiveEntry* ring_alloc(uint64_t n) {
+        if (n == 0 || n > cap) return nullptr;
+        uint64_t o = 0;
+        uint64_t* off = &o;
         if (live.empty()) {
             head = 0;
             *off = 0;
         } else {
-            const uint64_t tail = live.front().first;
+            const uint64_t tail = live.front().off;
             if (head > tail) {  // not wrapped: free [head, cap) and [0, tail)
                 if (head + n <= cap) *off = head;
                 else if (n <= tail) *off = 0;
-                else return false;
+                else return nullptr;
             } else {  // wrapped: free [head, tail)
                 if (head + n <= tail) *off = head;
-                else return false;
+                else return nullptr;
             }
         }
         head = *off + n;
-        live.emplace_back(*off, n);
-        return true;
+        live.push_back(LiveEntry{*off, n, false});
+        return &live.back();
+    }
+    // Advance the ring's tail over finished allocations.
+    void ring_release() {
+        while (!live.empty() && live.front().done) live.pop_front();
     }
 };
 
@@ -295,9 +342,10 @@ void admit(Server* s) {
         if (r->direct) {
             s->admitted_direct.push_back(r);
         } else {
-            uint64_t off = 0;
-            if (!s->ring_alloc(r->n, &off)) break;
-            r->off = off;
+            LiveEntry* e = s->ring_alloc(r->n);
+            if (e == nullptr) break;
+            r->ring = e;
+            r->off = e->off;
             s->admitted.push_back(r);
         }
         s->waiting.pop_front();
@@ -315,18 +363,18 @@ void complete(Server* s, Req* r, double t_done) {  // caller holds the lock
     s->st_t_last = r->t_done;
 }
 
-// Retire finished batches in launch order.  Caller holds the lock.
-void retire(Server* s) {
-    while (!s->inflight.empty() && s->inflight.front()->done) {
-        Batch* b = s->inflight.front();
-        s->inflight.pop_front();
-        for (uint64_t id : b->ids) {
-            s->live.pop_front();
-            complete(s, s->reqs[id], b->t_done);
-        }
-        s->slots[b->slot].busy = false;
-        delete b;
+// A batch finished: complete its requests, free its slot at once and
+// release ring space in admission order.  Caller holds the lock.
+void finish_batch(Server* s, Batch* b, double t_done) {
+    for (uint64_t id : b->ids) {
+        Req* r = s->reqs[id];
+        complete(s, r, t_done);
+        if (r->ring != nullptr) r->ring->done = true;
     }
+    s->slots[b->slot].busy = false;
+    s->inflight_batches--;
+    delete b;
+    s->ring_release();
     s->cv_done.notify_all();
 }
 
@@ -369,7 +417,6 @@ void scheduler(Server* s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
-        retire(s);
         admit(s);
         // long requests in device memory: the plain kernels straight on their
         // buffers, queued on the least loaded lane up to its depth
@@ -381,6 +428,7 @@ void scheduler(Server* s) {
             Req* r = s->admitted_direct.front();
             s->admitted_direct.pop_front();
             l->inflight++;
+            r->launched = true;
             r->t_launch = now_s();
             s->st_direct++;
             lk.unlock();
@@ -391,6 +439,7 @@ void scheduler(Server* s) {
             auto done = [s, l, r](double t) {
                 complete(s, r, t);
                 l->inflight--;
+                s->cv_done.notify_all();
             };
             if (st != MDX_OK || !track(s, l->waiter, l->stream, done)) {
                 // nothing will complete this request: finish it now
@@ -407,7 +456,7 @@ void scheduler(Server* s) {
             lane_free = lane_free || l.inflight < kLaneDepth;
         }
         if (s->stop && s->admitted.empty() && s->admitted_direct.empty() && s->waiting.empty() &&
-            s->inflight.empty() && !lanes_busy)
+            s->inflight_batches == 0 && !lanes_busy)
             break;
         const bool can_batch = free_slot >= 0 && !s->admitted.empty();
         const bool can_direct = lane_free && !s->admitted_direct.empty();
@@ -433,16 +482,14 @@ void scheduler(Server* s) {
         for (Req* r : batch) {
             b->ids.push_back(r->id);
             r->t_launch = t_launch;
+            r->launched = true;
         }
-        s->inflight.push_back(b);
+        s->inflight_batches++;
         s->st_batches++;
         lk.unlock();
         mdx_status st = launch_batch(s, sl, batch);
         lk.lock();
-        auto done = [b](double t) {
-            b->done = true;
-            b->t_done = t;
-        };
+        auto done = [s, b](double t) { finish_batch(s, b, t); };
         if (st != MDX_OK || !track(s, sl.waiter, sl.stream, done)) {
             // nothing will complete this batch: finish it now
             if (s->sticky == MDX_OK) s->sticky = st != MDX_OK ? st : MDX_ERR_CUDA;
@@ -479,30 +526,32 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
     if (s.cap > MDX_MAX_ELEMS) s.cap = MDX_MAX_ELEMS;
     if (cfg.max_batch_elems == 0 || cfg.max_batch_elems > s.cap) s.cfg.max_batch_elems = s.cap;
     bool ok = cudaGetDevice(&s.device) == cudaSuccess &&
-              cudaMalloc(&s.d_in, s.cap * 4) == cudaSuccess &&
-              cudaMalloc(&s.d_out, s.cap * 4) == cudaSuccess;
+              dev_alloc(&s.d_in, s.cap * 4) == cudaSuccess &&
+              dev_alloc(&s.d_out, s.cap * 4) == cudaSuccess;
     const uint32_t B = s.cfg.max_batch_requests;
+    int prio_low = 0, prio_high = 0;  // numerically lower = higher priority
+    if (ok) ok = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) == cudaSuccess;
     s.slots = std::vector<Slot>(cfg.num_streams);  // sized once: completions hold pointers
     for (auto& sl : s.slots) {
         if (!ok) break;
         sl.ws_bytes = mdx_segmented_workspace_size(s.cfg.max_batch_elems, B, MDX_ELEM_U32, cfg.m_max);
-        ok = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) == cudaSuccess &&
-             cudaMalloc(&sl.ws, sl.ws_bytes) == cudaSuccess &&
+        ok = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_high) == cudaSuccess &&
+             dev_alloc(&sl.ws, sl.ws_bytes) == cudaSuccess &&
              mdx_workspace_init(sl.ws, sl.ws_bytes, reinterpret_cast<mdx_stream_t>(sl.stream)) == MDX_OK &&
-             cudaMalloc(&sl.d_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
-             cudaMalloc(&sl.d_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
-             cudaMalloc(&sl.d_seg_sizes, sizeof(uint32_t) * B * cfg.m_max) == cudaSuccess &&
-             cudaMalloc(&sl.d_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess &&
-             cudaMallocHost(&sl.h_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
-             cudaMallocHost(&sl.h_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
-             cudaMallocHost(&sl.h_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess;
+             dev_alloc(&sl.d_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
+             dev_alloc(&sl.d_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
+             dev_alloc(&sl.d_seg_sizes, sizeof(uint32_t) * B * cfg.m_max) == cudaSuccess &&
+             dev_alloc(&sl.d_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess &&
+             pinned_alloc(&sl.h_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
+             pinned_alloc(&sl.h_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
+             pinned_alloc(&sl.h_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess;
     }
     s.lanes = std::vector<Lane>(kLanes);  // sized once: completions hold Lane pointers
     for (auto& l : s.lanes) {
         if (!ok) break;
         l.ws_bytes = mdx_workspace_size(s.cfg.max_batch_elems, MDX_ELEM_U32, cfg.m_max);
-        ok = cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) == cudaSuccess &&
-             cudaMalloc(&l.ws, l.ws_bytes) == cudaSuccess &&
+        ok = cudaStreamCreateWithPriority(&l.stream, cudaStreamNonBlocking, prio_low) == cudaSuccess &&
+             dev_alloc(&l.ws, l.ws_bytes) == cudaSuccess &&
              mdx_workspace_init(l.ws, l.ws_bytes, reinterpret_cast<mdx_stream_t>(l.stream)) == MDX_OK;
     }
     if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
@@ -516,6 +565,8 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
     *out = h;
     return MDX_OK;
 }
+
+void mdx_test_inject_alloc_failure(uint32_t nth) { g_fail_countdown.store(nth); }
 
 mdx_status mdx_server_submit(mdx_server h, const uint32_t* in, uint32_t* out, uint32_t* sizes,
                              uint64_t n, uint32_t m, uint64_t* ticket) {
@@ -563,9 +614,40 @@ mdx_status mdx_server_wait(mdx_server h, uint64_t ticket, double* latency_s) {
     Req* r = it->second;
     s.cv_done.wait(lk, [&] { return r->done; });
     if (latency_s) *latency_s = r->t_done - r->t_submit;
+    const mdx_status st = r->status != MDX_OK ? r->status : s.sticky;
     s.reqs.erase(it);
     delete r;
-    return s.sticky;
+    return st;
+}
+
+mdx_status mdx_server_cancel(mdx_server h, uint64_t ticket) {
+    if (h == nullptr) return MDX_ERR_INVALID;
+    Server& s = h->s;
+    {
+        std::lock_guard<std::mutex> lk(s.mu);
+        auto it = s.reqs.find(ticket);
+        if (it == s.reqs.end()) return MDX_ERR_INVALID;
+        Req* r = it->second;
+        if (r->launched || r->done) return MDX_ERR_INVALID;  // too late
+        auto drop = [r](std::deque<Req*>& q) {
+            auto qi = std::find(q.begin(), q.end(), r);
+            if (qi == q.end()) return false;
+            q.erase(qi);
+            return true;
+        };
+        if (!drop(s.waiting) && !drop(s.admitted) && !drop(s.admitted_direct))
+            return MDX_ERR_INVALID;
+        if (r->ring != nullptr) {
+            r->ring->done = true;  // its ring slot is released in admission order
+            s.ring_release();
+        }
+        r->status = MDX_ERR_CANCELLED;
+        r->done = true;
+        r->t_done = now_s();
+    }
+    s.cv_done.notify_all();
+    s.cv_sched.notify_all();
+    return MDX_OK;
 }
 
 mdx_status mdx_server_get_stats(mdx_server h, mdx_server_stats* out) {
@@ -577,7 +659,7 @@ mdx_status mdx_server_get_stats(mdx_server h, mdx_server_stats* out) {
     out->batches = s.st_batches;
     out->elements = s.st_elements;
     out->waiting = s.waiting.size();
-    out->inflight_batches = s.inflight.size();
+    out->inflight_batches = s.inflight_batches;
     auto pct = [](std::vector<double> v, double q) {
         if (v.empty()) return 0.0;
         std::sort(v.begin(), v.end());

@@ -46,7 +46,7 @@ def test_library_exports_every_declared_symbol(L):
 
 def test_version_and_strerror(L):
     assert "sm_100a" in mdx.version()
-    for s in range(7):
+    for s in range(8):
         assert mdx.strerror(s)
     assert mdx.strerror(mdx.MDX_ERR_TIMEOUT).startswith("device-side")
 

@@ -143,3 +143,70 @@ def test_long_device_requests_are_partitioned_in_place(cuda_ready):
                     assert np.array_equal(results[direct_min][k][1], es), f"request {k}"
     for (a_o, a_s), (b_o, b_s) in zip(results[0], results[2**64 - 1]):
         assert np.array_equal(a_o, b_o) and np.array_equal(a_s, b_s)
+
+
+def test_server_set_up_reports_each_failed_allocation_and_frees_the_rest(cuda_ready):
+    """Host-side fault injection: the k-th allocation of mdx_server_create
+    fails (as if memory were exhausted), for every k until creation needs no
+    more.  Each failure is reported as MDX_ERR_CUDA, no server is returned and
+    the device memory already allocated is freed again."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    L = mdx._bind_server(mdx.lib())
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    failures = 0
+    try:
+        for k in range(1, 200):
+            L.mdx_test_inject_alloc_failure(k)
+            try:
+                srv = mdx.Server(budget_bytes=64 << 20, num_streams=2)
+            except mdx.MdxError as e:
+                assert e.status == mdx.MDX_ERR_CUDA
+                failures += 1
+                continue
+            srv.close()  # k is past the last allocation: created normally
+            break
+    finally:
+        L.mdx_test_inject_alloc_failure(0)
+    assert failures >= 10  # rings, per-stream workspaces and tables, lanes
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert abs(free1 - free0) < (2 << 20), f"{free0 - free1} bytes not freed"
+
+
+def test_cancel_before_launch(cuda_ready):
+    """Requests queued behind a long batch are withdrawn before launch: their
+    wait reports MDX_ERR_CANCELLED and their outputs stay untouched; the
+    others complete and equal the oracle."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    with mdx.Server(budget_bytes=1 << 30, num_streams=1, direct_min_elems=1 << 40) as srv:
+        xa, da, oa = _request(torch, 1 << 26, 5)
+        sa = _sizes(torch, 4)
+        ta = srv.submit(da, oa, sa, 4)  # keeps the only batch stream busy
+        reqs = []
+        for i in range(24):
+            x, d, o = _request(torch, 5000 + 17 * i, 300 + i)
+            o.view(torch.int32).fill_(-559038737)  # 0xDEADBEEF
+            s = _sizes(torch, 8)
+            t = srv.submit(d, o, s, 8)
+            cancelled = srv.cancel(t) if i % 2 == 0 else False
+            reqs.append((x, o, s, t, cancelled))
+        srv.wait(ta)
+        n_cancelled = 0
+        for x, o, s, t, cancelled in reqs:
+            if cancelled:
+                n_cancelled += 1
+                with pytest.raises(mdx.MdxError) as ei:
+                    srv.wait(t)
+                assert ei.value.status == mdx.MDX_ERR_CANCELLED
+                assert bool((o.cpu().numpy() == 0xDEADBEEF).all())
+                assert not srv.cancel(t)  # unknown once collected
+            else:
+                srv.wait(t)
+                eo, es = oracle.partition(x, 8)
+                assert np.array_equal(o.cpu().numpy(), eo) and np.array_equal(s.cpu().numpy(), es)
+        assert n_cancelled >= 1
+        eo, es = oracle.partition(xa, 4)
+        assert np.array_equal(oa.cpu().numpy(), eo)

@@ -15,10 +15,10 @@ def test_tuning_table_roundtrip_and_validation():
     mdx_build.build()
     other_bucket = mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20)
     other_layout = mdx.get_tuning(mdx.ELEM_REC8, 7, 3000)
-    mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12, run_tiles=4, group_batch=16, lag_slack_pct=25,
+    mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12, run_tiles=4, group_batch=16, plain_two_kernel=1,
                    plain_ctas_per_sm=2)
     t = mdx.get_tuning(mdx.ELEM_U32, 7, 3000)  # m=7 -> class bound 8, log2 3000 -> 12
-    assert t == {"plain_ctas_per_sm": 2, "run_tiles": 4, "group_batch": 16, "lag_slack_pct": 25}
+    assert t == {"plain_ctas_per_sm": 2, "run_tiles": 4, "group_batch": 16, "plain_two_kernel": 1}
     assert mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20) == other_bucket   # other bucket untouched
     assert mdx.get_tuning(mdx.ELEM_REC8, 7, 3000) == other_layout     # other element layout
     with pytest.raises(mdx.MdxError):
@@ -27,6 +27,8 @@ def test_tuning_table_roundtrip_and_validation():
         mdx.set_tuning(mdx.ELEM_U32, 4, 0, 40, run_tiles=8)  # past the last bucket
     with pytest.raises(mdx.MdxError):
         mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, run_tiles=1000)
+    with pytest.raises(mdx.MdxError):
+        mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, plain_two_kernel=2)
     mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12)  # back to the defaults
     mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
 
@@ -43,8 +45,8 @@ def test_committed_table_is_well_formed():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("knobs", [dict(run_tiles=1, group_batch=1, lag_slack_pct=1, plain_ctas_per_sm=1),
-                                   dict(run_tiles=16, group_batch=32, lag_slack_pct=200,
+@pytest.mark.parametrize("knobs", [dict(run_tiles=1, group_batch=1, plain_two_kernel=1, plain_ctas_per_sm=1),
+                                   dict(run_tiles=16, group_batch=32, plain_two_kernel=0,
                                         plain_ctas_per_sm=2)])
 def test_results_do_not_depend_on_knobs(cuda_ready, knobs):
     torch = cuda_ready
