@@ -392,6 +392,17 @@ const char* mdx_strerror(mdx_status s);
  */
 void mdx_test_inject_alloc_failure(uint32_t nth);
 
+/*
+ * Makes a device-side wait run out, for tests (no reference counterpart):
+ * the one-kernel plain partition's grid barrier expects `extra_arrivals` more
+ * CTAs than its grid has, so no arrival completes it, and waits at most
+ * `wait_limit_ns` (0: the normal 1 s).  The call then latches
+ * MDX_ERR_TIMEOUT in its workspace (mdx_workspace_error) and writes no
+ * output; nothing faults or hangs.  After a timeout re-initialise the
+ * workspace (mdx_workspace_init).  extra_arrivals = 0 restores normal calls.
+ */
+void mdx_test_set_barrier_shortfall(uint32_t extra_arrivals, uint64_t wait_limit_ns);
+
 /* Library version string, e.g. "mdx 0.1.0 sm_100a". */
 const char* mdx_version(void);
 

@@ -45,10 +45,10 @@ mdx_status mdx_workspace_error(void* d_ws, mdx_stream_t stream) {
     return MDX_OK;
 }
 
-mdx_status mdx_partition_timed(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
-                               mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
-                               void* d_ws, size_t ws_bytes, mdx_stream_t stream,
-                               void* ev_count_done) {
+static mdx_status partition_impl(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                 mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                                 void* d_ws, size_t ws_bytes, mdx_stream_t stream,
+                                 void* ev_count_done, bool allow_fused) {
     cudaEvent_t ev = reinterpret_cast<cudaEvent_t>(ev_count_done);
     mdx_status s = check_elem(elem);
     if (s != MDX_OK) return s;
@@ -72,11 +72,23 @@ mdx_status mdx_partition_timed(const void* d_in, void* d_out, uint64_t n, mdx_el
     if (reinterpret_cast<uintptr_t>(d_ws) % kAlign) return MDX_ERR_WORKSPACE;
     unsigned char* ws = static_cast<unsigned char*>(d_ws);
     if (elem == MDX_ELEM_U32)
-        return dispatch_plain<uint32_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
+        return dispatch_plain<uint32_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev,
+                                        PlainStep::kBoth, nullptr, allow_fused);
     if (elem == MDX_ELEM_REC16)
-        return dispatch_plain<Rec16>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
-    return dispatch_plain<uint64_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev);
+        return dispatch_plain<Rec16>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev,
+                                     PlainStep::kBoth, nullptr, allow_fused);
+    return dispatch_plain<uint64_t>(d_in, d_out, n, discr, d_sizes, d_headflags, ws, L, st, ev,
+                                    PlainStep::kBoth, nullptr, allow_fused);
 }
+
+mdx_status mdx_partition_timed(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                               mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                               void* d_ws, size_t ws_bytes, mdx_stream_t stream,
+                               void* ev_count_done) {
+    return partition_impl(d_in, d_out, n, elem, discr, d_sizes, d_headflags, d_ws, ws_bytes, stream,
+                          ev_count_done, true);
+}
+
 
 mdx_status mdx_partition(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
                          mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags, void* d_ws,
@@ -342,6 +354,20 @@ mdx_status mdx_mdiscr_segm(uint32_t n, const void* d_in, const int32_t* d_segmen
 
 }  // extern "C"
 
+namespace mdx {
+// The plain partition without the one-kernel cooperative path, for callers
+// whose calls run side by side with other kernels (the serving loop's
+// in-place lanes): a cooperative grid needs the whole GPU at once, so it would
+// wait for every concurrent kernel to drain instead of interleaving with them.
+mdx_status partition_two_kernel(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                                void* d_ws, size_t ws_bytes, mdx_stream_t stream) {
+    return partition_impl(d_in, d_out, n, elem, discr, d_sizes, d_headflags, d_ws, ws_bytes, stream,
+                          nullptr, false);
+}
+}  // namespace mdx
+
+
 struct mdx_graph_st {
     cudaGraph_t graph;
     cudaGraphExec_t exec;
@@ -444,6 +470,11 @@ mdx_status mdx_get_tuning(mdx_elem elem, uint32_t m, uint64_t n, mdx_tuning* t) 
     t->group_batch = x.group_batch;
     t->plain_two_kernel = x.plain_two_kernel;
     return MDX_OK;
+}
+
+void mdx_test_set_barrier_shortfall(uint32_t extra_arrivals, uint64_t wait_limit_ns) {
+    g_test_bar_extra.store(extra_arrivals);
+    g_test_wait_ns.store(wait_limit_ns);
 }
 
 const char* mdx_strerror(mdx_status s) {

@@ -23,7 +23,8 @@
 //
 // The grid must be co-resident (every CTA waits for every other at the
 // barrier): the host launches it cooperatively with at most the occupancy
-// bound of CTAs.  Semantics and outputs are those of the two-kernel path
+// bound of CTAs.  A barrier wait that runs out latches kErrTimeout and leaves
+// the arrival counter behind: re-initialise the workspace after a timeout.  Semantics and outputs are those of the two-kernel path
 // (SeqMdiscr.h:10-57): stable order, class sizes, head flags.
 #pragma once
 
@@ -40,6 +41,8 @@ struct FusedArgs {
     uint32_t chunk_stride;  // row stride of chunk_cnt (a multiple of 4 >= num_chunks)
     uint32_t* bar_count;    // grid barrier: arrivals (low 16 bits) and failures (high 16 bits)
     uint32_t* bar_gen;      // grid barrier: generation (+2 per call), bit 0 = the call aborted
+    uint32_t bar_extra;     // arrivals expected beyond the grid (0; tests set 1 to make the wait run out)
+    uint64_t wait_ns;       // limit of the barrier wait
 };
 
 // Bounded grid barrier (thread 0 of each CTA).  Returns true when the call
@@ -50,7 +53,7 @@ __device__ __forceinline__ bool fused_grid_barrier(const FusedArgs& a, bool fail
                                                    // arrival moves it on only after this
     __threadfence();                               // this CTA's chunk counts, then the arrival
     const uint32_t old = atomicAdd(a.bar_count, failed ? 0x10001u : 1u);
-    if ((old & 0xffffu) == G - 1u) {
+    if ((old & 0xffffu) == G - 1u + a.bar_extra) {
         const bool any_fail = failed || (old >> 16) != 0u;
         atomicExch(a.bar_count, 0u);
         __threadfence();
@@ -63,7 +66,7 @@ __device__ __forceinline__ bool fused_grid_barrier(const FusedArgs& a, bool fail
         for (;;) {
             w = ld_acquire_u32(a.bar_gen);
             if ((w & ~1u) != (g & ~1u)) break;
-            if (globaltimer_ns() - t0 > kWaitLimitNs) {
+            if (globaltimer_ns() - t0 > a.wait_ns) {
                 atomicOr(a.p.error, kErrTimeout);
                 return false;
             }

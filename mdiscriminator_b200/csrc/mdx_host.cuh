@@ -6,6 +6,7 @@
 #include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched from the runtime)
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -247,6 +248,10 @@ struct DistOut {
 constexpr size_t kDistSkipOffset = 196;
 static_assert(kDistSkipOffset >= kPlainDoneOffset + 4 && kDistSkipOffset + 4 <= kHeaderBytes,
               "skip word inside the header, clear of the plain ticket");
+// Test setting of the one-kernel plain path (mdx_test_set_barrier_shortfall):
+// arrivals its grid barrier expects beyond the grid, and the wait's limit.
+inline std::atomic<uint32_t> g_test_bar_extra{0};
+inline std::atomic<uint64_t> g_test_wait_ns{0};
 // Grid barrier of the one-kernel plain path: arrival counter and generation.
 constexpr size_t kFusedBarOffset = 200;
 static_assert(kFusedBarOffset >= kDistSkipOffset + 4 && kFusedBarOffset + 8 <= kHeaderBytes,
@@ -256,7 +261,7 @@ template <class V, class D, int M>
 mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
                      uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
                      cudaStream_t stream, cudaEvent_t ev_mid, PlainStep step = PlainStep::kBoth,
-                     const DistOut* dist = nullptr) {
+                     const DistOut* dist = nullptr, bool allow_fused = true) {
     constexpr int ITEMS = ElemCfg<V>::kItems;
     constexpr int TILE = kThreads * ITEMS;
     auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
@@ -306,7 +311,8 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
         return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     }
-    if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr && tun.plain_two_kernel == 0) {
+    if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr && allow_fused &&
+        tun.plain_two_kernel == 0) {
         // one cooperative kernel: count, grid barrier, scatter (mdx_fused.cuh)
         using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
         CUtensorMap map;
@@ -330,6 +336,9 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
             fa.chunk_stride = (FG + 3u) & ~3u;
             fa.bar_count = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset);
             fa.bar_gen = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 4);
+            fa.bar_extra = g_test_bar_extra.load();
+            const uint64_t lim = g_test_wait_ns.load();
+            fa.wait_ns = lim != 0 ? lim : kWaitLimitNs;
             const OutFlat<V> o{static_cast<V*>(d_out),
                                static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
                                                      (16u / sizeof(V) - 1u))};
@@ -398,14 +407,15 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
 template <class V, class D>
 mdx_status dispatch_plain_m(const void* in, void* out, uint64_t n, D d, uint32_t m, uint32_t* sz,
                             uint32_t* hf, unsigned char* ws, const PlainLayout& L,
-                            cudaStream_t st, cudaEvent_t ev, PlainStep step, const DistOut* dist) {
+                            cudaStream_t st, cudaEvent_t ev, PlainStep step, const DistOut* dist,
+                            bool fu) {
     switch (class_bound(m)) {
-        case 2: return run_plain<V, D, 2>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
-        case 4: return run_plain<V, D, 4>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
-        case 8: return run_plain<V, D, 8>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
-        case 16: return run_plain<V, D, 16>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
-        case 32: return run_plain<V, D, 32>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
-        case 64: return run_plain<V, D, 64>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist);
+        case 2: return run_plain<V, D, 2>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist, fu);
+        case 4: return run_plain<V, D, 4>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist, fu);
+        case 8: return run_plain<V, D, 8>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist, fu);
+        case 16: return run_plain<V, D, 16>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist, fu);
+        case 32: return run_plain<V, D, 32>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist, fu);
+        case 64: return run_plain<V, D, 64>(in, out, n, d, m, sz, hf, ws, L, st, ev, step, dist, fu);
         default: return MDX_ERR_INVALID;
     }
 }
@@ -418,24 +428,25 @@ template <class V>
 mdx_status dispatch_plain(const void* in, void* out, uint64_t n, mdx_discr dc, uint32_t* sz,
                           uint32_t* hf, unsigned char* ws, const PlainLayout& L, cudaStream_t st,
                           cudaEvent_t ev, PlainStep step = PlainStep::kBoth,
-                          const DistOut* dist = nullptr) {
+                          const DistOut* dist = nullptr, bool allow_fused = true) {
     if (use_mask(dc))
         return dispatch_plain_m<V>(in, out, n, DiscrMask{dc.m - 1u}, dc.m, sz, hf, ws, L, st, ev,
-                                   step, dist);
+                                   step, dist, allow_fused);
     return dispatch_plain_m<V>(in, out, n, DiscrMod::make(dc.m), dc.m, sz, hf, ws, L, st, ev, step,
-                               dist);
+                               dist, allow_fused);
 }
 
 // ------------------------------------------------------------- segmented --
 constexpr int kPlanThreads = 256;
 constexpr uint32_t kMaxPlanBlocks = 1024;
 constexpr int kFlagsTile = 4096;
+constexpr uint32_t kMaxFlagChunks = 4096;
 
 inline uint32_t window_elems(mdx_elem e) { return tile_elems(e); }
 
 struct SegLayout {
     size_t run_loc, grp_loc, blk_runs, blk_grps, runs, groups, groups_end, run_cnt, run_base,
-        offsets, flag_status, total;
+        offsets, flag_stage, flag_cnt, flag_pre, total;
     uint64_t max_runs, max_groups;
 };
 
@@ -459,11 +470,13 @@ inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool
     L.run_cnt = align_up(L.groups_end + 4 * L.max_groups, kAlign);
     L.run_base = align_up(L.run_cnt + 4ull * M * L.max_runs, kAlign);
     L.offsets = align_up(L.run_base + 4ull * M * L.max_runs, kAlign);
-    L.flag_status = L.offsets;
+    L.flag_stage = L.flag_cnt = L.flag_pre = L.offsets;
     L.total = L.offsets;
-    if (flags_form) {
-        L.flag_status = align_up(L.offsets + 8 * (n + 1), kAlign);
-        L.total = align_up(L.flag_status + 8 * ((n + kFlagsTile - 1) / kFlagsTile + 1), kAlign);
+    if (flags_form) {  // offsets, staged start positions, per-chunk counts and prefixes
+        L.flag_stage = align_up(L.offsets + 8 * (n + 1), kAlign);
+        L.flag_cnt = align_up(L.flag_stage + 4 * n, kAlign);
+        L.flag_pre = align_up(L.flag_cnt + 4 * kMaxFlagChunks, kAlign);
+        L.total = align_up(L.flag_pre + 4 * kMaxFlagChunks, kAlign);
     }
     return L;
 }
@@ -573,18 +586,26 @@ mdx_status dispatch_segm(const void* in, void* out, uint64_t n, mdx_discr dc, co
 // area) and S into the header, ahead of run_segm with kSegsOnDevice.
 inline mdx_status launch_flags_to_offsets(const int32_t* d_flags, uint64_t n, unsigned char* ws,
                                           const SegLayout& L, cudaStream_t st) {
-    uint64_t* offs = reinterpret_cast<uint64_t*>(ws + L.offsets);
+    auto stage_fn = seg_flags_stage<kThreads, kFlagsTile>;
     int blocks = 0, sms = 0;
-    auto conv = seg_flags_to_offsets<kThreads, kFlagsTile>;
-    if (occupancy(reinterpret_cast<const void*>(conv), 0, &blocks, &sms) != cudaSuccess)
+    if (occupancy(reinterpret_cast<const void*>(stage_fn), 0, &blocks, &sms) != cudaSuccess)
         return MDX_ERR_CUDA;
-    const uint32_t tiles = static_cast<uint32_t>((n + kFlagsTile - 1) / kFlagsTile);
-    uint32_t G = static_cast<uint32_t>(blocks) * sms;
+    const uint64_t tiles = (n + kFlagsTile - 1) / kFlagsTile;
+    uint64_t G = static_cast<uint64_t>(blocks) * sms;
     if (G > tiles) G = tiles;
-    if (cudaMemsetAsync(ws + L.flag_status, 0, sizeof(uint64_t) * (tiles + 1), st) != cudaSuccess)
-        return MDX_ERR_CUDA;
-    conv<<<G, kThreads, 0, st>>>(d_flags, n, offs, reinterpret_cast<SegHeader*>(ws),
-                                 reinterpret_cast<uint64_t*>(ws + L.flag_status));
+    if (G > kMaxFlagChunks) G = kMaxFlagChunks;
+    if (G < 1) G = 1;
+    FlagsArgs fa;
+    fa.flags = d_flags;
+    fa.n = n;
+    fa.chunk = ((n + G - 1) / G + 3u) & ~uint64_t{3};
+    fa.stage = reinterpret_cast<uint32_t*>(ws + L.flag_stage);
+    fa.cnt = reinterpret_cast<uint32_t*>(ws + L.flag_cnt);
+    fa.pre = reinterpret_cast<uint32_t*>(ws + L.flag_pre);
+    fa.offsets = reinterpret_cast<uint64_t*>(ws + L.offsets);
+    fa.hdr = reinterpret_cast<SegHeader*>(ws);
+    stage_fn<<<static_cast<uint32_t>(G), kThreads, 0, st>>>(fa);
+    seg_flags_compact<kThreads><<<static_cast<uint32_t>(G), kThreads, 0, st>>>(fa);
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
 }
 

@@ -31,8 +31,8 @@
 //                   and tile_scatter (as the plain scatter), from those
 //                   positions.
 //
-// The partition kernels wait on no other CTA, only on their own bulk copies;
-// the head-flag converter below waits on earlier tiles (decoupled look-back).
+// The partition kernels and the head-flag converter wait on no other CTA, only
+// on their own bulk copies.
 // Every wait is bounded by kWaitLimitNs; one that runs out latches
 // kErrTimeout and publishes what it has, so no other CTA waits forever.
 //
@@ -57,17 +57,6 @@ constexpr int kRunTiles = 8;     // tiles per run of a large segment
 constexpr int kGroupBatch = 8;   // small-segment groups per ticket of seg_main
 constexpr int kMaxGroupBatch = 32;
 
-// look-back status word of the head-flag converter: [63:34] epoch (30 bits),
-// [33:32] state, [31:0] count
-constexpr uint64_t kStAgg = 1ull;
-constexpr uint64_t kStInc = 2ull;
-
-__device__ __forceinline__ uint64_t st_pack(uint32_t epoch, uint64_t state, uint32_t v) {
-    return (static_cast<uint64_t>(epoch & 0x3fffffffu) << 34) | (state << 32) | v;
-}
-__device__ __forceinline__ uint32_t st_epoch(uint64_t w) { return static_cast<uint32_t>(w >> 34); }
-__device__ __forceinline__ uint64_t st_state(uint64_t w) { return (w >> 32) & 3ull; }
-
 struct SegHeader {      // lives at the start of the segmented workspace
     uint32_t ticket;    // seg_main's group-batch tickets (reset by the planner)
     uint32_t error;     // latched error bits
@@ -77,9 +66,9 @@ struct SegHeader {      // lives at the start of the segmented workspace
     uint32_t plan_done; // planner CTA ticket
     uint64_t num_segs;  // S (written by the flags converter for the head-flag form)
     uint32_t reserved2;
-    uint32_t flags_ticket;  // tile ticket of the flags converter
-    uint32_t flags_done;    // finished tiles of the flags converter
-    uint32_t flags_epoch;   // look-back epoch of the flags converter
+    uint32_t reserved3;
+    uint32_t flags_done;    // finished chunks of the flags converter (reset by its last CTA)
+    uint32_t reserved4;
     uint32_t num_groups;    // small-segment groups this call
     uint32_t ticket2;       // run-scatter ticket counter (reset by the planner)
     uint32_t ticket3;       // run-count ticket counter (reset by the planner)
@@ -247,12 +236,6 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         a.hdr->ticket2 = 0u;
         a.hdr->ticket3 = 0u;
         a.hdr->plan_done = 0u;
-        // head-flag converter state for its next call
-        a.hdr->flags_ticket = 0u;
-        a.hdr->flags_done = 0u;
-        uint32_t fe = a.hdr->flags_epoch + 1u;
-        if (fe >= (1u << 30)) fe = 1u;
-        a.hdr->flags_epoch = fe;
     }
 }
 
@@ -349,20 +332,6 @@ struct SegSmem {
     static constexpr size_t kRingBytes = static_cast<size_t>(STAGES) * kTile * sizeof(V);
     static constexpr size_t kRunBytes = 1024 + kRingBytes + G::kStageBytes + G::kCntBytes;
 };
-
-// Bounded spin on a status word until it carries this epoch with state >=
-// `want`.  Returns false on timeout.
-__device__ __forceinline__ bool wait_status(const uint64_t* p, uint32_t epoch, uint64_t want,
-                                            uint64_t& w) {
-    w = ld_acquire_u64(p);
-    if (st_epoch(w) == epoch && st_state(w) >= want) return true;
-    const uint64_t t0 = globaltimer_ns();
-    for (;;) {
-        w = ld_acquire_u64(p);
-        if (st_epoch(w) == epoch && st_state(w) >= want) return true;
-        if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
-    }
-}
 
 // Per-thread class counters in 16-bit fields (M <= 16: (M+1)/2 words), wide
 // enough for any count within one group (< 2P < 2^16 elements).
@@ -1140,96 +1109,114 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
 // ------------------------------------------------ head flags -> offsets --
 // The reference's segment descriptor (MdiscrSegmHost.cu.h:36-42,
 // populateSizesArray HelpersCommon.h:105-151) is an n-entry array holding each
-// segment's length at its first element and 0 elsewhere.  One pass of a
-// decoupled look-back compaction writes the start positions (offsets[0..S-1]),
-// offsets[S] = n, and S into the header; the planner then checks that every
-// flag equals the distance to the next start.  Tiles of FT flags, dynamic tile
-// tickets, per-tile status words tagged with the converter's epoch.
+// segment's length at its first element and 0 elsewhere.  Two launches turn it
+// into offsets[0..S] and S (in the header); the planner then checks that every
+// flag equals the distance to the next start.
+//
+//   seg_flags_stage    CTA k reads chunk k of the flags once (tiles of FT
+//                      flags, 16 per thread), writes the positions of its
+//                      non-zero flags in order into its own part of a staging
+//                      array (stage[chunk start + j]) and its count; the last
+//                      CTA to finish (ticket, no waiting) scans the chunk
+//                      counts into chunk prefixes, S and offsets[S] = n.
+//   seg_flags_compact  CTA k moves its staged positions to offsets[prefix + j].
+//
+// No CTA waits on another: the single pass with a decoupled look-back that
+// this replaces spent most of its time walking predecessors, because ~10^3
+// tiles of a few microseconds each were in flight at once.
+struct FlagsArgs {
+    const int32_t* flags;
+    uint64_t n;
+    uint64_t chunk;      // flags per chunk (a multiple of 4)
+    uint32_t* stage;     // [n] staged start positions, chunk k's from k * chunk
+    uint32_t* cnt;       // [G] start positions per chunk
+    uint32_t* pre;       // [G] exclusive prefix of cnt
+    uint64_t* offsets;   // [S + 1]
+    SegHeader* hdr;
+};
+
 template <int THREADS, int FT>
-__global__ void __launch_bounds__(THREADS) seg_flags_to_offsets(const int32_t* flags, uint64_t n,
-                                                                uint64_t* offsets, SegHeader* hdr,
-                                                                uint64_t* tile_status) {
+__global__ void __launch_bounds__(THREADS) seg_flags_stage(FlagsArgs fa) {
     constexpr int ITEMS = FT / THREADS;
     constexpr int W = THREADS / 32;
-    static_assert(ITEMS * THREADS == FT, "tile");
-    __shared__ uint32_t tile_sh, base_sh, warp_tot[W];
+    static_assert(ITEMS * THREADS == FT && ITEMS % 4 == 0, "tile");
+    __shared__ uint32_t warp_tot[W];
     __shared__ int last_sh;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t num_tiles = static_cast<uint32_t>((n + FT - 1) / FT);
-    const uint32_t epoch = hdr->flags_epoch;
-    for (;;) {
-        if (tid == 0) tile_sh = atomicAdd(&hdr->flags_ticket, 1u);
-        __syncthreads();
-        const uint32_t t = tile_sh;
-        if (t >= num_tiles) break;
-        const uint64_t ts = static_cast<uint64_t>(t) * FT;
-        // blocked: thread holds flags ts + tid*ITEMS .. +ITEMS-1
-        uint32_t nz = 0;
+    const uint64_t c0 = min(static_cast<uint64_t>(blockIdx.x) * fa.chunk, fa.n);
+    const uint64_t c1 = min(c0 + fa.chunk, fa.n);
+    const bool vec = (reinterpret_cast<uintptr_t>(fa.flags) & 15u) == 0;
+    uint32_t running = 0;  // start positions of this chunk so far
+    bool bad = false;
+    for (uint64_t ts = c0; ts < c1; ts += FT) {
+        const uint64_t e0 = ts + static_cast<uint64_t>(tid) * ITEMS;
         int32_t f[ITEMS];
+        if (vec && e0 + ITEMS <= c1) {
+#pragma unroll
+            for (int q = 0; q < ITEMS / 4; q++) {
+                const int4 r = __ldg(reinterpret_cast<const int4*>(fa.flags + e0) + q);
+                f[4 * q] = r.x; f[4 * q + 1] = r.y; f[4 * q + 2] = r.z; f[4 * q + 3] = r.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < ITEMS; q++) f[q] = e0 + q < c1 ? __ldg(fa.flags + e0 + q) : 0;
+        }
+        uint32_t nz = 0;
 #pragma unroll
         for (int q = 0; q < ITEMS; q++) {
-            const uint64_t i = ts + static_cast<uint64_t>(tid) * ITEMS + q;
-            f[q] = i < n ? flags[i] : 0;
             nz += f[q] != 0 ? 1u : 0u;
+            bad |= f[q] < 0;
         }
         const uint32_t incl = warp_incl_scan(nz);
         if (lane == 31) warp_tot[warp] = incl;
         __syncthreads();
         uint32_t wpre = 0, agg = 0;
-        for (int w = 0; w < W; w++) {
-            wpre += w < warp ? warp_tot[w] : 0u;
-            agg += warp_tot[w];
-        }
-        if (warp == 0) {
-            uint32_t prefix = 0;
-            bool ok = true;
-            if (lane == 0) {
-                uint64_t* st = tile_status + t;
-                if (t == 0) {
-                    st_release_u64(st, st_pack(epoch, kStInc, agg));
-                } else {
-                    st_release_u64(st, st_pack(epoch, kStAgg, agg));
-                    for (uint32_t tt = t - 1u;; tt--) {
-                        uint64_t w;
-                        if (!wait_status(tile_status + tt, epoch, kStAgg, w)) {
-                            ok = false;
-                            break;
-                        }
-                        prefix += static_cast<uint32_t>(w);
-                        if (st_state(w) == kStInc) break;
-                    }
-                    st_release_u64(st, st_pack(epoch, kStInc, prefix + agg));
-                }
-                if (!ok) atomicOr(&hdr->error, kErrTimeout);
-                base_sh = prefix;
-            }
-        }
-        __syncthreads();
-        uint32_t pos = base_sh + wpre + incl - nz;
 #pragma unroll
-        for (int q = 0; q < ITEMS; q++) {
-            if (f[q] != 0) {
-                if (f[q] < 0) atomicOr(&hdr->error, kErrSegments);
-                offsets[pos++] = ts + static_cast<uint64_t>(tid) * ITEMS + q;
-            }
+        for (int w = 0; w < W; w++) {
+            const uint32_t x = warp_tot[w];
+            wpre += w < warp ? x : 0u;
+            agg += x;
         }
-        // the tile that finishes last writes S and offsets[S]
-        if (tid == 0) {
-            __threadfence();
-            last_sh = (atomicAdd(&hdr->flags_done, 1u) == num_tiles - 1u);
-        }
-        __syncthreads();
-        if (last_sh && tid == 0) {
-            const uint64_t w = ld_acquire_u64(tile_status + (num_tiles - 1u));
-            const uint64_t S = static_cast<uint32_t>(w);
-            hdr->num_segs = S;
-            offsets[S] = n;
-            if (n > 0 && flags[0] == 0) atomicOr(&hdr->error, kErrSegments);
-            // the ticket, done counter and epoch are reset by the planner,
-            // which runs after every CTA of this kernel has left its loop
-        }
-        __syncthreads();
+        uint32_t pos = running + wpre + incl - nz;
+#pragma unroll
+        for (int q = 0; q < ITEMS; q++)
+            if (f[q] != 0) fa.stage[c0 + pos++] = static_cast<uint32_t>(e0 + q);
+        running += agg;
+        __syncthreads();  // warp_tot is rewritten by the next tile
     }
+    if (bad) atomicOr(&fa.hdr->error, kErrSegments);
+    if (tid == 0) {
+        fa.cnt[blockIdx.x] = running;
+        __threadfence();
+        last_sh = (atomicAdd(&fa.hdr->flags_done, 1u) == gridDim.x - 1u);
+    }
+    __syncthreads();
+    if (!last_sh) return;
+    __threadfence();
+    // last CTA: exclusive scan of the chunk counts (one warp), S, offsets[S]
+    if (warp == 0) {
+        uint64_t run = 0;
+        for (uint32_t b0 = 0; b0 < gridDim.x; b0 += 32) {
+            const uint32_t b = b0 + lane;
+            const uint32_t x = b < gridDim.x ? __ldcg(&fa.cnt[b]) : 0u;
+            const uint32_t inc = warp_incl_scan(x);
+            if (b < gridDim.x) fa.pre[b] = static_cast<uint32_t>(run) + inc - x;
+            run += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        if (lane == 0) {
+            fa.hdr->num_segs = run;
+            fa.offsets[run] = fa.n;
+            if (fa.n > 0 && __ldg(fa.flags) == 0) atomicOr(&fa.hdr->error, kErrSegments);
+            fa.hdr->flags_done = 0u;  // for the next call
+        }
+    }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) seg_flags_compact(FlagsArgs fa) {
+    const uint64_t c0 = min(static_cast<uint64_t>(blockIdx.x) * fa.chunk, fa.n);
+    const uint32_t k = fa.cnt[blockIdx.x], p = fa.pre[blockIdx.x];
+    for (uint32_t j = threadIdx.x; j < k; j += THREADS) fa.offsets[p + j] = fa.stage[c0 + j];
 }
 
 }  // namespace mdx

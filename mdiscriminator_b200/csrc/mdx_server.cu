@@ -53,6 +53,11 @@
 #include "../../include/mdx.h"
 
 namespace mdx {
+// mdx_partition without the cooperative one-kernel path (mdx_capi.cu): the
+// in-place lanes run next to the batches and to each other.
+mdx_status partition_two_kernel(const void* d_in, void* d_out, uint64_t n, mdx_elem elem,
+                                mdx_discr discr, uint32_t* d_sizes, uint32_t* d_headflags,
+                                void* d_ws, size_t ws_bytes, mdx_stream_t stream);
 namespace server {
 
 constexpr int kCopyThreads = 256;
@@ -433,8 +438,9 @@ void scheduler(Server* s) {
             s->st_direct++;
             lk.unlock();
             const mdx_discr dc = {MDX_DISCR_MOD, r->m};
-            mdx_status st = mdx_partition(r->in, r->out, r->n, MDX_ELEM_U32, dc, r->sizes, nullptr,
-                                          l->ws, l->ws_bytes, reinterpret_cast<mdx_stream_t>(l->stream));
+            mdx_status st = partition_two_kernel(r->in, r->out, r->n, MDX_ELEM_U32, dc, r->sizes,
+                                                 nullptr, l->ws, l->ws_bytes,
+                                                 reinterpret_cast<mdx_stream_t>(l->stream));
             lk.lock();
             auto done = [s, l, r](double t) {
                 complete(s, r, t);
