@@ -373,6 +373,9 @@ typedef struct {
     uint32_t group_batch;        /* segmented: small-segment groups per work item (default 8, at most 32) */
     uint32_t plain_two_kernel;   /* plain path: 1 = count and scatter as two kernels; 0 (default) =
                                     one cooperative kernel where the input allows TMA */
+    uint32_t pool_pct;           /* one-kernel plain path: % of every chunk's tiles that the CTAs
+                                    share by ticket at the end of each phase (0: default 25;
+                                    100: none) */
 } mdx_tuning;
 
 mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,

@@ -75,7 +75,9 @@ inline uint32_t max_chunks_of(uint64_t n, mdx_elem e) {
 }
 
 struct PlainLayout {
-    size_t class_base, class_tot, chunk_cnt, chunk_pre, total;
+    size_t class_base, class_tot, chunk_cnt, chunk_pre;
+    size_t ready, tile_cnt, tile_pre;  // the one-kernel path's ready words and [tile][class] tables
+    size_t total;
 };
 
 inline PlainLayout plain_layout(uint64_t n, mdx_elem e, uint32_t m) {
@@ -86,8 +88,14 @@ inline PlainLayout plain_layout(uint64_t n, mdx_elem e, uint32_t m) {
     L.class_base = kHeaderBytes;
     L.class_tot = L.class_base + kMaxClasses * 4;
     L.chunk_cnt = align_up(L.class_tot + kMaxClasses * 4, kAlign);
-    L.chunk_pre = align_up(L.chunk_cnt + M * G * 4, kAlign);
-    L.total = align_up(L.chunk_pre + M * G * 4, kAlign);
+    // [class][chunk] counts, then the chunks' ready words right after them
+    // (one memset clears both), then the [class][chunk] prefixes
+    L.ready = L.chunk_cnt + M * G * 4;
+    L.chunk_pre = align_up(L.ready + 4 * G, kAlign);
+    const size_t T = num_tiles_of(n, e);
+    L.tile_cnt = align_up(L.chunk_pre + M * G * 4, kAlign);
+    L.tile_pre = align_up(L.tile_cnt + M * T * 4, kAlign);
+    L.total = align_up(L.tile_pre + M * T * 4, kAlign);
     return L;
 }
 
@@ -207,6 +215,7 @@ struct Tuning {
     uint32_t run_tiles = kRunTiles;
     uint32_t group_batch = kGroupBatch;
     uint32_t plain_two_kernel = 0;  // 1: count and scatter as two kernels
+    uint32_t pool_pct = 0;          // one-kernel path: % of every chunk drained by ticket (0: default)
 };
 struct TuningTable {
     std::mutex mu;
@@ -252,9 +261,11 @@ static_assert(kDistSkipOffset >= kPlainDoneOffset + 4 && kDistSkipOffset + 4 <= 
 // arrivals its grid barrier expects beyond the grid, and the wait's limit.
 inline std::atomic<uint32_t> g_test_bar_extra{0};
 inline std::atomic<uint64_t> g_test_wait_ns{0};
-// Grid barrier of the one-kernel plain path: arrival counter and generation.
+// Grid barrier and chunk tickets of the one-kernel plain path: arrival
+// counter, generation, count-phase and scatter-phase tickets.
 constexpr size_t kFusedBarOffset = 200;
-static_assert(kFusedBarOffset >= kDistSkipOffset + 4 && kFusedBarOffset + 8 <= kHeaderBytes,
+constexpr uint32_t kFusedPoolPct = 25;  // share of every chunk drained by ticket (default)
+static_assert(kFusedBarOffset >= kDistSkipOffset + 4 && kFusedBarOffset + 16 <= kHeaderBytes,
               "barrier words inside the header");
 
 template <class V, class D, int M>
@@ -334,11 +345,25 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
             fa.p.num_chunks = FG;
             fa.p.use_tma = 1;
             fa.chunk_stride = (FG + 3u) & ~3u;
+            // pool: this share of every chunk's tiles is drained by ticket
+            const uint32_t min_len = nt / FG;
+            const uint32_t pct = tun.pool_pct ? tun.pool_pct : kFusedPoolPct;
+            fa.pool = pct >= 100u ? 0u : min_len * pct / 100u;
+            if (fa.pool >= min_len) fa.pool = min_len > 0 ? min_len - 1u : 0u;
+            fa.tile_cnt = reinterpret_cast<uint32_t*>(ws + L.tile_cnt);
+            fa.tile_pre = reinterpret_cast<uint32_t*>(ws + L.tile_pre);
+            fa.ready = reinterpret_cast<uint32_t*>(ws + L.ready);
             fa.bar_count = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset);
             fa.bar_gen = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 4);
+            fa.cnt_ticket = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 8);
+            fa.sct_ticket = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 12);
             fa.bar_extra = g_test_bar_extra.load();
             const uint64_t lim = g_test_wait_ns.load();
             fa.wait_ns = lim != 0 ? lim : kWaitLimitNs;
+            // chunk sums are added up by atomics; ready words start unset
+            if (cudaMemsetAsync(ws + L.chunk_cnt, 0, L.ready + 4 * FG - L.chunk_cnt, stream) !=
+                cudaSuccess)
+                return MDX_ERR_CUDA;
             const OutFlat<V> o{static_cast<V*>(d_out),
                                static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
                                                      (16u / sizeof(V) - 1u))};
