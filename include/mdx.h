@@ -374,7 +374,7 @@ typedef struct {
     uint32_t plain_two_kernel;   /* plain path: 1 = count and scatter as two kernels; 0 (default) =
                                     one cooperative kernel where the input allows TMA */
     uint32_t pool_pct;           /* one-kernel plain path: % of every chunk's tiles that the CTAs
-                                    share by ticket at the end of each phase (0: default 25;
+                                    share by ticket at the end of each phase (0: default 10;
                                     100: none) */
 } mdx_tuning;
 

@@ -151,16 +151,30 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     // producer (thread 0): own tiles, then pool tickets
     uint32_t p_own = 0;  // own tiles issued
     bool p_done = false;
+    // the next pool ticket is taken one tile ahead, so the atomic's round trip
+    // overlaps a tile instead of delaying the copy it names
+    uint32_t p_ticket = 0;
+    bool p_have = false;
     auto produce = [&](uint32_t slot, bool scatter) {
         uint32_t m = kSlotEnd;
         const uint32_t own_n = t1 - own_lo;
+        uint32_t* tk = scatter ? fa.sct_ticket : fa.cnt_ticket;
         if (p_own < own_n) {
             m = scatter ? t1 - 1u - p_own : own_lo + p_own;
             p_own++;
+            if (p_own == own_n && q > 0) {
+                p_ticket = atomicAdd(tk, 1u);
+                p_have = true;
+            }
         } else if (!p_done) {
-            const uint32_t t = atomicAdd(scatter ? fa.sct_ticket : fa.cnt_ticket, 1u);
-            if (t < G * q) m = pool_tile(t, scatter) | kSlotPool;
-            else p_done = true;
+            const uint32_t t = p_have ? p_ticket : atomicAdd(tk, 1u);
+            if (t < G * q) {
+                m = pool_tile(t, scatter) | kSlotPool;
+                p_ticket = atomicAdd(tk, 1u);
+                p_have = true;
+            } else {
+                p_done = true;
+            }
         }
         meta[slot] = m;
         const uint32_t tile = m & ~kSlotPool;
@@ -462,6 +476,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     // --------------------------------------------------------- scatter phase
     p_own = 0;
     p_done = false;
+    p_have = false;
     if (tid == 0)
         for (uint32_t s = 0; s < STAGES; s++) produce((seq + s) % STAGES, true);
     // a pool tile's cursors (thread c < M): its chunk's base + its prefix in

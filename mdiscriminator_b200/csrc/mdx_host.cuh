@@ -264,7 +264,7 @@ inline std::atomic<uint64_t> g_test_wait_ns{0};
 // Grid barrier and chunk tickets of the one-kernel plain path: arrival
 // counter, generation, count-phase and scatter-phase tickets.
 constexpr size_t kFusedBarOffset = 200;
-constexpr uint32_t kFusedPoolPct = 25;  // share of every chunk drained by ticket (default)
+constexpr uint32_t kFusedPoolPct = 10;  // share of every chunk drained by ticket (default)
 static_assert(kFusedBarOffset >= kDistSkipOffset + 4 && kFusedBarOffset + 16 <= kHeaderBytes,
               "barrier words inside the header");
 
@@ -311,6 +311,11 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.m = m;
     a.use_tma = 0;
     a.skip = nullptr;
+    a.chunk_stride = (G + 3u) & ~3u;
+    // a whole call: every scatter CTA forms its own prefixes (no serial scan);
+    // the distributed steps keep the scan in the count kernel, whose class
+    // totals go to the other ranks before the scatter
+    a.prefix_in_scatter = step == PlainStep::kBoth ? 1 : 0;
     if (m == 1 && step == PlainStep::kBoth) {  // one class: the partition is a copy
         if ((d_headflags != nullptr &&
              cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess) ||
@@ -399,8 +404,24 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
             const OutFlat<V> o{static_cast<V*>(d_out),
                                static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
                                                      (16u / sizeof(V) - 1u))};
-            plain_scatter_tma_kernel<V, D, M, kThreads, kStages>
-                <<<G, kThreads, smem, stream>>>(a, d, map, o);
+            auto scatter = plain_scatter_tma_kernel<V, D, M, kThreads, kStages>;
+            if (step == PlainStep::kBoth && ev_mid == nullptr) {
+                // programmatic dependent launch: scheduled while the count grid
+                // drains, it starts its first tile copies before waiting for it
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(G);
+                cfg.blockDim = dim3(kThreads);
+                cfg.dynamicSmemBytes = smem;
+                cfg.stream = stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                attr[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                if (cudaLaunchKernelEx(&cfg, scatter, a, d, map, o) != cudaSuccess) return MDX_ERR_CUDA;
+            } else {
+                scatter<<<G, kThreads, smem, stream>>>(a, d, map, o);
+            }
         } else if constexpr (sizeof(V) == 16) {
             return MDX_ERR_UNSUPPORTED;  // no sharded 16-byte record kernels
         } else {

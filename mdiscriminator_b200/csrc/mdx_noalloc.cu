@@ -202,6 +202,8 @@ mdx_status run(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint3
     a.error = reinterpret_cast<uint32_t*>(ws) + 1;
     a.m = m;
     a.skip = nullptr;
+    a.chunk_stride = G;
+    a.prefix_in_scatter = 0;  // the last counting CTA scans the chunk counts
     CUtensorMap map;
     a.use_tma = row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
     const OutFlat<V> o{static_cast<V*>(d_out),

@@ -60,7 +60,21 @@ struct PlainArgs {
     uint32_t m;
     int use_tma;          // the tensor map passed to the scatter kernel is valid
     const uint32_t* skip; // scatter: return at once if *skip != 0 (null: never)
+    uint32_t chunk_stride;   // row stride of chunk_cnt / chunk_pre (>= num_chunks; a multiple
+                             // of 4 when prefix_in_scatter)
+    int prefix_in_scatter;   // 1: the count kernel only counts; every scatter CTA forms its
+                             // own chunk prefix and the class bases (CTA 0 writes sizes and
+                             // head flags).  0: the last counting CTA scans them for all.
 };
+
+// Programmatic dependent launch: the count kernel lets the scatter grid be
+// scheduled at once; the scatter waits for the count grid's results (its
+// memory operations complete and visible) only where it needs them.  Both are
+// no-ops in a launch without the programmatic attribute.
+__device__ __forceinline__ void pdl_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Chunk k covers tiles [k*T/G, (k+1)*T/G).
 __device__ __forceinline__ void chunk_tiles(uint32_t k, uint32_t T, uint32_t G, uint32_t& t0,
@@ -169,7 +183,8 @@ __device__ void plain_finish_scan(const PlainArgs& a, uint32_t* tot_sh) {
             const uint32_t kb = k0 + lane * PER;
             uint32_t x[PER];
 #pragma unroll
-            for (uint32_t q = 0; q < PER; q++) x[q] = kb + q < G ? __ldcg(&a.chunk_cnt[c * G + kb + q]) : 0u;
+            for (uint32_t q = 0; q < PER; q++)
+                x[q] = kb + q < G ? __ldcg(&a.chunk_cnt[c * a.chunk_stride + kb + q]) : 0u;
             uint32_t s = 0;
 #pragma unroll
             for (uint32_t q = 0; q < PER; q++) s += x[q];
@@ -177,7 +192,7 @@ __device__ void plain_finish_scan(const PlainArgs& a, uint32_t* tot_sh) {
             uint32_t pre = run + incl - s;
 #pragma unroll
             for (uint32_t q = 0; q < PER; q++) {
-                if (kb + q < G) a.chunk_pre[c * G + kb + q] = pre;
+                if (kb + q < G) a.chunk_pre[c * a.chunk_stride + kb + q] = pre;
                 pre += x[q];
             }
             run += __shfl_sync(0xffffffffu, incl, 31);
@@ -201,16 +216,17 @@ __device__ void plain_finish_scan(const PlainArgs& a, uint32_t* tot_sh) {
 }
 
 template <class V, class D, int M, int THREADS, int TILE>
-__global__ void __launch_bounds__(THREADS) plain_count_kernel(PlainArgs a, D d) {
+__global__ void __launch_bounds__(THREADS, 4) plain_count_kernel(PlainArgs a, D d) {
     constexpr int W = THREADS / 32;
     constexpr int VEC = 16 / static_cast<int>(sizeof(V));
-    constexpr int UNROLL = 4;
+    constexpr int UNROLL = M <= 8 ? 8 : 4;  // 16-byte loads in flight per thread (registers allowing)
     __shared__ uint32_t red[W][M];
     __shared__ uint32_t tot_sh[M];
     __shared__ int am_last;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t G = a.num_chunks, k = blockIdx.x;
+    pdl_launch_dependents();  // the scatter grid may be scheduled as CTAs here finish
     uint32_t t0, t1;
     chunk_tiles(k, a.num_tiles, G, t0, t1);
     const uint64_t e0 = static_cast<uint64_t>(t0) * TILE;
@@ -240,7 +256,7 @@ __global__ void __launch_bounds__(THREADS) plain_count_kernel(PlainArgs a, D d) 
 #pragma unroll
                         for (int q = 0; q < VEC; q++) pc.add(d(e[q]));
                     }
-                    if (u & 1) pc.fold();  // every two vectors: <= 8 increments
+                    if (VEC == 4 ? (u & 1) : ((u & 3) == 3)) pc.fold();  // <= 8 increments
                 }
             }
             uint32_t k = 0;
@@ -302,8 +318,9 @@ __global__ void __launch_bounds__(THREADS) plain_count_kernel(PlainArgs a, D d) 
         uint32_t s = 0;
 #pragma unroll
         for (int w = 0; w < W; w++) s += red[w][tid];
-        a.chunk_cnt[tid * G + k] = s;
+        a.chunk_cnt[tid * a.chunk_stride + k] = s;
     }
+    if (a.prefix_in_scatter) return;  // the scatter CTAs form the prefixes
     __threadfence();
     __syncthreads();
     if (tid == 0) am_last = (atomicAdd(a.done, 1u) == G - 1u);
@@ -352,8 +369,9 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
 
     __shared__ __align__(8) uint64_t bars[STAGES];
     __shared__ TileShared<M> sh;
+    __shared__ uint32_t tot_sh[M], pre_sh[M];
 
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t G = a.num_chunks, k = blockIdx.x;
     uint32_t t0, t1;
     chunk_tiles(k, a.num_tiles, G, t0, t1);
@@ -365,12 +383,14 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
     // mismatch found by plain_dist_bases_kernel leaves everything unwritten
     if (a.skip != nullptr && *a.skip != 0u) return;
 
-    if (tid < M)
-        sh.cursor[0][tid] = a.class_base[tid] + a.chunk_pre[tid * G + k] + a.chunk_cnt[tid * G + k];
     if (tid == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; s++) mbar_init(&bars[s], 1);
         mbar_fence_init();
+    }
+    if (tid < M) {
+        tot_sh[tid] = 0u;
+        pre_sh[tid] = 0u;
     }
     __syncthreads();
 
@@ -386,8 +406,67 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
             mbar_arrive(bar);
         }
     };
+    // the first tiles only read the input: their copies start before the
+    // count grid's results are needed
     if (tid == 0)
         for (uint32_t i = 0; i < STAGES && i < cnt; i++) issue(i);
+    pdl_wait();
+    const uint32_t stride = a.chunk_stride;
+    if (a.prefix_in_scatter) {
+        // this chunk's exclusive class prefix and the class totals from the
+        // [class][chunk] counts (TPC threads per class, 16-byte loads)
+        constexpr int TPC = THREADS / M;
+        constexpr int RW = TPC < 32 ? TPC : 32;
+        const uint32_t c = static_cast<uint32_t>(tid / TPC), l = static_cast<uint32_t>(tid % TPC);
+        const uint4* row = reinterpret_cast<const uint4*>(a.chunk_cnt + static_cast<uint64_t>(c) * stride);
+        uint32_t tot = 0, pre = 0;
+        for (uint32_t q4 = l; q4 < stride / 4u; q4 += TPC) {
+            const uint4 x = __ldcg(row + q4);
+            const uint32_t j = 4u * q4;
+            const uint32_t xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (uint32_t u = 0; u < 4; u++) {
+                const uint32_t v = (j + u < G) ? xv[u] : 0u;
+                tot += v;
+                pre += (j + u < k) ? v : 0u;
+            }
+        }
+#pragma unroll
+        for (int off = RW / 2; off > 0; off >>= 1) {
+            tot += __shfl_xor_sync(0xffffffffu, tot, off);
+            pre += __shfl_xor_sync(0xffffffffu, pre, off);
+        }
+        if ((lane % RW) == 0) {
+            atomicAdd(&tot_sh[c], tot);
+            atomicAdd(&pre_sh[c], pre);
+        }
+        __syncthreads();
+        if (warp == 0) {  // class bases: exclusive scan of the totals
+            uint32_t carry = 0;
+#pragma unroll
+            for (int h = 0; h < (M + 31) / 32; h++) {
+                const uint32_t cc = static_cast<uint32_t>(lane + 32 * h);
+                const uint32_t x = cc < static_cast<uint32_t>(M) ? tot_sh[cc] : 0u;
+                const uint32_t incl = warp_incl_scan(x);
+                const uint32_t bc = carry + incl - x;
+                if (cc < static_cast<uint32_t>(M)) {
+                    sh.cursor[0][cc] = bc + pre_sh[cc] + __ldcg(a.chunk_cnt + static_cast<uint64_t>(cc) * stride + k);
+                    if (k == 0) {
+                        a.class_base[cc] = bc;
+                        a.class_tot[cc] = x;
+                        if (a.sizes != nullptr && cc < a.m) a.sizes[cc] = x;
+                        // head-flag form (SeqMdiscr.h:47-49); zeroed before the count kernel
+                        if (a.headflags != nullptr && x > 0) a.headflags[bc] = x;
+                    }
+                }
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+        }
+    } else if (tid < M) {
+        const uint64_t o = static_cast<uint64_t>(tid) * stride + k;
+        sh.cursor[0][tid] = a.class_base[tid] + a.chunk_pre[o] + a.chunk_cnt[o];
+    }
+    __syncthreads();
 
     const uint32_t e0 = tid * ITEMS;
     for (uint32_t i = 0; i < cnt; i++) {

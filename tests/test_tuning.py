@@ -19,7 +19,7 @@ def test_tuning_table_roundtrip_and_validation():
                    plain_ctas_per_sm=2)
     t = mdx.get_tuning(mdx.ELEM_U32, 7, 3000)  # m=7 -> class bound 8, log2 3000 -> 12
     assert t == {"plain_ctas_per_sm": 2, "run_tiles": 4, "group_batch": 16, "plain_two_kernel": 1,
-                 "pool_pct": 25}
+                 "pool_pct": 10}
     assert mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20) == other_bucket   # other bucket untouched
     assert mdx.get_tuning(mdx.ELEM_REC8, 7, 3000) == other_layout     # other element layout
     with pytest.raises(mdx.MdxError):
