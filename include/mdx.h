@@ -342,6 +342,7 @@ typedef struct {
     uint64_t direct;              /* requests partitioned in place */
     double queue_p50_s, queue_p99_s;  /* submit -> launch of the request's batch (or lane) */
     double exec_p50_s, exec_p99_s;    /* launch -> completion stamp */
+    double launch_busy_s;             /* host time spent issuing launches since the reset */
 } mdx_server_stats;
 
 mdx_status mdx_server_create(mdx_server* server, const mdx_server_config* config);

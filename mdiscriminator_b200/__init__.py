@@ -653,7 +653,8 @@ class ServerStats(ctypes.Structure):
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double), ("mean_s", ctypes.c_double),
                 ("window_s", ctypes.c_double), ("direct", ctypes.c_uint64),
                 ("queue_p50_s", ctypes.c_double), ("queue_p99_s", ctypes.c_double),
-                ("exec_p50_s", ctypes.c_double), ("exec_p99_s", ctypes.c_double)]
+                ("exec_p50_s", ctypes.c_double), ("exec_p99_s", ctypes.c_double),
+                ("launch_busy_s", ctypes.c_double)]
 
 
 def _bind_server(L):

@@ -4,9 +4,10 @@ table mdiscriminator_b200 loads at import (tuning.json).
 Keys: element layout (4-byte values / 8-byte records), class bound (the
 smallest power of two >= m) and a range of ceil(log2 n).  Knobs:
 
-* plain path: CTAs per SM of the chunk grid (`plain_ctas_per_sm`), and one
-  cooperative kernel against count and scatter as two kernels
-  (`plain_two_kernel`);
+* plain path: count and scatter as two kernels against one cooperative
+  kernel (`plain_two_kernel`), CTAs per SM of the chunk grid
+  (`plain_ctas_per_sm`) and, for the one-kernel path, the share of every chunk
+  drained by ticket (`pool_pct`);
 * segmented path: tiles per run of a large segment (`run_tiles`) and
   small-segment groups per work item (`group_batch`).
 
@@ -33,11 +34,16 @@ if os.path.dirname(HERE) not in sys.path:
 
 import mdiscriminator_b200 as mdx  # noqa: E402
 
-# n buckets: (timed n, ceil(log2 n) range the winner is installed for)
-BUCKETS = [(1 << 20, (0, 21)), (1 << 24, (22, 25)), (1 << 27, (26, 33))]
+# n buckets: (timed n of 4-byte values, ceil(log2 n) range the winner is
+# installed for); 8-byte records are timed at half the count (same bytes)
+BUCKETS = [(1 << 20, (0, 21)), (1 << 24, (22, 25)), (1 << 28, (26, 33))]
+
+# plain-path candidates: (plain_two_kernel, plain_ctas_per_sm, pool_pct)
+PLAIN_CANDIDATES = [(1, 4, 0), (1, 3, 0), (1, 0, 0),
+                    (0, 4, 100), (0, 4, 10), (0, 4, 20), (0, 4, 33), (0, 3, 10)]
 
 
-def timeit(fn, torch, reps=9, warm=2):
+def timeit(fn, torch, reps=20, warm=3):
     for _ in range(warm):
         fn()
     torch.cuda.synchronize()
@@ -79,27 +85,32 @@ def main(argv=None):
     for elem in (mdx.ELEM_U32, mdx.ELEM_REC8):
         ename = "u32" if elem == mdx.ELEM_U32 else "rec8"
         dtype = torch.int32 if elem == mdx.ELEM_U32 else torch.int64
-        for n, (lo, hi) in buckets:
+        for n4, (lo, hi) in buckets:
+            n = n4 if elem == mdx.ELEM_U32 else n4 // 2
             d = torch.randint(0, 1 << 31, (n,), device=dev, dtype=torch.int64, generator=g).to(dtype)
             out = torch.empty_like(d)
             ws = mdx.new_workspace(mdx.workspace_size(n, elem, 64), dev)
             for M in bounds:
                 sizes = torch.empty(M, dtype=torch.uint32, device=dev)
                 best = None
-                for k, two in itertools.product((2, 3, 4, 0), (0, 1)):
-                    mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=k, plain_two_kernel=two)
+                for two, k, pool in PLAIN_CANDIDATES:
+                    mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=k, plain_two_kernel=two,
+                                   pool_pct=pool)
                     ms = timeit(lambda: mdx.partition(d, ("mask", M), out=out, sizes=sizes, ws=ws),
                                 torch)
+                    if ws.error() != mdx.MDX_OK:
+                        raise SystemExit(f"device error while tuning {ename} m={M}")
                     if best is None or ms < best[0]:
-                        best = (ms, k, two)
+                        best = (ms, k, two, pool)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "plain",
                                 "plain_ctas_per_sm": best[1], "plain_two_kernel": best[2],
-                                "ms": best[0]})
+                                "pool_pct": best[3], "ms": best[0]})
                 mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=best[1],
-                               plain_two_kernel=best[2])
+                               plain_two_kernel=best[2], pool_pct=best[3])
             del d, out, ws
         seg_bounds = [2, 4, 8, 16]
-        for n_target, (lo, hi) in buckets:
+        for n4, (lo, hi) in buckets:
+            n_target = min(n4 if elem == mdx.ELEM_U32 else n4 // 2, 1 << 27)
             offs = lognormal_offsets(n_target, 3)
             n = int(offs[-1])
             S = len(offs) - 1
@@ -115,20 +126,23 @@ def main(argv=None):
                 pe = next(e for e in entries
                           if e["elem"] == ename and e["m"] == M and e["path"] == "plain"
                           and e["log2_n"] == [lo, hi])
-                plain_k, plain_two = pe["plain_ctas_per_sm"], pe["plain_two_kernel"]
+                plain_k, plain_two, pool = pe["plain_ctas_per_sm"], pe["plain_two_kernel"], pe["pool_pct"]
                 best = None
                 for rt, gb in cands:
                     mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
-                                   plain_two_kernel=plain_two, run_tiles=rt, group_batch=gb)
+                                   plain_two_kernel=plain_two, pool_pct=pool, run_tiles=rt,
+                                   group_batch=gb)
                     ms = timeit(lambda: mdx.partition_segmented(d, do, ("mask", M), out=out,
-                                                                seg_sizes=ss, ws=ws), torch, reps=5)
+                                                                seg_sizes=ss, ws=ws), torch)
                     if best is None or ms < best[0]:
                         best = (ms, rt, gb)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "segmented",
                                 "plain_ctas_per_sm": plain_k, "plain_two_kernel": plain_two,
-                                "run_tiles": best[1], "group_batch": best[2], "ms": best[0]})
+                                "pool_pct": pool, "run_tiles": best[1], "group_batch": best[2],
+                                "ms": best[0]})
                 mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
-                               plain_two_kernel=plain_two, run_tiles=best[1], group_batch=best[2])
+                               plain_two_kernel=plain_two, pool_pct=pool, run_tiles=best[1],
+                               group_batch=best[2])
             del d, out, ws
     # one entry per key: the segmented entry (it carries the plain knob too)
     merged = {}

@@ -269,6 +269,7 @@ struct Server {
 
     // statistics
     uint64_t st_submitted = 0, st_completed = 0, st_batches = 0, st_elements = 0, st_direct = 0;
+    double st_launch_s = 0;  // host time inside launch calls
     std::vector<double> latencies, queue_lat, exec_lat;
     double st_t0 = 0, st_t_last = 0;
 
@@ -438,10 +439,13 @@ void scheduler(Server* s) {
             s->st_direct++;
             lk.unlock();
             const mdx_discr dc = {MDX_DISCR_MOD, r->m};
+            const double tl0 = now_s();
             mdx_status st = partition_two_kernel(r->in, r->out, r->n, MDX_ELEM_U32, dc, r->sizes,
                                                  nullptr, l->ws, l->ws_bytes,
                                                  reinterpret_cast<mdx_stream_t>(l->stream));
+            const double tl1 = now_s();
             lk.lock();
+            s->st_launch_s += tl1 - tl0;
             auto done = [s, l, r](double t) {
                 complete(s, r, t);
                 l->inflight--;
@@ -493,8 +497,11 @@ void scheduler(Server* s) {
         s->inflight_batches++;
         s->st_batches++;
         lk.unlock();
+        const double tl0 = now_s();
         mdx_status st = launch_batch(s, sl, batch);
+        const double tl1 = now_s();
         lk.lock();
+        s->st_launch_s += tl1 - tl0;
         auto done = [s, b](double t) { finish_batch(s, b, t); };
         if (st != MDX_OK || !track(s, sl.waiter, sl.stream, done)) {
             // nothing will complete this batch: finish it now
@@ -685,6 +692,7 @@ mdx_status mdx_server_get_stats(mdx_server h, mdx_server_stats* out) {
     out->exec_p99_s = pct(s.exec_lat, 0.99);
     out->window_s = s.st_t_last > s.st_t0 ? s.st_t_last - s.st_t0 : 0.0;
     out->direct = s.st_direct;
+    out->launch_busy_s = s.st_launch_s;
     return MDX_OK;
 }
 
@@ -693,6 +701,7 @@ mdx_status mdx_server_reset_stats(mdx_server h) {
     Server& s = h->s;
     std::lock_guard<std::mutex> lk(s.mu);
     s.st_submitted = s.st_completed = s.st_batches = s.st_elements = s.st_direct = 0;
+    s.st_launch_s = 0;
     s.latencies.clear();
     s.queue_lat.clear();
     s.exec_lat.clear();
