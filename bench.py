@@ -287,7 +287,15 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
     the server's request pool; requests' data in device memory (views of a
     resident array, outputs to distinct slices).  p50 / p99 latency (submit to
     completion) and elements/s per load, against one plain partition per
-    request issued back to back on one stream."""
+    request issued back to back on one stream.
+
+    The load generator runs with Python's garbage collector off (one
+    collection before each load): a generation-2 collection inside the submit
+    loop paused submission for 63 ms at 50k requests/s, after which the next
+    ~3,000 requests went in as one burst above the server's capacity and their
+    queueing, not the server's, set the p99.  `max_lag_ms` reports how far
+    the submissions ran behind their Poisson schedule."""
+    import gc
     import math
 
     import numpy as np
@@ -298,8 +306,7 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
     out_pool = torch.empty(1 << 30, dtype=torch.int32, device=dev)
     sizes_pool = torch.empty((1 << 16, 16), dtype=torch.int32, device=dev)
     res = []
-    srv = mdx.Server(budget_bytes=16 << 30, num_streams=4, max_batch_requests=1024,
-                     max_batch_elems=1 << 28)
+    srv = mdx.Server(budget_bytes=16 << 30, num_streams=4, max_batch_requests=1024)
 
     def make_requests(k):
         n = np.exp(rng.uniform(math.log(1 << 10), math.log(1 << 24), size=k)).astype(np.int64)
@@ -321,32 +328,40 @@ def served_measurement(torch, mdx, dev, peak, loads=(1000, 5000, 20000, 50000), 
         k = max(int(load * duration_s), 200)
         reqs = make_requests(k)
         arrivals = np.cumsum(rng.exponential(1.0 / load, size=k))
+        gc.collect()
+        gc.disable()
         srv.reset_stats()
         tickets = []
+        lag = 0.0
         t0 = time.perf_counter()
         for (d_in, d_out, sz, m, _), ta in zip(reqs, arrivals):
             while time.perf_counter() - t0 < ta:
                 pass
+            lag = max(lag, time.perf_counter() - t0 - ta)
             tickets.append(srv.submit(d_in, d_out, sz, m))
         t_sub = time.perf_counter() - t0
+        gc.enable()
         for t in tickets:
             srv.wait(t)
         st = srv.stats()
         elems = sum(r[4] for r in reqs)
         res.append({"offered_req_per_s": load, "achieved_submit_rate": k / t_sub,
-                    "requests": k, "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
+                    "max_lag_ms": lag * 1e3, "requests": k, "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3,
                     "queue_p99_ms": st["queue_p99_s"] * 1e3, "exec_p99_ms": st["exec_p99_s"] * 1e3,
                     "direct": st["direct"],
                     "gelem_per_s": elems / st["window_s"] / 1e9 if st["window_s"] > 0 else None,
                     "batches": st["batches"], "mean_request_elems": elems / k})
     # capacity: every request of a closed batch submitted at once
     reqs = make_requests(2000)
+    gc.collect()
+    gc.disable()
     srv.reset_stats()
     t0 = time.perf_counter()
     tickets = [srv.submit(d_in, d_out, sz, m) for d_in, d_out, sz, m, _ in reqs]
     for t in tickets:
         srv.wait(t)
     t_all = time.perf_counter() - t0
+    gc.enable()
     st = srv.stats()
     elems = sum(r[4] for r in reqs)
     saturated = {"requests": len(reqs), "gelem_per_s": elems / t_all / 1e9,

@@ -327,7 +327,8 @@ typedef struct {
     uint64_t budget_bytes;        /* device memory for request data (both rings) */
     uint32_t num_streams;         /* batches in flight at once (0: 2) */
     uint32_t max_batch_requests;  /* requests per batched launch (0: 1024, <= 65535) */
-    uint64_t max_batch_elems;     /* elements per batched launch (0: ring size) */
+    uint64_t max_batch_elems;     /* elements per batched launch (0: 2^24, at most the ring);
+                                     also the longest request the pool takes */
     uint32_t m_max;               /* largest m a request may use (0: 16, <= 16) */
     uint64_t direct_min_elems;    /* requests at least this long whose buffers are device
                                      memory are partitioned in place, without the pool's

@@ -16,14 +16,14 @@
 //    input into its ring slot, the per-segment-m segmented partition
 //    (mdx_partition_segmented_multi: one segment per request), a scatter
 //    kernel copying results and class sizes back to each request, and an
-//    event whose completion the slot's waiter thread stamps.  Requests that arrive while
+//    event whose completion the poller thread stamps.  Requests that arrive while
 //    batches run are admitted as ring space frees and launched on another
 //    stream: their work overlaps the batches already on the device.
 //  * In place: a request of at least direct_min_elems whose buffers are all
 //    device memory (and do not overlap) takes no ring space; it is admitted in
 //    its FIFO turn and partitioned by the plain kernels straight on its own
-//    buffers, queued on two lanes (a stream and a workspace each, up to four
-//    requests in stream order on each), so
+//    buffers, queued on four lanes (a stream, a workspace and a launcher
+//    thread each, up to four requests in stream order on each), so
 //    the long requests that carry most elements skip the pool's two copies
 //    and do not cut the runs of short requests that share a batch.
 //  * Priorities: the batch streams (short requests) are created with the
@@ -61,6 +61,7 @@ mdx_status partition_two_kernel(const void* d_in, void* d_out, uint64_t n, mdx_e
 namespace server {
 
 constexpr int kCopyThreads = 256;
+constexpr uint64_t kDefaultBatchElems = 1ull << 24;  // elements per batched launch (default)
 constexpr uint32_t kCopyChunk = 8192;  // elements per copy CTA
 
 struct CopyJob {            // one request in a batch
@@ -191,15 +192,14 @@ struct Batch;
 
 // Completion of the work on one stream: the scheduler records an event after
 // each unit of work (a batch, an in-place request) and queues it here with
-// what to do when it is done; the waiter thread waits for the events in order
-// (cudaEventSynchronize, without the server's lock), stamps the time and runs
-// the action under the lock.  Nothing is queued on the stream itself, so the
-// stream never stalls on the host.
+// what to do when it is done.  One poller thread serves every stream's queue:
+// it queries the front events (cudaEventQuery, without the server's lock),
+// stamps the time and runs the actions under the lock.  Nothing is queued on
+// the stream itself, so the stream never stalls on the host.  One polling
+// thread, instead of a cudaEventSynchronize spinning per stream, keeps the
+// server to one busy core however many streams it drives.
 struct Waiter {
     std::deque<std::pair<cudaEvent_t, std::function<void(double)>>> q;  // under Server::mu
-    std::condition_variable cv;
-    bool stop = false;
-    std::thread th;
 };
 
 struct Slot {                   // one stream's worth of batch resources
@@ -207,13 +207,12 @@ struct Slot {                   // one stream's worth of batch resources
     cudaStream_t stream = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
-    uint64_t* d_offsets = nullptr;  // [max_batch + 1]
-    uint32_t* d_seg_m = nullptr;    // [max_batch]
     uint32_t* d_seg_sizes = nullptr;  // [max_batch * m_max]
-    CopyJob* d_jobs = nullptr;      // [2 * max_batch]: gather then scatter
-    uint64_t* h_offsets = nullptr;  // pinned staging
-    uint32_t* h_seg_m = nullptr;
-    CopyJob* h_jobs = nullptr;
+    // a batch's descriptors, packed: segment offsets [S + 1], per-segment m [S],
+    // copy jobs [2 S] (gather then scatter); staged in pinned memory and
+    // uploaded by one copy
+    unsigned char* d_desc = nullptr;
+    unsigned char* h_desc = nullptr;
     bool busy = false;
 };
 
@@ -230,9 +229,26 @@ struct Lane {
     cudaStream_t stream = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
-    uint32_t inflight = 0;
+    uint32_t inflight = 0;      // queued for launch or on the GPU
+    std::deque<Req*> todo;      // assigned by the scheduler, not launched yet (under Server::mu)
+    std::condition_variable cv;
+    bool stop = false;
+    std::thread launcher;       // issues this lane's launches, off the scheduler thread
     Waiter waiter;
 };
+
+// Packed batch descriptors: byte offsets of the three parts for S requests.
+struct DescLayout {
+    size_t offsets, seg_m, jobs, total;
+};
+inline DescLayout desc_layout(uint32_t S) {
+    DescLayout d;
+    d.offsets = 0;
+    d.seg_m = (sizeof(uint64_t) * (S + 1) + 15) & ~size_t{15};
+    d.jobs = (d.seg_m + sizeof(uint32_t) * S + 15) & ~size_t{15};
+    d.total = d.jobs + sizeof(CopyJob) * 2 * S;
+    return d;
+}
 
 struct Batch {
     int slot;
@@ -265,6 +281,10 @@ struct Server {
     uint64_t next_id = 1;
     bool stop = false;
     std::thread sched;
+    std::vector<Waiter*> waiters;  // every slot's and lane's completion queue
+    std::condition_variable cv_poll;
+    bool poll_stop = false;
+    std::thread poller;
     mdx_status sticky = MDX_OK;   // first failure of a launch (reported by wait)
 
     // statistics
@@ -304,20 +324,47 @@ struct Server {
     }
 };
 
-void waiter_loop(Server* s, Waiter* w) {
+// The poller: completes tracked work in each stream's order.  While anything
+// is in flight it polls the front events (a pause of a few hundred
+// nanoseconds between rounds that find nothing); with nothing in flight it
+// sleeps until track() queues an event.
+void poll_loop(Server* s) {
+    cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
+    std::vector<std::pair<Waiter*, cudaEvent_t>> fronts;
+    std::vector<cudaError_t> res;
     for (;;) {
-        while (w->q.empty() && !w->stop) w->cv.wait(lk);
-        if (w->q.empty()) break;  // stopped with nothing in flight
-        cudaEvent_t ev = w->q.front().first;
+        fronts.clear();
+        for (Waiter* w : s->waiters)
+            if (!w->q.empty()) fronts.emplace_back(w, w->q.front().first);
+        if (fronts.empty()) {
+            if (s->poll_stop) break;
+            s->cv_poll.wait(lk);
+            continue;
+        }
         lk.unlock();
-        cudaEventSynchronize(ev);
+        res.resize(fronts.size());
+        bool any = false;
+        for (size_t i = 0; i < fronts.size(); i++) {
+            res[i] = cudaEventQuery(fronts[i].second);
+            any = any || res[i] != cudaErrorNotReady;
+        }
+        if (!any) {
+            for (int k = 0; k < 64; k++) __builtin_ia32_pause();
+            lk.lock();
+            continue;
+        }
         const double t = now_s();
         lk.lock();
-        auto done = std::move(w->q.front().second);
-        w->q.pop_front();
-        done(t);
-        s->free_events.push_back(ev);
+        for (size_t i = 0; i < fronts.size(); i++) {
+            if (res[i] == cudaErrorNotReady) continue;
+            if (res[i] != cudaSuccess && s->sticky == MDX_OK) s->sticky = MDX_ERR_CUDA;
+            Waiter* w = fronts[i].first;  // only this thread pops: the front is unchanged
+            auto done = std::move(w->q.front().second);
+            w->q.pop_front();
+            done(t);
+            s->free_events.push_back(fronts[i].second);
+        }
         s->cv_sched.notify_all();
     }
 }
@@ -336,7 +383,7 @@ bool track(Server* s, Waiter& w, cudaStream_t st, std::function<void(double)> do
         return false;
     }
     w.q.emplace_back(ev, std::move(done));
-    w.cv.notify_one();
+    s->cv_poll.notify_one();
     return true;
 }
 
@@ -387,36 +434,73 @@ void finish_batch(Server* s, Batch* b, double t_done) {
 mdx_status launch_batch(Server* s, Slot& sl, const std::vector<Req*>& batch) {
     const uint64_t base = batch.front()->off;
     const uint32_t S = static_cast<uint32_t>(batch.size());
+    const DescLayout dl = desc_layout(S);
+    uint64_t* h_offsets = reinterpret_cast<uint64_t*>(sl.h_desc + dl.offsets);
+    uint32_t* h_seg_m = reinterpret_cast<uint32_t*>(sl.h_desc + dl.seg_m);
+    CopyJob* h_jobs = reinterpret_cast<CopyJob*>(sl.h_desc + dl.jobs);
     uint64_t acc = 0;
     uint32_t chunks = 0;
     for (uint32_t i = 0; i < S; i++) {
         Req* r = batch[i];
-        sl.h_offsets[i] = acc;
-        sl.h_seg_m[i] = r->m;
-        sl.h_jobs[i] = CopyJob{r->in, s->d_in + r->off, r->n, nullptr, nullptr, 0, chunks};
-        sl.h_jobs[S + i] = CopyJob{s->d_out + r->off, r->out, r->n,
-                                   sl.d_seg_sizes + static_cast<uint64_t>(i) * s->cfg.m_max,
-                                   r->sizes, r->m, chunks};
+        h_offsets[i] = acc;
+        h_seg_m[i] = r->m;
+        h_jobs[i] = CopyJob{r->in, s->d_in + r->off, r->n, nullptr, nullptr, 0, chunks};
+        h_jobs[S + i] = CopyJob{s->d_out + r->off, r->out, r->n,
+                                sl.d_seg_sizes + static_cast<uint64_t>(i) * s->cfg.m_max,
+                                r->sizes, r->m, chunks};
         chunks += static_cast<uint32_t>((r->n + kCopyChunk - 1) / kCopyChunk);
         acc += r->n;
     }
-    sl.h_offsets[S] = acc;
+    h_offsets[S] = acc;
     cudaStream_t st = sl.stream;
-    if (cudaMemcpyAsync(sl.d_offsets, sl.h_offsets, sizeof(uint64_t) * (S + 1),
-                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(sl.d_seg_m, sl.h_seg_m, sizeof(uint32_t) * S, cudaMemcpyHostToDevice, st) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(sl.d_jobs, sl.h_jobs, sizeof(CopyJob) * 2 * S, cudaMemcpyHostToDevice, st) !=
-            cudaSuccess)
+    if (cudaMemcpyAsync(sl.d_desc, sl.h_desc, dl.total, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return MDX_ERR_CUDA;
-    copy_jobs<<<chunks, kCopyThreads, 0, st>>>(sl.d_jobs, S);
+    const uint64_t* d_offsets = reinterpret_cast<const uint64_t*>(sl.d_desc + dl.offsets);
+    const uint32_t* d_seg_m = reinterpret_cast<const uint32_t*>(sl.d_desc + dl.seg_m);
+    const CopyJob* d_jobs = reinterpret_cast<const CopyJob*>(sl.d_desc + dl.jobs);
+    copy_jobs<<<chunks, kCopyThreads, 0, st>>>(d_jobs, S);
     mdx_status r = mdx_partition_segmented_multi(
-        s->d_in + base, s->d_out + base, acc, MDX_ELEM_U32, sl.d_seg_m, s->cfg.m_max,
-        sl.d_offsets, S, sl.d_seg_sizes, nullptr, sl.ws, sl.ws_bytes,
+        s->d_in + base, s->d_out + base, acc, MDX_ELEM_U32, d_seg_m, s->cfg.m_max,
+        d_offsets, S, sl.d_seg_sizes, nullptr, sl.ws, sl.ws_bytes,
         reinterpret_cast<mdx_stream_t>(st));
     if (r != MDX_OK) return r;
-    copy_jobs<<<chunks, kCopyThreads, 0, st>>>(sl.d_jobs + S, S);
+    copy_jobs<<<chunks, kCopyThreads, 0, st>>>(d_jobs + S, S);
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+}
+
+// A lane's launcher: issues the in-place requests the scheduler assigned to
+// the lane, in order, so their host-side launch cost runs beside the
+// scheduler's batch launches instead of behind them.
+void lane_loop(Server* s, Lane* l) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        while (l->todo.empty() && !l->stop) l->cv.wait(lk);
+        if (l->todo.empty()) break;  // stopped with nothing assigned
+        Req* r = l->todo.front();
+        l->todo.pop_front();
+        r->t_launch = now_s();
+        lk.unlock();
+        const mdx_discr dc = {MDX_DISCR_MOD, r->m};
+        const double tl0 = now_s();
+        mdx_status st = partition_two_kernel(r->in, r->out, r->n, MDX_ELEM_U32, dc, r->sizes, nullptr,
+                                             l->ws, l->ws_bytes,
+                                             reinterpret_cast<mdx_stream_t>(l->stream));
+        const double tl1 = now_s();
+        lk.lock();
+        s->st_launch_s += tl1 - tl0;
+        auto done = [s, l, r](double t) {
+            complete(s, r, t);
+            l->inflight--;
+            s->cv_done.notify_all();
+        };
+        if (st != MDX_OK || !track(s, l->waiter, l->stream, done)) {
+            // nothing will complete this request: finish it now
+            if (s->sticky == MDX_OK) s->sticky = st != MDX_OK ? st : MDX_ERR_CUDA;
+            done(now_s());
+            s->cv_sched.notify_all();
+        }
+    }
 }
 
 void scheduler(Server* s) {
@@ -435,27 +519,9 @@ void scheduler(Server* s) {
             s->admitted_direct.pop_front();
             l->inflight++;
             r->launched = true;
-            r->t_launch = now_s();
             s->st_direct++;
-            lk.unlock();
-            const mdx_discr dc = {MDX_DISCR_MOD, r->m};
-            const double tl0 = now_s();
-            mdx_status st = partition_two_kernel(r->in, r->out, r->n, MDX_ELEM_U32, dc, r->sizes,
-                                                 nullptr, l->ws, l->ws_bytes,
-                                                 reinterpret_cast<mdx_stream_t>(l->stream));
-            const double tl1 = now_s();
-            lk.lock();
-            s->st_launch_s += tl1 - tl0;
-            auto done = [s, l, r](double t) {
-                complete(s, r, t);
-                l->inflight--;
-                s->cv_done.notify_all();
-            };
-            if (st != MDX_OK || !track(s, l->waiter, l->stream, done)) {
-                // nothing will complete this request: finish it now
-                if (s->sticky == MDX_OK) s->sticky = st != MDX_OK ? st : MDX_ERR_CUDA;
-                done(now_s());
-            }
+            l->todo.push_back(r);  // the lane's own thread issues it
+            l->cv.notify_one();
         }
         int free_slot = -1;
         for (size_t k = 0; k < s->slots.size(); k++)
@@ -537,7 +603,11 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
     s.cfg = cfg;
     s.cap = cfg.budget_bytes / 8;  // u32 input ring + u32 output ring
     if (s.cap > MDX_MAX_ELEMS) s.cap = MDX_MAX_ELEMS;
-    if (cfg.max_batch_elems == 0 || cfg.max_batch_elems > s.cap) s.cfg.max_batch_elems = s.cap;
+    // a batch runs at the batch streams' high priority: capped so that one
+    // batch cannot hold the GPU for long while in-place requests wait (without
+    // a cap, 50k requests/s queued long requests for ~14 ms at p99; 2^24: 0.24 ms)
+    if (cfg.max_batch_elems == 0) s.cfg.max_batch_elems = kDefaultBatchElems;
+    if (s.cfg.max_batch_elems > s.cap) s.cfg.max_batch_elems = s.cap;
     bool ok = cudaGetDevice(&s.device) == cudaSuccess &&
               dev_alloc(&s.d_in, s.cap * 4) == cudaSuccess &&
               dev_alloc(&s.d_out, s.cap * 4) == cudaSuccess;
@@ -551,13 +621,9 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
         ok = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_high) == cudaSuccess &&
              dev_alloc(&sl.ws, sl.ws_bytes) == cudaSuccess &&
              mdx_workspace_init(sl.ws, sl.ws_bytes, reinterpret_cast<mdx_stream_t>(sl.stream)) == MDX_OK &&
-             dev_alloc(&sl.d_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
-             dev_alloc(&sl.d_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
+             dev_alloc(&sl.d_desc, desc_layout(B).total) == cudaSuccess &&
              dev_alloc(&sl.d_seg_sizes, sizeof(uint32_t) * B * cfg.m_max) == cudaSuccess &&
-             dev_alloc(&sl.d_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess &&
-             pinned_alloc(&sl.h_offsets, sizeof(uint64_t) * (B + 1)) == cudaSuccess &&
-             pinned_alloc(&sl.h_seg_m, sizeof(uint32_t) * B) == cudaSuccess &&
-             pinned_alloc(&sl.h_jobs, sizeof(CopyJob) * 2 * B) == cudaSuccess;
+             pinned_alloc(&sl.h_desc, desc_layout(B).total) == cudaSuccess;
     }
     s.lanes = std::vector<Lane>(kLanes);  // sized once: completions hold Lane pointers
     for (auto& l : s.lanes) {
@@ -572,8 +638,10 @@ mdx_status mdx_server_create(mdx_server* out, const mdx_server_config* cfg_in) {
         return MDX_ERR_CUDA;
     }
     s.st_t0 = now_s();
-    for (auto& sl : s.slots) sl.waiter.th = std::thread(waiter_loop, &s, &sl.waiter);
-    for (auto& l : s.lanes) l.waiter.th = std::thread(waiter_loop, &s, &l.waiter);
+    for (auto& sl : s.slots) s.waiters.push_back(&sl.waiter);
+    for (auto& l : s.lanes) s.waiters.push_back(&l.waiter);
+    s.poller = std::thread(poll_loop, &s);
+    for (auto& l : s.lanes) l.launcher = std::thread(lane_loop, &s, &l);
     s.sched = std::thread(scheduler, &s);
     *out = h;
     return MDX_OK;
@@ -585,8 +653,7 @@ mdx_status mdx_server_submit(mdx_server h, const uint32_t* in, uint32_t* out, ui
                              uint64_t n, uint32_t m, uint64_t* ticket) {
     if (h == nullptr || ticket == nullptr) return MDX_ERR_INVALID;
     Server& s = h->s;
-    if (m < 1 || m > s.cfg.m_max || n == 0 || n > s.cap || n > s.cfg.max_batch_elems)
-        return MDX_ERR_INVALID;
+    if (m < 1 || m > s.cfg.m_max || n == 0 || n > MDX_MAX_ELEMS) return MDX_ERR_INVALID;
     // every buffer must be reachable from kernels: device memory, or
     // page-locked host memory mapped into the device's address space
     const uint32_t* d_in = device_view(in);
@@ -604,6 +671,11 @@ mdx_status mdx_server_submit(mdx_server h, const uint32_t* in, uint32_t* out, ui
         const char* ib = reinterpret_cast<const char*>(d_in);
         const char* ob = reinterpret_cast<const char*>(d_out);
         r->direct = !(ib < ob + n * 4 && ob < ib + n * 4);  // overlapping buffers go through the ring
+    }
+    // a request through the pool must fit one batch and the ring
+    if (!r->direct && (n > s.cap || n > s.cfg.max_batch_elems)) {
+        delete r;
+        return MDX_ERR_INVALID;
     }
     {
         std::lock_guard<std::mutex> lk(s.mu);
@@ -721,30 +793,27 @@ mdx_status mdx_server_destroy(mdx_server h) {
         s.cv_sched.notify_all();
         s.sched.join();
     }
-    {  // the scheduler left with nothing in flight: the waiters have no work left
+    {  // the scheduler left with nothing in flight: launchers and waiters have no work left
         std::lock_guard<std::mutex> lk(s.mu);
-        for (auto& sl : s.slots) sl.waiter.stop = true;
-        for (auto& l : s.lanes) l.waiter.stop = true;
-    }
-    for (auto& sl : s.slots) {
-        sl.waiter.cv.notify_all();
-        if (sl.waiter.th.joinable()) sl.waiter.th.join();
+        for (auto& l : s.lanes) l.stop = true;
     }
     for (auto& l : s.lanes) {
-        l.waiter.cv.notify_all();
-        if (l.waiter.th.joinable()) l.waiter.th.join();
+        l.cv.notify_all();
+        if (l.launcher.joinable()) l.launcher.join();
     }
+    {
+        std::lock_guard<std::mutex> lk(s.mu);
+        s.poll_stop = true;
+    }
+    s.cv_poll.notify_all();
+    if (s.poller.joinable()) s.poller.join();
     for (cudaEvent_t ev : s.free_events) cudaEventDestroy(ev);
     for (auto& sl : s.slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         cudaFree(sl.ws);
-        cudaFree(sl.d_offsets);
-        cudaFree(sl.d_seg_m);
+        cudaFree(sl.d_desc);
         cudaFree(sl.d_seg_sizes);
-        cudaFree(sl.d_jobs);
-        cudaFreeHost(sl.h_offsets);
-        cudaFreeHost(sl.h_seg_m);
-        cudaFreeHost(sl.h_jobs);
+        cudaFreeHost(sl.h_desc);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     for (auto& l : s.lanes) {

@@ -181,7 +181,8 @@ def test_cancel_before_launch(cuda_ready):
     others complete and equal the oracle."""
     import mdiscriminator_b200 as mdx
     torch = cuda_ready
-    with mdx.Server(budget_bytes=1 << 30, num_streams=1, direct_min_elems=1 << 40) as srv:
+    with mdx.Server(budget_bytes=1 << 30, num_streams=1, direct_min_elems=1 << 40,
+                    max_batch_elems=1 << 26) as srv:
         xa, da, oa = _request(torch, 1 << 26, 5)
         sa = _sizes(torch, 4)
         ta = srv.submit(da, oa, sa, 4)  # keeps the only batch stream busy
