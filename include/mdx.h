@@ -378,6 +378,11 @@ typedef struct {
     uint32_t pool_pct;           /* one-kernel plain path: % of every chunk's tiles that the CTAs
                                     share by ticket at the end of each phase (0: default 10;
                                     100: none) */
+    uint32_t mid_tiles;          /* segmented: a segment of more than one tile spanning at most this
+                                    many tiles (2, the most the medium-segment kernel holds) is read
+                                    once, counted and scattered from shared memory; 0 (default) and
+                                    1: none, every segment longer than a tile goes through count +
+                                    scatter runs */
 } mdx_tuning;
 
 mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,

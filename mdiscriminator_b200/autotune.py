@@ -8,8 +8,9 @@ smallest power of two >= m) and a range of ceil(log2 n).  Knobs:
   kernel (`plain_two_kernel`), CTAs per SM of the chunk grid
   (`plain_ctas_per_sm`) and, for the one-kernel path, the share of every chunk
   drained by ticket (`pool_pct`);
-* segmented path: tiles per run of a large segment (`run_tiles`) and
-  small-segment groups per work item (`group_batch`).
+* segmented path: tiles per run of a large segment (`run_tiles`),
+  small-segment groups per work item (`group_batch`) and whether segments of
+  two tiles are read once by the medium-segment kernel (`mid_tiles`).
 
 The reference picked its block shapes by recompiling with -D macros and
 timing them (cuda_code/run.py:12-96); here the choice is made at run time.
@@ -128,21 +129,25 @@ def main(argv=None):
                           and e["log2_n"] == [lo, hi])
                 plain_k, plain_two, pool = pe["plain_ctas_per_sm"], pe["plain_two_kernel"], pe["pool_pct"]
                 best = None
-                for rt, gb in cands:
+                # (run_tiles, group_batch) without medium segments, then the
+                # winner with the medium-segment kernel on
+                for rt, gb, mid in [(rt, gb, 1) for rt, gb in cands] + [None]:
+                    if mid is None:
+                        rt, gb, mid = best[1], best[2], 2
                     mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
                                    plain_two_kernel=plain_two, pool_pct=pool, run_tiles=rt,
-                                   group_batch=gb)
+                                   group_batch=gb, mid_tiles=mid)
                     ms = timeit(lambda: mdx.partition_segmented(d, do, ("mask", M), out=out,
                                                                 seg_sizes=ss, ws=ws), torch)
                     if best is None or ms < best[0]:
-                        best = (ms, rt, gb)
+                        best = (ms, rt, gb, mid)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "segmented",
                                 "plain_ctas_per_sm": plain_k, "plain_two_kernel": plain_two,
                                 "pool_pct": pool, "run_tiles": best[1], "group_batch": best[2],
-                                "ms": best[0]})
+                                "mid_tiles": best[3], "ms": best[0]})
                 mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
                                plain_two_kernel=plain_two, pool_pct=pool, run_tiles=best[1],
-                               group_batch=best[2])
+                               group_batch=best[2], mid_tiles=best[3])
             del d, out, ws
     # one entry per key: the segmented entry (it carries the plain knob too)
     merged = {}

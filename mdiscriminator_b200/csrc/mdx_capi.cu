@@ -448,7 +448,8 @@ mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_
     if (check_elem(elem) != MDX_OK || t == nullptr || m < 1 || m > MDX_MAX_CLASSES ||
         log2_n_lo > log2_n_hi || log2_n_hi > 33)
         return MDX_ERR_INVALID;
-    if (t->run_tiles > 64 || t->group_batch > 1024 || t->plain_two_kernel > 1 || t->pool_pct > 100)
+    if (t->run_tiles > 64 || t->group_batch > 1024 || t->plain_two_kernel > 1 || t->pool_pct > 100 ||
+        t->mid_tiles > static_cast<uint32_t>(kMidTiles))
         return MDX_ERR_INVALID;
     TuningTable& tt = tuning_table();
     std::lock_guard<std::mutex> lk(tt.mu);
@@ -459,6 +460,7 @@ mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_
         x.group_batch = t->group_batch ? t->group_batch : kGroupBatch;
         x.plain_two_kernel = t->plain_two_kernel;
         x.pool_pct = t->pool_pct;
+        x.mid_tiles = t->mid_tiles;
     }
     return MDX_OK;
 }
@@ -472,6 +474,7 @@ mdx_status mdx_get_tuning(mdx_elem elem, uint32_t m, uint64_t n, mdx_tuning* t) 
     t->group_batch = x.group_batch;
     t->plain_two_kernel = x.plain_two_kernel;
     t->pool_pct = x.pool_pct ? x.pool_pct : kFusedPoolPct;
+    t->mid_tiles = x.mid_tiles >= 2 ? x.mid_tiles : 1u;
     return MDX_OK;
 }
 

@@ -216,6 +216,7 @@ struct Tuning {
     uint32_t group_batch = kGroupBatch;
     uint32_t plain_two_kernel = 0;  // 1: count and scatter as two kernels
     uint32_t pool_pct = 0;          // one-kernel path: % of every chunk drained by ticket (0: default)
+    uint32_t mid_tiles = 0;         // segmented: medium segments up to this many tiles (0, 1: none)
 };
 struct TuningTable {
     std::mutex mu;
@@ -492,8 +493,8 @@ inline uint32_t window_elems(mdx_elem e) { return tile_elems(e); }
 
 struct SegLayout {
     size_t run_loc, grp_loc, blk_runs, blk_grps, runs, groups, groups_end, run_cnt, run_base,
-        offsets, flag_stage, flag_cnt, flag_pre, total;
-    uint64_t max_runs, max_groups;
+        mid_loc, blk_mids, mids, offsets, flag_stage, flag_cnt, flag_pre, total;
+    uint64_t max_runs, max_groups, max_mids;
 };
 
 // flags_form: room for n+1 offsets and the converter's tile status words.
@@ -515,7 +516,11 @@ inline SegLayout seg_layout(uint64_t n, uint64_t S, mdx_elem e, uint32_t m, bool
     L.groups_end = align_up(L.groups + 4 * L.max_groups, kAlign);
     L.run_cnt = align_up(L.groups_end + 4 * L.max_groups, kAlign);
     L.run_base = align_up(L.run_cnt + 4ull * M * L.max_runs, kAlign);
-    L.offsets = align_up(L.run_base + 4ull * M * L.max_runs, kAlign);
+    L.max_mids = n / (P + 1) + 2;  // a medium segment holds more than P elements
+    L.mid_loc = align_up(L.run_base + 4ull * M * L.max_runs, kAlign);
+    L.blk_mids = align_up(L.mid_loc + 4 * (S + 1), kAlign);
+    L.mids = align_up(L.blk_mids + 4 * kMaxPlanBlocks, kAlign);
+    L.offsets = align_up(L.mids + 4 * L.max_mids, kAlign);
     L.flag_stage = L.flag_cnt = L.flag_pre = L.offsets;
     L.total = L.offsets;
     if (flags_form) {  // offsets, staged start positions, per-chunk counts and prefixes
@@ -541,12 +546,15 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
                     const SegLayout& L, cudaStream_t st, const uint32_t* d_seg_m = nullptr) {
     using SL = SegSmem<V, M, kThreads, kStages>;
     constexpr int P = SL::kTile;
+    using ML = MidSmem<V, M, kThreads, kMidTiles>;
     auto main_fn = seg_main<V, D, M, kThreads, kStages>;
     auto scatter_fn = seg_run_scatter<V, D, M, kThreads, kStages>;
-    int blocks = 0, sms = 0, sblocks = 0;
+    auto mid_fn = seg_mid<V, D, M, kThreads, kMidTiles>;
+    int blocks = 0, sms = 0, sblocks = 0, mblocks = 0;
     if (occupancy(reinterpret_cast<const void*>(main_fn), SL::kBytes, &blocks, &sms) != cudaSuccess ||
         occupancy(reinterpret_cast<const void*>(scatter_fn), SL::kRunBytes, &sblocks, &sms) !=
-            cudaSuccess)
+            cudaSuccess ||
+        occupancy(reinterpret_cast<const void*>(mid_fn), ML::kBytes, &mblocks, &sms) != cudaSuccess)
         return MDX_ERR_CUDA;
     SegArgs a;
     a.in = d_in;
@@ -568,6 +576,10 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     a.groups_end = reinterpret_cast<uint32_t*>(ws + L.groups_end);
     a.run_cnt = reinterpret_cast<uint32_t*>(ws + L.run_cnt);
     a.run_base = reinterpret_cast<uint32_t*>(ws + L.run_base);
+    a.mid_loc = reinterpret_cast<uint32_t*>(ws + L.mid_loc);
+    a.blk_mids = reinterpret_cast<uint32_t*>(ws + L.blk_mids);
+    a.mids = reinterpret_cast<uint32_t*>(ws + L.mids);
+    a.max_mids = static_cast<uint32_t>(L.max_mids);
     a.plan_blocks = plan_blocks_for(S_bound);
     a.max_runs = static_cast<uint32_t>(L.max_runs);
     a.max_groups = static_cast<uint32_t>(L.max_groups);
@@ -578,6 +590,9 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         a.run_tiles = tun.run_tiles >= 1 ? tun.run_tiles : kRunTiles;
         a.group_batch = tun.group_batch >= 1 ? tun.group_batch : kGroupBatch;
         if (a.group_batch > static_cast<uint32_t>(kMaxGroupBatch)) a.group_batch = kMaxGroupBatch;
+        // 0 (default) and 1: no medium segments
+        a.mid_tiles = tun.mid_tiles >= 2 ? tun.mid_tiles : 0u;
+        if (a.mid_tiles > static_cast<uint32_t>(kMidTiles)) a.mid_tiles = kMidTiles;
     }
     CUtensorMap map;
     a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::G::kRows) ? 1 : 0;
@@ -589,6 +604,8 @@ mdx_status run_segm(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     seg_plan_spans<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
     seg_plan_emit<P, kPlanThreads><<<a.plan_blocks, kPlanThreads, 0, st>>>(a);
     main_fn<<<static_cast<uint32_t>(blocks) * sms, kThreads, SL::kBytes, st>>>(a, d);
+    if (a.mid_tiles > 0)
+        mid_fn<<<static_cast<uint32_t>(mblocks) * sms, kThreads, ML::kBytes, st>>>(a, d, map);
     {
         auto count_fn = seg_run_count<V, D, M, kThreads>;
         int cblocks = 0;

@@ -54,15 +54,16 @@ namespace mdx {
 
 // Defaults of the run-time knobs (the autotuner may choose others):
 constexpr int kRunTiles = 8;     // tiles per run of a large segment
+constexpr int kMidTiles = 2;     // most tiles a medium segment may span (seg_mid's slab)
 constexpr int kGroupBatch = 8;   // small-segment groups per ticket of seg_main
 constexpr int kMaxGroupBatch = 32;
 
 struct SegHeader {      // lives at the start of the segmented workspace
     uint32_t ticket;    // seg_main's group-batch tickets (reset by the planner)
     uint32_t error;     // latched error bits
-    uint32_t reserved0;
+    uint32_t num_mids;  // medium segments this call
     uint32_t num_runs;  // large-segment runs this call
-    uint32_t reserved1;
+    uint32_t ticket4;   // seg_mid's segment tickets (reset by the planner)
     uint32_t plan_done; // planner CTA ticket
     uint64_t num_segs;  // S (written by the flags converter for the head-flag form)
     uint32_t reserved2;
@@ -111,6 +112,12 @@ struct SegArgs {
     uint32_t m_bound;          // classes of any segment are < m_bound (per-segment m clamped)
     uint32_t run_tiles;        // tiles per run of a large segment
     uint32_t group_batch;      // small-segment groups per work item
+    uint32_t mid_tiles;        // a segment of more than one tile that spans at most this
+                               // many row-aligned tiles is medium (0: none are)
+    uint32_t* mid_loc;         // [S] block-local exclusive medium-segment offsets
+    uint32_t* blk_mids;        // [plan blocks] medium-segment totals, then offsets
+    uint32_t* mids;            // [max_mids] the medium segments, in order
+    uint32_t max_mids;
 };
 
 // The discriminator of segment s: the launch's, or -- when the call carries
@@ -142,6 +149,17 @@ __device__ __forceinline__ bool group_head(const SegArgs& a, uint64_t s, uint64_
     return s == 0 || a.offsets[s - 1] / GW != a0 / GW || (s % kGroupSegs) == 0;
 }
 
+// A segment [a0, a1) longer than one tile is medium when the tiles that hold
+// it, counted from the 128-byte row of its first element (a tile is
+// P * sizeof(V) = 16 KB, so a row is P / 128 elements), number at most
+// mid_tiles: seg_mid then reads it once.  The longer ones are cut into runs.
+template <int P>
+__device__ __forceinline__ bool is_mid(const SegArgs& a, uint64_t a0, uint64_t a1) {
+    constexpr uint64_t kPerRow = static_cast<uint64_t>(P) / 128u;
+    const uint64_t rb = a0 & ~(kPerRow - 1u);
+    return a.mid_tiles > 0u && (a1 - rb + P - 1u) / P <= a.mid_tiles;
+}
+
 __device__ __forceinline__ uint64_t seg_count(const SegArgs& a) {
     return a.num_segs == kSegsOnDevice ? a.hdr->num_segs : a.num_segs;
 }
@@ -151,24 +169,28 @@ __device__ __forceinline__ uint64_t seg_count(const SegArgs& a) {
 template <int P, int THREADS>
 __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
     constexpr int W = THREADS / 32;
-    __shared__ uint32_t warp_runs[W], warp_grps[W];
+    __shared__ uint32_t warp_runs[W], warp_grps[W], warp_mids[W];
     __shared__ int am_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t S = seg_count(a);
     const uint64_t G = gridDim.x;
     const uint64_t R = (S + G - 1) / G;
     const uint64_t s0 = blockIdx.x * R, s1 = min(s0 + R, S);
-    uint32_t carry_r = 0, carry_g = 0;
+    uint32_t carry_r = 0, carry_g = 0, carry_m = 0;
     for (uint64_t base = s0; base < s1; base += THREADS) {
         const uint64_t s = base + tid;
-        uint32_t runs = 0, head = 0;
+        uint32_t runs = 0, head = 0, mid = 0;
         if (s < s1) {
             const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
             if (a1 < a0 || a1 > a.n || (s == 0 && a0 != 0) || (s + 1 == S && a1 != a.n)) {
                 atomicOr(&a.hdr->error, kErrSegments);
             } else if (a1 - a0 > static_cast<uint64_t>(P)) {
-                const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
-                runs = (span + a.run_tiles - 1) / a.run_tiles;
+                if (is_mid<P>(a, a0, a1)) {
+                    mid = 1;
+                } else {
+                    const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
+                    runs = (span + a.run_tiles - 1) / a.run_tiles;
+                }
             } else {
                 head = group_head<P>(a, s, a0) ? 1u : 0u;
             }
@@ -180,30 +202,37 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         }
         const uint32_t ir = warp_incl_scan(runs);
         const uint32_t ig = warp_incl_scan(head);
+        const uint32_t im = warp_incl_scan(mid);
         if (lane == 31) {
             warp_runs[warp] = ir;
             warp_grps[warp] = ig;
+            warp_mids[warp] = im;
         }
         __syncthreads();
-        uint32_t pr = 0, pg = 0, tr = 0, tg = 0;
+        uint32_t pr = 0, pg = 0, pm = 0, tr = 0, tg = 0, tm = 0;
         for (int w = 0; w < W; w++) {
-            const uint32_t xr = warp_runs[w], xg = warp_grps[w];
+            const uint32_t xr = warp_runs[w], xg = warp_grps[w], xm = warp_mids[w];
             pr += (w < warp) ? xr : 0u;
             pg += (w < warp) ? xg : 0u;
+            pm += (w < warp) ? xm : 0u;
             tr += xr;
             tg += xg;
+            tm += xm;
         }
         if (s < s1) {
             a.run_loc[s] = carry_r + pr + ir - runs;
             a.grp_loc[s] = carry_g + pg + ig - head;
+            a.mid_loc[s] = carry_m + pm + im - mid;
         }
         carry_r += tr;
         carry_g += tg;
+        carry_m += tm;
         __syncthreads();
     }
     if (tid == 0) {
         a.blk_runs[blockIdx.x] = carry_r;
         a.blk_grps[blockIdx.x] = carry_g;
+        a.blk_mids[blockIdx.x] = carry_m;
     }
     __threadfence();
     __syncthreads();
@@ -212,8 +241,8 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
     if (!am_last) return;
     __threadfence();
     // last CTA: exclusive scans of the block totals (in place)
-    if (warp < 2) {
-        uint32_t* arr = warp == 0 ? a.blk_runs : a.blk_grps;
+    if (warp < 3) {
+        uint32_t* arr = warp == 0 ? a.blk_runs : warp == 1 ? a.blk_grps : a.blk_mids;
         uint32_t run = 0;
         for (uint32_t b0 = 0; b0 < gridDim.x; b0 += 32) {
             const uint32_t b = b0 + lane;
@@ -225,8 +254,10 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         if (lane == 0) {
             if (warp == 0) {
                 a.hdr->num_runs = run <= a.max_runs ? run : 0u;  // over capacity: malformed
-            } else {
+            } else if (warp == 1) {
                 a.hdr->num_groups = run <= a.max_groups ? run : 0u;
+            } else {
+                a.hdr->num_mids = run <= a.max_mids ? run : 0u;
             }
         }
     }
@@ -235,6 +266,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
         a.hdr->ticket = 0u;
         a.hdr->ticket2 = 0u;
         a.hdr->ticket3 = 0u;
+        a.hdr->ticket4 = 0u;
         a.hdr->plan_done = 0u;
     }
 }
@@ -249,7 +281,9 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
     const uint64_t R = (S + G - 1) / G;
     const uint64_t s0 = blockIdx.x * R, s1 = min(s0 + R, S);
     const uint32_t roff = a.blk_runs[blockIdx.x], goff = a.blk_grps[blockIdx.x];
+    const uint32_t moff = a.blk_mids[blockIdx.x];
     const uint32_t num_runs = a.hdr->num_runs, num_groups = a.hdr->num_groups;
+    const uint32_t num_mids = a.hdr->num_mids;
     for (uint64_t base = s0; base < s1; base += THREADS) {
         if (tid == 0) list_n = 0;
         __syncthreads();
@@ -257,7 +291,10 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
         if (s < s1) {
             const uint64_t a0 = a.offsets[s], a1 = a.offsets[s + 1];
             if (a1 >= a0 && a1 <= a.n) {
-                if (a1 - a0 > static_cast<uint64_t>(P)) {
+                if (a1 - a0 > static_cast<uint64_t>(P) && is_mid<P>(a, a0, a1)) {
+                    const uint32_t pos = moff + a.mid_loc[s];
+                    if (pos < num_mids) a.mids[pos] = static_cast<uint32_t>(s);
+                } else if (a1 - a0 > static_cast<uint64_t>(P)) {
                     const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
                     const uint32_t nr = (span + a.run_tiles - 1) / a.run_tiles;
                     const uint32_t pos = roff + a.run_loc[s];
@@ -1102,6 +1139,231 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         }
         ring_uses += ntiles;
         if (failed) break;
+    }
+    if (tid < M) bulk_wait_all();
+}
+
+// ------------------------------------------------------- medium segments --
+// A medium segment (more than one tile, at most mid_tiles <= KMAX row-aligned
+// tiles) is read from HBM once: all its tiles come by TMA into a shared slab;
+// a count pass over the slab gives the segment's class totals (its sizes, head
+// flags and the class cursors at its start); tile_scatter then places the
+// tiles from the slab in order with forward cursors, as the plain scatter
+// does.  The run path reads the same elements twice (count, then scatter).
+//
+// CTA b takes the medium segments b, b + G, b + 2G, ... (G CTAs), so it knows
+// its next segment in advance: the next segment's offsets are loaded during
+// the current count pass, and its tiles are requested while the current
+// segment is scattered -- a tile slot as soon as the current segment's tile
+// in it has been taken into registers, the slots the current segment does not
+// use at once.  The loads of one segment thus overlap the scatter of the one
+// before.  A slab of two tiles keeps the kernel at four CTAs per SM (a slab of
+// four at two CTAs per SM was slower: the tile step needs the occupancy).
+//
+// Measured (100,000 LogNormal(ln 1024, 1.5) segments, u32, m = 4): the
+// segments of two tiles take 165 us here against 152 us less in the run
+// kernels, so the single read does not pay for itself there -- the tile step,
+// not the re-read, bounds those segments (a segment of ~1.5 tiles costs two
+// tile steps either way).  It stays a tuned option (mid_tiles) and is off by
+// default.
+template <class V, int M, int THREADS, int KMAX>
+struct MidSmem {
+    using G = TileGeom<V, THREADS, M>;
+    static constexpr size_t kSlabBytes = static_cast<size_t>(KMAX) * G::kTile * sizeof(V);
+    static constexpr size_t kBytes = 1024 + kSlabBytes + G::kStageBytes + G::kCntBytes;
+};
+
+template <class V, class D, int M, int THREADS, int KMAX>
+__global__ void __launch_bounds__(THREADS, 4)
+    seg_mid(SegArgs a, D d, const __grid_constant__ CUtensorMap tmap) {
+    using L = MidSmem<V, M, THREADS, KMAX>;
+    using TG = typename L::G;
+    constexpr int ITEMS = TG::kItems;
+    constexpr int P = TG::kTile;
+    constexpr int ROWS = TG::kRows;
+    constexpr uint32_t AU = TG::kAU;
+    constexpr int W = THREADS / 32;
+    constexpr uint32_t kPerRow = 128u / sizeof(V);
+    static_assert(M <= 16 && M >= 2, "class bound");
+    static_assert(KMAX >= 2 && KMAX <= 32, "one phase bit per slab tile");
+    static_assert(ROWS <= 256, "TMA box height");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    unsigned char* base = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    V* slab = reinterpret_cast<V*>(base);
+    V* stage = reinterpret_cast<V*>(base + L::kSlabBytes);
+    uint16_t* cnt_sm = reinterpret_cast<uint16_t*>(base + L::kSlabBytes + TG::kStageBytes);
+
+    __shared__ __align__(8) uint64_t bars[KMAX];
+    __shared__ TileShared<M> sh;
+    __shared__ uint32_t red[W][M];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const V* in = static_cast<const V*>(a.in);
+    V* out = static_cast<V*>(a.out);
+    const uint32_t out_phase =
+        static_cast<uint32_t>(reinterpret_cast<uintptr_t>(out) / sizeof(V)) & (AU - 1u);
+    const bool tma_ok = a.use_tma != 0;
+    const uint64_t map_elems = (a.n * sizeof(V) / 128u) * kPerRow;
+    const uint32_t num_mids = a.hdr->num_mids;
+    const uint32_t G = gridDim.x;
+    const uint32_t e0 = tid * ITEMS;
+    uint32_t parity = 0;  // bit i: the phase of bars[i] that completes next
+
+    // A segment's element range and its tiles from the 128-byte row of a0 (at
+    // most mid_tiles <= KMAX by the planner's classification).
+    struct Seg {
+        uint64_t a0, a1, rb;
+        uint32_t s, ntiles;
+    };
+    auto make_seg = [&](uint32_t s, uint64_t a0, uint64_t a1) {
+        Seg g;
+        g.s = s;
+        g.a0 = a0;
+        g.a1 = a1;
+        g.rb = a0 & ~static_cast<uint64_t>(kPerRow - 1u);
+        g.ntiles = static_cast<uint32_t>(
+            min((a1 - g.rb + P - 1u) / P, static_cast<uint64_t>(KMAX)));
+        return g;
+    };
+    // a tile comes by TMA when the segment's part of it lies inside the
+    // tensor map (the input's whole 128-byte rows; rows past the map read as
+    // zeros and lie outside the segment)
+    auto via_tma = [&](const Seg& g, uint32_t i) {
+        return tma_ok && min(g.a1, g.rb + static_cast<uint64_t>(i + 1) * P) <= map_elems;
+    };
+    auto issue = [&](const Seg& g, uint32_t i) {  // tile i of g into slab slot i
+        if (via_tma(g, i)) {
+            mbar_arrive_expect_tx(&bars[i], P * sizeof(V));
+            tma_load_2d(slab + static_cast<size_t>(i) * P, &tmap, 0,
+                        static_cast<int32_t>(g.rb / kPerRow + static_cast<uint64_t>(i) * ROWS),
+                        &bars[i]);
+        } else {
+            mbar_arrive(&bars[i]);
+        }
+    };
+    auto range = [&](const Seg& g, uint32_t i, uint32_t& lo, uint32_t& hi) {
+        const uint64_t ts = g.rb + static_cast<uint64_t>(i) * P;
+        lo = static_cast<uint32_t>(max(g.a0, ts) - ts);
+        hi = static_cast<uint32_t>(min(g.a1, ts + P) - ts);
+    };
+    auto take = [&](const Seg& g, uint32_t i, uint32_t lo, uint32_t hi, V (&v)[ITEMS]) {
+        if (via_tma(g, i)) {
+            take_swizzled<V, ITEMS>(slab + static_cast<size_t>(i) * P, v);
+        } else {
+            const uint64_t ts = g.rb + static_cast<uint64_t>(i) * P;
+#pragma unroll
+            for (int q = 0; q < ITEMS; q++)
+                v[q] = (e0 + q >= lo && e0 + q < hi) ? in[ts + e0 + q] : V();
+        }
+    };
+
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < KMAX; q++) mbar_init(&bars[q], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    uint32_t t = blockIdx.x;
+    if (t >= num_mids) return;
+    Seg cur;
+    {
+        const uint32_t s = a.mids[t];
+        cur = make_seg(s, a.offsets[s], a.offsets[s + 1]);
+    }
+    if (tid == 0)
+        for (uint32_t i = 0; i < cur.ntiles; i++) issue(cur, i);
+    // the segment after the next one: its index is loaded one iteration early
+    uint32_t s_next = t + G < num_mids ? a.mids[t + G] : 0u;
+
+    for (; t < num_mids; t += G) {
+        const bool has_next = t + G < num_mids;
+        uint64_t n0 = 0, n1 = 0;
+        if (has_next) {  // used after the count pass
+            n0 = a.offsets[s_next];
+            n1 = a.offsets[s_next + 1];
+        }
+        const uint32_t s_after = t + 2u * G < num_mids ? a.mids[t + 2u * G] : 0u;
+        const D dj = seg_discr(a, d, cur.s);
+
+        // ---- count pass: lane c of every warp keeps the warp's count of class c
+        uint32_t wt = 0;
+        bool ok = true;
+        for (uint32_t i = 0; i < cur.ntiles; i++) {
+            ok = mbar_wait_bounded(&bars[i], (parity >> i) & 1u) && ok;
+            uint32_t lo, hi;
+            range(cur, i, lo, hi);
+            const bool full = lo == 0u && hi == static_cast<uint32_t>(P);
+            V v[ITEMS];
+            take(cur, i, lo, hi, v);
+            NibbleCounts<M> nc;
+            nc.init();
+            uint32_t last_c = M;  // element 15 stays out of the nibbles (a nibble holds 15)
+#pragma unroll
+            for (int j = 0; j < ITEMS; j++) {
+                if (full || (e0 + j >= lo && e0 + j < hi)) {
+                    const uint32_t c = dj(v[j]);
+                    if (j < 15) nc.inc(c); else last_c = c;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < M; c++) {
+                const uint32_t x = __reduce_add_sync(
+                    0xffffffffu, nc.get(c) + (last_c == static_cast<uint32_t>(c) ? 1u : 0u));
+                if (lane == c) wt += x;
+            }
+        }
+        if (lane < M) red[warp][lane] = wt;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(&a.hdr->error, kErrTimeout);
+                for (uint32_t i = 0; i < cur.ntiles; i++)  // copies still in flight
+                    (void)mbar_wait_bounded(&bars[i], (parity >> i) & 1u);
+            }
+            break;
+        }
+        parity ^= cur.ntiles >= 32u ? 0xffffffffu : ((1u << cur.ntiles) - 1u);
+        Seg nxt{};
+        if (has_next) nxt = make_seg(s_next, n0, n1);
+
+        // ---- the segment's class totals: sizes, head flags, cursors
+        if (warp == 0) {
+            uint32_t tot = 0;
+            if (lane < M) {
+#pragma unroll
+                for (int w = 0; w < W; w++) tot += red[w][lane];
+            }
+            const uint32_t excl = warp_incl_scan(tot) - tot;
+            if (lane < M) {
+                sh.cursor[0][lane] = static_cast<uint32_t>(cur.a0) + excl;
+                if (a.seg_sizes != nullptr && static_cast<uint32_t>(lane) < a.m)
+                    a.seg_sizes[static_cast<uint64_t>(cur.s) * a.m + lane] = tot;
+                if (a.headflags != nullptr && tot > 0) a.headflags[cur.a0 + excl] = tot;
+            }
+            // the next segment's tiles in the slots this one leaves unused
+            if (lane == 0 && has_next)
+                for (uint32_t i = cur.ntiles; i < nxt.ntiles; i++) issue(nxt, i);
+        }
+        __syncthreads();
+
+        // ---- scatter pass from the slab; slot i takes the next segment's tile
+        // i once this segment's tile i is in registers
+        for (uint32_t i = 0; i < cur.ntiles; i++) {
+            uint32_t lo, hi;
+            range(cur, i, lo, hi);
+            const bool full = lo == 0u && hi == static_cast<uint32_t>(P);
+            V v[ITEMS];
+            take(cur, i, lo, hi, v);
+            (void)tile_scatter<V, D, M, THREADS, true>(
+                dj, v, lo, hi, full, stage, cnt_sm, sh, i & 1u, OutFlat<V>{out, out_phase}, true,
+                [&] {
+                    if (tid == 0 && has_next && i < nxt.ntiles) issue(nxt, i);
+                });
+        }
+        cur = nxt;
+        s_next = s_after;
     }
     if (tid < M) bulk_wait_all();
 }

@@ -161,6 +161,56 @@ def test_mixed_large_and_small(cuda_ready):
         check(cuda_ready, x, offs, m, kind)
 
 
+def _medium_lengths(P, seed):
+    """Segments around the medium-segment bounds (more than one tile, at most
+    mid_tiles row-aligned tiles), at varied 128-byte-row phases (the small
+    segments between them shift each start), ending with a medium segment
+    whose last elements lie past the input's last whole 128-byte row."""
+    rng = np.random.default_rng(seed)
+    edges = [P + 1, P + 40, 2 * P - 64, 2 * P - 33, 2 * P - 32, 2 * P - 1, 2 * P, 2 * P + 1,
+             3 * P - 5, 4 * P + 1, 9 * P]
+    lengths = []
+    for _ in range(3):
+        for L in edges:
+            lengths.append(int(L))
+            lengths.append(int(rng.integers(1, 40)))
+    row = P // 128  # elements per 128-byte row
+    a0 = sum(lengths)
+    lengths.append(2 * P - a0 % row - row + 7)  # two tiles; the input ends 7 elements into a row
+    return lengths
+
+
+@pytest.mark.parametrize("rec", [False, True])
+@pytest.mark.parametrize("mid_tiles", [1, 2])
+def test_medium_segments(cuda_ready, mid_tiles, rec):
+    """Medium segments are read once by seg_mid (both tiles in shared memory,
+    count pass, then the tile scatter); mid_tiles = 1 sends them through
+    the run kernels instead.  Both must give the oracle's result."""
+    import mdiscriminator_b200 as mdx
+    torch = cuda_ready
+    P = P_U32 // 2 if rec else P_U32
+    elem = mdx.ELEM_REC8 if rec else mdx.ELEM_U32
+    lengths = _medium_lengths(P, 70 + mid_tiles)
+    offs = offsets_from_lengths(lengths)
+    n = int(offs[-1])
+    assert n % (P // 128) == 7
+    x = oracle.fill_uniform_u32(n, 71 + mid_tiles)
+    if rec:
+        x = x.astype(np.uint64) | (np.arange(n, dtype=np.uint64) << np.uint64(32))
+    saved = {m: mdx.get_tuning(elem, m, n) for m in (3, 16)}
+    try:
+        for m, kind in ((3, "mod"), (16, "mask")):
+            t = dict(saved[m])
+            t["mid_tiles"] = mid_tiles
+            mdx.set_tuning(elem, m, 0, 33, **t)
+            assert mdx.get_tuning(elem, m, n)["mid_tiles"] == mid_tiles
+            check(torch, x, offs, m, kind)
+    finally:
+        for m, t in saved.items():
+            mdx.set_tuning(elem, m, 0, 33, **t)
+        mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
+
+
 @pytest.mark.parametrize("m", [2, 4, 16])
 def test_records(cuda_ready, m):
     lengths = lognormal_lengths(800, 30 + m, mu=np.log(700))

@@ -19,7 +19,7 @@ def test_tuning_table_roundtrip_and_validation():
                    plain_ctas_per_sm=2)
     t = mdx.get_tuning(mdx.ELEM_U32, 7, 3000)  # m=7 -> class bound 8, log2 3000 -> 12
     assert t == {"plain_ctas_per_sm": 2, "run_tiles": 4, "group_batch": 16, "plain_two_kernel": 1,
-                 "pool_pct": 10}
+                 "pool_pct": 10, "mid_tiles": 1}
     assert mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20) == other_bucket   # other bucket untouched
     assert mdx.get_tuning(mdx.ELEM_REC8, 7, 3000) == other_layout     # other element layout
     with pytest.raises(mdx.MdxError):
@@ -30,6 +30,8 @@ def test_tuning_table_roundtrip_and_validation():
         mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, run_tiles=1000)
     with pytest.raises(mdx.MdxError):
         mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, plain_two_kernel=2)
+    with pytest.raises(mdx.MdxError):
+        mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, mid_tiles=3)  # more than seg_mid's slab holds
     mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12)  # back to the defaults
     mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
 
@@ -46,9 +48,10 @@ def test_committed_table_is_well_formed():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("knobs", [dict(run_tiles=1, group_batch=1, plain_two_kernel=1, plain_ctas_per_sm=1),
+@pytest.mark.parametrize("knobs", [dict(run_tiles=1, group_batch=1, plain_two_kernel=1, plain_ctas_per_sm=1,
+                                        mid_tiles=1),
                                    dict(run_tiles=16, group_batch=32, plain_two_kernel=0,
-                                        plain_ctas_per_sm=2)])
+                                        plain_ctas_per_sm=2, mid_tiles=2)])
 def test_results_do_not_depend_on_knobs(cuda_ready, knobs):
     torch = cuda_ready
     rng = np.random.default_rng(4)
