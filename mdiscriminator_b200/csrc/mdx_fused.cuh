@@ -535,6 +535,8 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
 #pragma unroll
                 for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
             }
+            // m = 2 keeps the nibble step here: tile_filter measured 1 % slower
+            // in this kernel (N = 2^28 u32: 0.544 against 0.538 ms per call)
             done = tile_scatter<V, D, M, THREADS, false>(d, v, 0u, valid, full, stage, cnt_sm, sh, tp,
                                                          out, ok, refill);
         } else {

@@ -491,8 +491,13 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
 #pragma unroll
                 for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
             }
-            done = tile_scatter<V, D, M, THREADS, false>(d, v, 0u, valid, full, stage, cnt_sm, sh,
+            if constexpr (M == 2)
+                done = tile_filter<V, D, THREADS, false>(d, v, 0u, valid, full, stage,
+                                                         reinterpret_cast<uint32_t*>(cnt_sm), sh,
                                                          i & 1u, out, ok, refill);
+            else
+                done = tile_scatter<V, D, M, THREADS, false>(d, v, 0u, valid, full, stage, cnt_sm,
+                                                             sh, i & 1u, out, ok, refill);
         } else {  // striped elements (warp ranks)
             const uint32_t w0 = static_cast<uint32_t>(tid >> 5) * 32u * ITEMS + (tid & 31);
             if (tma_ok && full) {
