@@ -448,6 +448,11 @@ def configs_measurement(torch, mdx, dev, peak, reps=10, warmup=3):
     entry("c2b", d, 8, "N=2^28 int32, class ~ Zipf(1.1) over 8 classes, v = 8*U[0,2^28) + class, "
                        "m=8 (v & 7)")
     del d
+    d = make_input(torch, 1 << 28, W.SEEDS["c2a"], dev)
+    for m in (2, 16, 32, 64):
+        entry(f"c2a_m{m}", d, m, f"N=2^28 int32 uniform [0,2^31) (the headline input), m={m} "
+                                 f"(v & {m - 1})")
+    del d
     for presorted in (False, True):
         for m in (2, 4, 16, 32, 64):
             d = W.records_torch(torch, 1 << 27, W.SEEDS["c3"], m, presorted, dev)
@@ -700,11 +705,11 @@ def main():
         mdx.partition(d_in, discr, out=d_out, sizes=sizes, ws=ws)
     barrier()
 
-    # timed region: K partitions, events on the launching stream
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for _, mid, _ in ev:  # torch creates the CUDA event on its first record
-        mid.record(stream)
+    # timed region: K partitions on the path the tuning table picks for this
+    # size (one cooperative kernel, or count + scatter with programmatic
+    # dependent launch), events on the launching stream
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
     clocks = ClockSampler(local)
     clocks.start()
     barrier()
@@ -713,8 +718,8 @@ def main():
     t_start.record(stream)
     for i in range(args.steps):
         ev[i][0].record(stream)
-        mdx.partition(d_in, discr, out=d_out, sizes=sizes, ws=ws, count_done_event=ev[i][1])
-        ev[i][2].record(stream)
+        mdx.partition(d_in, discr, out=d_out, sizes=sizes, ws=ws)
+        ev[i][1].record(stream)
     t_end.record(stream)
     barrier()
     clk = clocks.stop()
@@ -727,10 +732,22 @@ def main():
     if err != mdx.MDX_OK:
         raise SystemExit(f"device error during the timed region: {mdx.strerror(err)}")
     step_s = total_s / args.steps
-    count_ms = [a.elapsed_time(b) for a, b, _ in ev]
-    scat_ms = [b.elapsed_time(c) for _, b, c in ev]
-    call_ms = [a.elapsed_time(c) for a, _, c in ev]
+    call_ms = [a.elapsed_time(b) for a, b in ev]
     value = world * n / step_s / 1e9
+    # the two kernels apart (after the timed region): count and scatter as two
+    # launches with an event between them (no dependent launch across it)
+    kev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(10)]
+    for _, mid, _ in kev:  # torch creates the CUDA event on its first record
+        mid.record(stream)
+    barrier()
+    for a0, mid, a1 in kev:
+        a0.record(stream)
+        mdx.partition(d_in, discr, out=d_out, sizes=sizes, ws=ws, count_done_event=mid)
+        a1.record(stream)
+    barrier()
+    count_ms = [a.elapsed_time(b) for a, b, _ in kev[2:]]
+    scat_ms = [b.elapsed_time(c) for _, b, c in kev[2:]]
+    split_call_ms = [a.elapsed_time(c) for a, _, c in kev[2:]]
 
     # end to end through the public API: every step copies its input from
     # pinned host memory, partitions it and copies the result and the sizes
@@ -814,7 +831,10 @@ def main():
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
             "peak_source": peak_src,
-            "what": "one partition call (count + scatter kernels) against 2*N*4 + 4*m bytes",
+            "what": "one partition call on the tuned path against 2*N*4 + 4*m bytes",
+            "path": ("count + scatter kernels, dependent launch"
+                     if mdx.get_tuning(mdx.ELEM_U32, m, n)["plain_two_kernel"]
+                     else "one cooperative kernel"),
             "frac_of_two_pass_bound": (3 * n * 4 + 4 * m) / call_s / 1e9 / peak,
             "kernels": {
                 "count": {"ms": cnt_s * 1e3, "alg_bytes": n * 4,
@@ -825,6 +845,9 @@ def main():
                             "achieved_gbs": 2 * n * 4 / sct_s / 1e9,
                             "frac": 2 * n * 4 / sct_s / 1e9 / peak,
                             "traffic": tr.get("scatter_kernel_bytes")},
+                "split_call_ms": statistics.mean(split_call_ms),
+                "note": "kernels timed apart: 8 calls as two launches with an event "
+                        "between count and scatter, after the timed region",
             },
         }
         configs = None

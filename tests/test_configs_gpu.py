@@ -9,6 +9,7 @@ sizes:
 
 * N = 2^20 u32, m = 4 (class = v mod 4)
 * N = 2^28 u32, m = 8, uniform and Zipf(1.1)-skewed classes
+* the uniform N = 2^28 u32 input at m in {2, 16, 32, 64}
 * N = 2^27 8-byte records {key, payload = index}, class = key & (m - 1),
   m in {2, 4, 16, 32, 64}, random keys and keys pre-sorted by class.
 """
@@ -79,6 +80,22 @@ def test_c2_n2p28_m8_bench_input(cuda_ready, dist):
     _compare(res[0].view(np.uint32), exp[0], "permutation")
     if hf:
         _compare(res[2], exp[2], "head flags")
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("m", [2, 16, 32, 64])
+def test_c2a_other_class_counts(cuda_ready, m):
+    """The headline input (N = 2^28 u32, the bench's seed) at the other class
+    counts the bench times, against the oracle."""
+    torch = cuda_ready
+    from mdiscriminator_b200 import workloads as W
+    d = W.uniform_u32_torch(torch, 1 << 28, W.SEEDS["c2a"], "cuda")
+    x = d.cpu().numpy().view(np.uint32)
+    go, gs = _gpu_partition(torch, d, m, "mask")
+    del d
+    eo, es = oracle.partition(x, m, kind=oracle.DISCR_MASK)
+    _compare(gs, es, "sizes")
+    _compare(go.view(np.uint32), eo, "permutation")
     torch.cuda.empty_cache()
 
 
