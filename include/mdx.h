@@ -383,6 +383,9 @@ typedef struct {
                                     once, counted and scattered from shared memory; 0 (default) and
                                     1: none, every segment longer than a tile goes through count +
                                     scatter runs */
+    uint32_t tile_bytes;         /* plain path: bytes of a tile per thread, 64 (default, 0) or 32
+                                    (tiles half as long: more CTAs busy on short inputs; count +
+                                    scatter as two kernels; 4- and 8-byte elements) */
 } mdx_tuning;
 
 mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,

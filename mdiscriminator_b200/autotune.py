@@ -6,8 +6,9 @@ smallest power of two >= m) and a range of ceil(log2 n).  Knobs:
 
 * plain path: count and scatter as two kernels against one cooperative
   kernel (`plain_two_kernel`), CTAs per SM of the chunk grid
-  (`plain_ctas_per_sm`) and, for the one-kernel path, the share of every chunk
-  drained by ticket (`pool_pct`);
+  (`plain_ctas_per_sm`), the tile geometry (`tile_bytes`: 64 or 32 bytes of
+  a tile per thread, 256 threads; two-kernel path) and, for the one-kernel
+  path, the share of every chunk drained by ticket (`pool_pct`);
 * segmented path: tiles per run of a large segment (`run_tiles`),
   small-segment groups per work item (`group_batch`) and whether segments of
   two tiles are read once by the medium-segment kernel (`mid_tiles`).
@@ -39,9 +40,10 @@ import mdiscriminator_b200 as mdx  # noqa: E402
 # installed for); 8-byte records are timed at half the count (same bytes)
 BUCKETS = [(1 << 20, (0, 21)), (1 << 24, (22, 25)), (1 << 28, (26, 33))]
 
-# plain-path candidates: (plain_two_kernel, plain_ctas_per_sm, pool_pct)
-PLAIN_CANDIDATES = [(1, 4, 0), (1, 3, 0), (1, 0, 0),
-                    (0, 4, 100), (0, 4, 10), (0, 4, 20), (0, 4, 33), (0, 3, 10)]
+# plain-path candidates: (plain_two_kernel, plain_ctas_per_sm, pool_pct, tile_bytes)
+PLAIN_CANDIDATES = [(1, 4, 0, 64), (1, 3, 0, 64), (1, 0, 0, 64), (1, 4, 0, 32), (1, 0, 0, 32),
+                    (0, 4, 100, 64), (0, 4, 10, 64), (0, 4, 20, 64), (0, 4, 33, 64),
+                    (0, 3, 10, 64)]
 
 
 def timeit(fn, torch, reps=20, warm=3):
@@ -94,20 +96,20 @@ def main(argv=None):
             for M in bounds:
                 sizes = torch.empty(M, dtype=torch.uint32, device=dev)
                 best = None
-                for two, k, pool in PLAIN_CANDIDATES:
+                for two, k, pool, tb in PLAIN_CANDIDATES:
                     mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=k, plain_two_kernel=two,
-                                   pool_pct=pool)
+                                   pool_pct=pool, tile_bytes=tb)
                     ms = timeit(lambda: mdx.partition(d, ("mask", M), out=out, sizes=sizes, ws=ws),
                                 torch)
                     if ws.error() != mdx.MDX_OK:
                         raise SystemExit(f"device error while tuning {ename} m={M}")
                     if best is None or ms < best[0]:
-                        best = (ms, k, two, pool)
+                        best = (ms, k, two, pool, tb)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "plain",
                                 "plain_ctas_per_sm": best[1], "plain_two_kernel": best[2],
-                                "pool_pct": best[3], "ms": best[0]})
+                                "pool_pct": best[3], "tile_bytes": best[4], "ms": best[0]})
                 mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=best[1],
-                               plain_two_kernel=best[2], pool_pct=best[3])
+                               plain_two_kernel=best[2], pool_pct=best[3], tile_bytes=best[4])
             del d, out, ws
         seg_bounds = [2, 4, 8, 16]
         for n4, (lo, hi) in buckets:
@@ -128,26 +130,26 @@ def main(argv=None):
                           if e["elem"] == ename and e["m"] == M and e["path"] == "plain"
                           and e["log2_n"] == [lo, hi])
                 plain_k, plain_two, pool = pe["plain_ctas_per_sm"], pe["plain_two_kernel"], pe["pool_pct"]
+                tb = pe["tile_bytes"]
                 best = None
                 # (run_tiles, group_batch) without medium segments, then the
                 # winner with the medium-segment kernel on
-                for rt, gb, mid in [(rt, gb, 1) for rt, gb in cands] + [None]:
-                    if mid is None:
-                        rt, gb, mid = best[1], best[2], 2
+                for cand in [(rt, gb, 1) for rt, gb in cands] + [None]:
+                    rt, gb, mid = cand if cand is not None else (best[1], best[2], 2)
                     mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
-                                   plain_two_kernel=plain_two, pool_pct=pool, run_tiles=rt,
-                                   group_batch=gb, mid_tiles=mid)
+                                   plain_two_kernel=plain_two, pool_pct=pool, tile_bytes=tb,
+                                   run_tiles=rt, group_batch=gb, mid_tiles=mid)
                     ms = timeit(lambda: mdx.partition_segmented(d, do, ("mask", M), out=out,
                                                                 seg_sizes=ss, ws=ws), torch)
                     if best is None or ms < best[0]:
                         best = (ms, rt, gb, mid)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "segmented",
                                 "plain_ctas_per_sm": plain_k, "plain_two_kernel": plain_two,
-                                "pool_pct": pool, "run_tiles": best[1], "group_batch": best[2],
-                                "mid_tiles": best[3], "ms": best[0]})
+                                "pool_pct": pool, "tile_bytes": tb, "run_tiles": best[1],
+                                "group_batch": best[2], "mid_tiles": best[3], "ms": best[0]})
                 mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
-                               plain_two_kernel=plain_two, pool_pct=pool, run_tiles=best[1],
-                               group_batch=best[2], mid_tiles=best[3])
+                               plain_two_kernel=plain_two, pool_pct=pool, tile_bytes=tb,
+                               run_tiles=best[1], group_batch=best[2], mid_tiles=best[3])
             del d, out, ws
     # one entry per key: the segmented entry (it carries the plain knob too)
     merged = {}

@@ -217,6 +217,7 @@ struct Tuning {
     uint32_t plain_two_kernel = 0;  // 1: count and scatter as two kernels
     uint32_t pool_pct = 0;          // one-kernel path: % of every chunk drained by ticket (0: default)
     uint32_t mid_tiles = 0;         // segmented: medium segments up to this many tiles (0, 1: none)
+    uint32_t tile_bytes = 0;        // plain path: tile bytes per thread (0, 64: 64; 32: 32)
 };
 struct TuningTable {
     std::mutex mu;
@@ -269,20 +270,25 @@ constexpr uint32_t kFusedPoolPct = 10;  // share of every chunk drained by ticke
 static_assert(kFusedBarOffset >= kDistSkipOffset + 4 && kFusedBarOffset + 16 <= kHeaderBytes,
               "barrier words inside the header");
 
-template <class V, class D, int M>
-mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
-                     uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
-                     cudaStream_t stream, cudaEvent_t ev_mid, PlainStep step = PlainStep::kBoth,
-                     const DistOut* dist = nullptr, bool allow_fused = true) {
-    constexpr int ITEMS = ElemCfg<V>::kItems;
+// BPT: bytes of a tile per thread (64: the tiles of every path; 32: tiles
+// half as long, two-kernel path only, for the sizes where the tuning table
+// picks them).
+template <class V, class D, int M, int BPT>
+mdx_status run_plain_g(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
+                       uint32_t* d_sizes, uint32_t* d_headflags, unsigned char* ws,
+                       const PlainLayout& L, cudaStream_t stream, cudaEvent_t ev_mid,
+                       PlainStep step, const DistOut* dist, bool allow_fused) {
+    constexpr int ITEMS = BPT / static_cast<int>(sizeof(V));
     constexpr int TILE = kThreads * ITEMS;
+    static_assert(BPT != 64 || ITEMS == ElemCfg<V>::kItems, "64-byte tiles");
     auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
     const void* scatter_fn;
     size_t smem;
     {
-        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
+        using SL = ScatterTmaSmem<V, kThreads, kStages, M, BPT>;
         static_assert(SL::kTile == TILE, "both kernels use the same tiles");
-        scatter_fn = reinterpret_cast<const void*>(plain_scatter_tma_kernel<V, D, M, kThreads, kStages>);
+        scatter_fn = reinterpret_cast<const void*>(
+            plain_scatter_tma_kernel<V, D, M, kThreads, kStages, OutFlat<V>, BPT>);
         smem = SL::kBytes;
     }
     int blocks = 0, sms = 0;
@@ -328,63 +334,65 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
         return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     }
-    if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr && allow_fused &&
-        tun.plain_two_kernel == 0) {
-        // one cooperative kernel: count, grid barrier, scatter (mdx_fused.cuh)
-        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
-        CUtensorMap map;
-        if (make_row_map(&map, d_in, n, sizeof(V), SL::kRows)) {
-            auto fused = plain_fused_kernel<V, D, M, kThreads, kStages>;
-            int fb = 0, fs = 0;
-            if (occupancy(reinterpret_cast<const void*>(fused), smem, &fb, &fs) != cudaSuccess)
-                return MDX_ERR_CUDA;
-            if (tun.plain_ctas_per_sm > 0 && static_cast<int>(tun.plain_ctas_per_sm) < fb)
-                fb = static_cast<int>(tun.plain_ctas_per_sm);
-            uint32_t FG = static_cast<uint32_t>(fb) * static_cast<uint32_t>(fs);
-            if (FG > nt) FG = nt;
-            if (FG > kMaxChunks) FG = kMaxChunks;
-            if (d_headflags != nullptr &&
-                cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess)
-                return MDX_ERR_CUDA;
-            FusedArgs fa;
-            fa.p = a;
-            fa.p.num_chunks = FG;
-            fa.p.use_tma = 1;
-            fa.chunk_stride = (FG + 3u) & ~3u;
-            // pool: this share of every chunk's tiles is drained by ticket
-            const uint32_t min_len = nt / FG;
-            const uint32_t pct = tun.pool_pct ? tun.pool_pct : kFusedPoolPct;
-            fa.pool = pct >= 100u ? 0u : min_len * pct / 100u;
-            if (fa.pool >= min_len) fa.pool = min_len > 0 ? min_len - 1u : 0u;
-            fa.tile_cnt = reinterpret_cast<uint32_t*>(ws + L.tile_cnt);
-            fa.tile_pre = reinterpret_cast<uint32_t*>(ws + L.tile_pre);
-            fa.ready = reinterpret_cast<uint32_t*>(ws + L.ready);
-            fa.bar_count = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset);
-            fa.bar_gen = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 4);
-            fa.cnt_ticket = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 8);
-            fa.sct_ticket = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 12);
-            fa.bar_extra = g_test_bar_extra.load();
-            const uint64_t lim = g_test_wait_ns.load();
-            fa.wait_ns = lim != 0 ? lim : kWaitLimitNs;
-            // chunk sums are added up by atomics; ready words start unset
-            if (cudaMemsetAsync(ws + L.chunk_cnt, 0, L.ready + 4 * FG - L.chunk_cnt, stream) !=
-                cudaSuccess)
-                return MDX_ERR_CUDA;
-            const OutFlat<V> o{static_cast<V*>(d_out),
-                               static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
-                                                     (16u / sizeof(V) - 1u))};
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(FG);
-            cfg.blockDim = dim3(kThreads);
-            cfg.dynamicSmemBytes = smem;
-            cfg.stream = stream;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeCooperative;
-            attr[0].val.cooperative = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            if (cudaLaunchKernelEx(&cfg, fused, fa, d, map, o) != cudaSuccess) return MDX_ERR_CUDA;
-            return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+    if constexpr (BPT == 64) {  // the one-kernel path has 64-byte tiles only
+        if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr && allow_fused &&
+            tun.plain_two_kernel == 0) {
+            // one cooperative kernel: count, grid barrier, scatter (mdx_fused.cuh)
+            using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
+            CUtensorMap map;
+            if (make_row_map(&map, d_in, n, sizeof(V), SL::kRows)) {
+                auto fused = plain_fused_kernel<V, D, M, kThreads, kStages>;
+                int fb = 0, fs = 0;
+                if (occupancy(reinterpret_cast<const void*>(fused), smem, &fb, &fs) != cudaSuccess)
+                    return MDX_ERR_CUDA;
+                if (tun.plain_ctas_per_sm > 0 && static_cast<int>(tun.plain_ctas_per_sm) < fb)
+                    fb = static_cast<int>(tun.plain_ctas_per_sm);
+                uint32_t FG = static_cast<uint32_t>(fb) * static_cast<uint32_t>(fs);
+                if (FG > nt) FG = nt;
+                if (FG > kMaxChunks) FG = kMaxChunks;
+                if (d_headflags != nullptr &&
+                    cudaMemsetAsync(d_headflags, 0, n * sizeof(uint32_t), stream) != cudaSuccess)
+                    return MDX_ERR_CUDA;
+                FusedArgs fa;
+                fa.p = a;
+                fa.p.num_chunks = FG;
+                fa.p.use_tma = 1;
+                fa.chunk_stride = (FG + 3u) & ~3u;
+                // pool: this share of every chunk's tiles is drained by ticket
+                const uint32_t min_len = nt / FG;
+                const uint32_t pct = tun.pool_pct ? tun.pool_pct : kFusedPoolPct;
+                fa.pool = pct >= 100u ? 0u : min_len * pct / 100u;
+                if (fa.pool >= min_len) fa.pool = min_len > 0 ? min_len - 1u : 0u;
+                fa.tile_cnt = reinterpret_cast<uint32_t*>(ws + L.tile_cnt);
+                fa.tile_pre = reinterpret_cast<uint32_t*>(ws + L.tile_pre);
+                fa.ready = reinterpret_cast<uint32_t*>(ws + L.ready);
+                fa.bar_count = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset);
+                fa.bar_gen = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 4);
+                fa.cnt_ticket = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 8);
+                fa.sct_ticket = reinterpret_cast<uint32_t*>(ws + kFusedBarOffset + 12);
+                fa.bar_extra = g_test_bar_extra.load();
+                const uint64_t lim = g_test_wait_ns.load();
+                fa.wait_ns = lim != 0 ? lim : kWaitLimitNs;
+                // chunk sums are added up by atomics; ready words start unset
+                if (cudaMemsetAsync(ws + L.chunk_cnt, 0, L.ready + 4 * FG - L.chunk_cnt, stream) !=
+                    cudaSuccess)
+                    return MDX_ERR_CUDA;
+                const OutFlat<V> o{static_cast<V*>(d_out),
+                                   static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
+                                                         (16u / sizeof(V) - 1u))};
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(FG);
+                cfg.blockDim = dim3(kThreads);
+                cfg.dynamicSmemBytes = smem;
+                cfg.stream = stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeCooperative;
+                attr[0].val.cooperative = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                if (cudaLaunchKernelEx(&cfg, fused, fa, d, map, o) != cudaSuccess) return MDX_ERR_CUDA;
+                return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+            }
         }
     }
     if (step != PlainStep::kScatter) {
@@ -398,14 +406,14 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
     }
     if (step == PlainStep::kCount) return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     {
-        using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
+        using SL = ScatterTmaSmem<V, kThreads, kStages, M, BPT>;
         CUtensorMap map;
         a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
         if (dist == nullptr) {
             const OutFlat<V> o{static_cast<V*>(d_out),
                                static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
                                                      (16u / sizeof(V) - 1u))};
-            auto scatter = plain_scatter_tma_kernel<V, D, M, kThreads, kStages>;
+            auto scatter = plain_scatter_tma_kernel<V, D, M, kThreads, kStages, OutFlat<V>, BPT>;
             if (step == PlainStep::kBoth && ev_mid == nullptr) {
                 // programmatic dependent launch: scheduled while the count grid
                 // drains, it starts its first tile copies before waiting for it
@@ -423,8 +431,8 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
             } else {
                 scatter<<<G, kThreads, smem, stream>>>(a, d, map, o);
             }
-        } else if constexpr (sizeof(V) == 16) {
-            return MDX_ERR_UNSUPPORTED;  // no sharded 16-byte record kernels
+        } else if constexpr (sizeof(V) == 16 || BPT != 64) {
+            return MDX_ERR_UNSUPPORTED;  // no sharded 16-byte record kernels; sharded: 64-byte tiles
         } else {
             // the sharded instantiation is a kernel of its own: give it the
             // shared-memory attribute too (the grid stays the count's G, the
@@ -449,6 +457,21 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
         }
     }
     return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
+}
+
+template <class V, class D, int M>
+mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m, uint32_t* d_sizes,
+                     uint32_t* d_headflags, unsigned char* ws, const PlainLayout& L,
+                     cudaStream_t stream, cudaEvent_t ev_mid, PlainStep step = PlainStep::kBoth,
+                     const DistOut* dist = nullptr, bool allow_fused = true) {
+    if constexpr (sizeof(V) <= 8) {
+        const Tuning tun = tuning_for(sizeof(V) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_U32, M, n);
+        if (tun.tile_bytes == 32 && dist == nullptr && step == PlainStep::kBoth)
+            return run_plain_g<V, D, M, 32>(d_in, d_out, n, d, m, d_sizes, d_headflags, ws, L,
+                                            stream, ev_mid, step, dist, allow_fused);
+    }
+    return run_plain_g<V, D, M, 64>(d_in, d_out, n, d, m, d_sizes, d_headflags, ws, L, stream,
+                                    ev_mid, step, dist, allow_fused);
 }
 
 template <class V, class D>

@@ -330,9 +330,9 @@ __global__ void __launch_bounds__(THREADS, 4) plain_count_kernel(PlainArgs a, D 
     plain_finish_scan<M, THREADS>(a, tot_sh);
 }
 
-template <class V, int THREADS, int STAGES, int M>
+template <class V, int THREADS, int STAGES, int M, int BPT = 64>
 struct ScatterTmaSmem {
-    using G = TileGeom<V, THREADS, M>;
+    using G = TileGeom<V, THREADS, M, BPT>;
     static constexpr int kItems = G::kItems;
     static constexpr int kTile = G::kTile;
     static constexpr int kRows = G::kRows;
@@ -349,12 +349,13 @@ struct ScatterTmaSmem {
 // matrix) or tile_scatter_wide (17..64 classes: warp ranks from ballots),
 // then a shared-memory stage at the destination's 16-byte phase and bulk
 // stores of every class run (mdx_tile.cuh).  OUT: one output array, or the
-// output chunks of several ranks (distributed partition).
-template <class V, class D, int M, int THREADS, int STAGES, class OUT = OutFlat<V>>
+// output chunks of several ranks (distributed partition).  BPT: bytes of a
+// tile per thread (64, or 32 for tiles half as long).
+template <class V, class D, int M, int THREADS, int STAGES, class OUT = OutFlat<V>, int BPT = 64>
 __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 64 registers
     plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap,
                              const __grid_constant__ OUT out) {
-    using L = ScatterTmaSmem<V, THREADS, STAGES, M>;
+    using L = ScatterTmaSmem<V, THREADS, STAGES, M, BPT>;
     constexpr int ITEMS = L::kItems;
     constexpr int TILE = L::kTile;
     constexpr int ROWS = L::kRows;

@@ -1,7 +1,8 @@
 // mdx_tile.cuh -- the per-tile rank / stage / write-out step shared by the
 // plain scatter kernel and the segmented scatter items (m <= 16).
 //
-// A tile is THREADS * ITEMS elements (64 contiguous bytes per thread).  For
+// A tile is THREADS * ITEMS elements (BPT = 64 or 32 contiguous bytes per
+// thread: two tile geometries, chosen per call by the tuning table).  For
 // the elements of tile-local range [lo, hi):
 //  * pass 1: each thread ranks its own consecutive elements with 4-bit
 //    counters in a register (local rank = number of its earlier elements of
@@ -69,9 +70,10 @@ __device__ __forceinline__ void unpack16_to<Rec16>(const uint4& r, Rec16* e) {
     e[0].w[0] = r.x; e[0].w[1] = r.y; e[0].w[2] = r.z; e[0].w[3] = r.w;
 }
 
-template <class V, int THREADS, int M>
+template <class V, int THREADS, int M, int BPT = 64>
 struct TileGeom {
-    static constexpr int kItems = 64 / static_cast<int>(sizeof(V));  // 64 bytes per thread
+    static_assert(BPT == 64 || BPT == 32, "64 or 32 bytes per thread");
+    static constexpr int kItems = BPT / static_cast<int>(sizeof(V));  // BPT bytes per thread
     static constexpr int kTile = THREADS * kItems;
     static constexpr int kRows = kTile * static_cast<int>(sizeof(V)) / 128;  // 128-byte rows
     static constexpr uint32_t kAU = 16 / sizeof(V);                 // elements per 16 bytes
@@ -133,17 +135,20 @@ struct OutSharded {
     }
 };
 
-// Take a thread's 64 bytes of a tile that TMA placed in shared memory with
-// the 128-byte swizzle (16-byte chunk q of 128-byte row r sits at chunk
-// q ^ (r & 7)).
+// Take a thread's ITEMS * sizeof(V) (64 or 32) bytes of a tile that TMA
+// placed in shared memory with the 128-byte swizzle (16-byte chunk q of
+// 128-byte row r sits at chunk q ^ (r & 7)).
 template <class V, int ITEMS>
 __device__ __forceinline__ void take_swizzled(const V* tile, V (&v)[ITEMS]) {
     constexpr uint32_t AU = 16 / sizeof(V);
+    constexpr uint32_t BPT = ITEMS * sizeof(V);
+    static_assert(BPT == 64 || BPT == 32, "64 or 32 bytes per thread");
+    constexpr uint32_t TPR = 128 / BPT, CPT = BPT / 16;  // threads per row, chunks per thread
     const unsigned char* tb = reinterpret_cast<const unsigned char*>(tile);
-    const uint32_t row = threadIdx.x >> 1;
+    const uint32_t row = threadIdx.x / TPR;
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const uint32_t chunk = ((threadIdx.x & 1u) * 4u + q) ^ (row & 7u);
+    for (uint32_t q = 0; q < CPT; q++) {
+        const uint32_t chunk = ((threadIdx.x % TPR) * CPT + q) ^ (row & 7u);
         const uint4 r = *reinterpret_cast<const uint4*>(tb + row * 128u + chunk * 16u);
         unpack16_to<V>(r, &v[q * AU]);
     }
@@ -155,20 +160,21 @@ __device__ __forceinline__ void take_swizzled(const V* tile, V (&v)[ITEMS]) {
 // `after_counts` runs right after the first barrier (the input ring slot is
 // consumed by then).  Returns false, having written nothing, when `ok` is
 // false on any thread.
-template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts>
-__device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeof(V)], uint32_t lo,
+template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts,
+          int ITEMS>
+__device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[ITEMS], uint32_t lo,
                                              uint32_t hi, bool full, V* stage, uint16_t* cnt_sm,
                                              TileShared<M>& sh, uint32_t par, const OUT& out,
                                              bool ok, AfterCounts after_counts) {
-    using G = TileGeom<V, THREADS, M>;
-    constexpr int ITEMS = G::kItems;
+    using G = TileGeom<V, THREADS, M, ITEMS * static_cast<int>(sizeof(V))>;
+    static_assert(G::kItems == ITEMS, "geometry");
     constexpr uint32_t AU = G::kAU;
     constexpr int W = THREADS / 32;
     constexpr int PER = THREADS / 32;
     constexpr int LR = (ITEMS + 7) / 8;
     static_assert(M <= 16 && M >= 2, "class bound");
     static_assert(M <= 2 * W, "each warp scans at most two rows");
-    static_assert(ITEMS == 16 || ITEMS == 8 || ITEMS == 4, "64 bytes of 4-, 8- or 16-byte elements");
+    static_assert(ITEMS == 16 || ITEMS == 8 || ITEMS == 4 || ITEMS == 2, "thread elements");
     static_assert(PER == 8, "row scans load 8 entries per lane");
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -337,13 +343,12 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[64 / sizeo
 // kernel 0.383 ms with either step, against 0.337 ms for a plain 1 GiB
 // device copy); the whole call at m = 2 is 1.02x the count kernel plus that
 // copy.
-template <class V, class D, int THREADS, bool FORWARD, class OUT, class AfterCounts>
-__device__ __forceinline__ bool tile_filter(const D& d, const V (&v)[64 / sizeof(V)], uint32_t lo,
+template <class V, class D, int THREADS, bool FORWARD, class OUT, class AfterCounts, int ITEMS>
+__device__ __forceinline__ bool tile_filter(const D& d, const V (&v)[ITEMS], uint32_t lo,
                                             uint32_t hi, bool full, V* stage, uint32_t* scr,
                                             TileShared<2>& sh, uint32_t par, const OUT& out, bool ok,
                                             AfterCounts after_counts) {
-    using G = TileGeom<V, THREADS, 2>;
-    constexpr int ITEMS = G::kItems;
+    using G = TileGeom<V, THREADS, 2, ITEMS * static_cast<int>(sizeof(V))>;
     constexpr uint32_t AU = G::kAU;
     constexpr int W = THREADS / 32;
     static_assert(ITEMS <= 16 && W <= 32, "16-bit packed warp counts, one lane per warp");
@@ -479,14 +484,14 @@ __device__ __forceinline__ void take_striped_swizzled(const V* tile, V (&v)[ITEM
     }
 }
 
-template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts>
-__device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[64 / sizeof(V)],
+template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts,
+          int ITEMS>
+__device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[ITEMS],
                                                   uint32_t lo, uint32_t hi, bool full, V* stage,
                                                   uint32_t* wtab, TileShared<M>& sh, uint32_t par,
                                                   const OUT& out, bool ok,
                                                   AfterCounts after_counts) {
-    using G = TileGeom<V, THREADS, M>;
-    constexpr int ITEMS = G::kItems;
+    using G = TileGeom<V, THREADS, M, ITEMS * static_cast<int>(sizeof(V))>;
     constexpr uint32_t AU = G::kAU;
     constexpr int W = THREADS / 32;
     constexpr int B = M == 32 ? 5 : 6;
