@@ -9,7 +9,8 @@
 // after their own part, at the end of each phase:
 //
 //   count phase   own part [t0 + q, t1) through the CTA's TMA ring
-//                 (cp.async.bulk.tensor, 128-byte swizzle, no multicast),
+//                 (cp.async.bulk.tensor, 128-byte swizzle -- none for more
+//                 than 16 classes -- no multicast),
 //                 counted from shared memory with 4-bit packed counters; then
 //                 pool tiles by ticket (tile idx of chunk j for ticket
 //                 idx * G + j, so concurrent tiles lie far apart), each reduced
@@ -245,7 +246,10 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
             const uint32_t valid = static_cast<uint32_t>(min(static_cast<uint64_t>(TILE), a.n - ts));
             V v[ITEMS];
             if (tma_tile) {
-                take_swizzled<V, ITEMS>(ring + slot * TILE, v);
+                // counts do not depend on the order within a tile: for more
+                // than 16 classes the tile is unswizzled and read striped
+                if constexpr (M <= 16) take_swizzled<V, ITEMS>(ring + slot * TILE, v);
+                else take_striped<V, ITEMS>(ring + slot * TILE, v);
             } else {
 #pragma unroll
                 for (int j = 0; j < ITEMS; j++) v[j] = (e0 + j < valid) ? in[ts + e0 + j] : V();
@@ -542,7 +546,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         } else {
             const uint32_t w0 = static_cast<uint32_t>(tid >> 5) * 32u * ITEMS + (tid & 31);
             if (tma_tile) {
-                take_striped_swizzled<V, ITEMS>(ring + slot * TILE, v);
+                take_striped<V, ITEMS>(ring + slot * TILE, v);
             } else {
 #pragma unroll
                 for (int j = 0; j < ITEMS; j++)

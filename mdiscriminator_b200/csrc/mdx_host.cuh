@@ -187,9 +187,13 @@ inline EncodeTiledFn tensor_map_encoder() {
 }
 
 // The n elements viewed as rows of 128 bytes (n * sizeof(V) / 128 whole rows),
-// boxes of `box_rows` rows, 128-byte swizzle.  False if TMA cannot be used
-// (unaligned base, fewer rows than one box, encoder unavailable).
-inline bool make_row_map(CUtensorMap* map, const void* base, uint64_t n, size_t elem, uint32_t box_rows) {
+// boxes of `box_rows` rows, 128-byte swizzle (thread-contiguous tile steps
+// read 16-byte chunks of every row) or none (the warp-rank step of more than
+// 16 classes reads the tile striped, one word per lane).  False if TMA
+// cannot be used (unaligned base, fewer rows than one box, encoder
+// unavailable).
+inline bool make_row_map(CUtensorMap* map, const void* base, uint64_t n, size_t elem, uint32_t box_rows,
+                         bool swizzle = true) {
     std::memset(map, 0, sizeof(*map));
     if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return false;
     const uint64_t rows = n * elem / 128;  // whole 128-byte rows
@@ -203,7 +207,8 @@ inline bool make_row_map(CUtensorMap* map, const void* base, uint64_t n, size_t 
     const cuuint32_t estr[2] = {1, 1};
     const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_UINT32;
     return enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_INTERLEAVE_NONE,
+               swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -340,7 +345,7 @@ mdx_status run_plain_g(const void* d_in, void* d_out, uint64_t n, D d, uint32_t 
             // one cooperative kernel: count, grid barrier, scatter (mdx_fused.cuh)
             using SL = ScatterTmaSmem<V, kThreads, kStages, M>;
             CUtensorMap map;
-            if (make_row_map(&map, d_in, n, sizeof(V), SL::kRows)) {
+            if (make_row_map(&map, d_in, n, sizeof(V), SL::kRows, M <= 16)) {
                 auto fused = plain_fused_kernel<V, D, M, kThreads, kStages>;
                 int fb = 0, fs = 0;
                 if (occupancy(reinterpret_cast<const void*>(fused), smem, &fb, &fs) != cudaSuccess)
@@ -408,7 +413,7 @@ mdx_status run_plain_g(const void* d_in, void* d_out, uint64_t n, D d, uint32_t 
     {
         using SL = ScatterTmaSmem<V, kThreads, kStages, M, BPT>;
         CUtensorMap map;
-        a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows) ? 1 : 0;
+        a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows, M <= 16) ? 1 : 0;
         if (dist == nullptr) {
             const OutFlat<V> o{static_cast<V*>(d_out),
                                static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &

@@ -344,7 +344,8 @@ struct ScatterTmaSmem {
 // Scatter kernel: CTA k re-reads chunk k (tiles in reverse order) and writes
 // every element at class_base[c] + chunk_pre[c][k] + its rank in the chunk.
 // Tiles arrive by tensor TMA (one 2-D box of 128-byte rows per tile, 128-byte
-// swizzle, STAGES-deep mbarrier ring) and go through tile_scatter (m <= 16:
+// swizzle for m <= 16 and none above, STAGES-deep mbarrier ring) and go
+// through tile_filter (m = 2), tile_scatter (m <= 16:
 // thread-local nibble ranks, a block scan over the [class][thread] count
 // matrix) or tile_scatter_wide (17..64 classes: warp ranks from ballots),
 // then a shared-memory stage at the destination's 16-byte phase and bulk
@@ -502,7 +503,7 @@ __global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 6
         } else {  // striped elements (warp ranks)
             const uint32_t w0 = static_cast<uint32_t>(tid >> 5) * 32u * ITEMS + (tid & 31);
             if (tma_ok && full) {
-                take_striped_swizzled<V, ITEMS>(ring + (i % STAGES) * TILE, v);
+                take_striped<V, ITEMS>(ring + (i % STAGES) * TILE, v);
             } else {
 #pragma unroll
                 for (int j = 0; j < ITEMS; j++)

@@ -457,7 +457,8 @@ __device__ __forceinline__ bool tile_filter(const D& d, const V (&v)[ITEMS], uin
 // With more than 16 classes the per-thread nibble counters no longer fit in a
 // register pair, so ranks come from the warp instead (striped layout):
 //  * in round j lane l of warp w holds tile element w*32*ITEMS + j*32 + l, so
-//    (warp, round, lane) is input order;
+//    (warp, round, lane) is input order; TMA places these tiles without
+//    swizzle, so a round is one conflict-free shared load per lane;
 //  * the lanes of a round that share a class are found from log2(M) ballots
 //    of the class bits (peers = AND over bits of ballot or ~ballot), the rank
 //    in the round is popc(peers & lanemask_lt);
@@ -465,32 +466,27 @@ __device__ __forceinline__ bool tile_filter(const D& d, const V (&v)[ITEMS], uin
 //    in a register, read by one shuffle per element and advanced by a popcount
 //    of the lanes of class k (the same AND over bits with k's own bits);
 //  * warp 0 turns the [warp][class] counts into class runs at the
-//    destination's 16-byte phase and stage bases per (warp, class); pass 2 and
-//    the write-out are those of tile_scatter.
+//    destination's 16-byte phase and stage bases per (warp, class), which pass
+//    2 reads from shared memory; the write-out is that of tile_scatter.
+// The step is bound by the ALU pipe (ncu, m = 64: 72 % of peak), so full
+// tiles take a path without the bounds tests and selects.
 
-// A warp's striped elements of a tile that TMA placed in shared memory with
-// the 128-byte swizzle.
+// A warp's striped elements of a tile that TMA placed in shared memory
+// without swizzle (element e at tile[e]).
 template <class V, int ITEMS>
-__device__ __forceinline__ void take_striped_swizzled(const V* tile, V (&v)[ITEMS]) {
-    const unsigned char* tb = reinterpret_cast<const unsigned char*>(tile);
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    constexpr uint32_t PER_ROW = 128 / sizeof(V);
+__device__ __forceinline__ void take_striped(const V* tile, V (&v)[ITEMS]) {
+    const V* p = tile + (threadIdx.x >> 5) * 32u * ITEMS + (threadIdx.x & 31u);
 #pragma unroll
-    for (int j = 0; j < ITEMS; j++) {
-        const uint32_t e = warp * 32u * ITEMS + j * 32u + lane;
-        const uint32_t row = e / PER_ROW, col = (e % PER_ROW) * sizeof(V);
-        const uint32_t chunk = (col >> 4) ^ (row & 7u);
-        v[j] = *reinterpret_cast<const V*>(tb + row * 128u + chunk * 16u + (col & 15u));
-    }
+    for (int j = 0; j < ITEMS; j++) v[j] = p[j * 32];
 }
 
-template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts,
-          int ITEMS>
-__device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[ITEMS],
-                                                  uint32_t lo, uint32_t hi, bool full, V* stage,
-                                                  uint32_t* wtab, TileShared<M>& sh, uint32_t par,
-                                                  const OUT& out, bool ok,
-                                                  AfterCounts after_counts) {
+template <class V, class D, int M, int THREADS, bool FORWARD, bool FULL, class OUT,
+          class AfterCounts, int ITEMS>
+__device__ __forceinline__ bool tile_scatter_wide_impl(const D& d, const V (&v)[ITEMS],
+                                                       uint32_t lo, uint32_t hi, V* stage,
+                                                       uint32_t* wtab, TileShared<M>& sh,
+                                                       uint32_t par, const OUT& out, bool ok,
+                                                       AfterCounts after_counts) {
     using G = TileGeom<V, THREADS, M, ITEMS * static_cast<int>(sizeof(V))>;
     constexpr uint32_t AU = G::kAU;
     constexpr int W = THREADS / 32;
@@ -500,6 +496,7 @@ __device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[ITEMS
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = lanemask_lt();
+    const uint32_t ew = static_cast<uint32_t>(warp) * 32u * ITEMS + static_cast<uint32_t>(lane);
 
     // ---- pass 1: warp ranks.  Lane k builds the mask of the lanes holding
     // class k (and k + 32): one LOP3 per class bit against its own bits; an
@@ -513,29 +510,33 @@ __device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[ITEMS
     for (int q = 0; q < ITEMS / 2; q++) rk[q] = 0;
 #pragma unroll
     for (int j = 0; j < ITEMS; j++) {
-        const uint32_t e = static_cast<uint32_t>(warp) * 32u * ITEMS + j * 32u + lane;
-        const bool valid = full || (e >= lo && e < hi);
+        bool valid = true;
+        if constexpr (!FULL) {
+            const uint32_t e = ew + j * 32u;
+            valid = e >= lo && e < hi;
+        }
         const uint32_t c = valid ? d(v[j]) : 0u;
-        uint32_t com = full ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
+        uint32_t com = FULL ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
 #pragma unroll
         for (int i = 0; i < 5; i++) com &= __ballot_sync(0xffffffffu, (c >> i) & 1u) ^ inv[i];
         uint32_t peers, base;
         const uint32_t x = __shfl_sync(0xffffffffu, runs, c & 31u);
         if constexpr (B == 6) {
             const uint32_t b5 = __ballot_sync(0xffffffffu, (c >> 5) & 1u);
-            const uint32_t com0 = com & ~b5, com1 = com & b5;
-            const uint32_t p0 = __shfl_sync(0xffffffffu, com0, c & 31u);
-            const uint32_t p1 = __shfl_sync(0xffffffffu, com1, c & 31u);
-            peers = (c >> 5) ? p1 : p0;
-            base = (c >> 5) ? (x >> 16) : (x & 0xffffu);
-            runs += static_cast<uint32_t>(__popc(com0)) | (static_cast<uint32_t>(__popc(com1)) << 16);
+            const uint32_t com1 = com & b5;
+            // lanes of class (c mod 32) with the same sixth bit as c
+            const uint32_t p = __shfl_sync(0xffffffffu, com, c & 31u);
+            peers = p & ((c & 32u) ? b5 : ~b5);
+            base = (x >> ((c & 32u) >> 1)) & 0xffffu;
+            const uint32_t n1 = static_cast<uint32_t>(__popc(com1));
+            runs += (static_cast<uint32_t>(__popc(com)) - n1) + (n1 << 16);
         } else {
             peers = __shfl_sync(0xffffffffu, com, c);
             base = x;
             runs += static_cast<uint32_t>(__popc(com));
         }
         const uint32_t r = base + __popc(peers & lt);
-        rk[j >> 1] |= (r & 0xffffu) << (16 * (j & 1));
+        rk[j >> 1] |= r << (16 * (j & 1));
     }
     wtab[warp * M + lane] = runs & 0xffffu;
     if constexpr (M == 64) wtab[warp * M + lane + 32] = runs >> 16;
@@ -578,23 +579,15 @@ __device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[ITEMS
     __syncthreads();  // (B)
 
     // ---- pass 2: stage slot = base of (warp, class) + warp rank
-    const uint32_t sb0 = wtab[warp * M + lane];
-    uint32_t sb1 = 0u;
-    if constexpr (M == 64) sb1 = wtab[warp * M + lane + 32];
+    const uint32_t* wb = wtab + warp * M;
 #pragma unroll
     for (int j = 0; j < ITEMS; j++) {
-        const uint32_t e = static_cast<uint32_t>(warp) * 32u * ITEMS + j * 32u + lane;
-        const bool valid = full || (e >= lo && e < hi);
-        const uint32_t c = valid ? d(v[j]) : 0u;
-        uint32_t sb;
-        if constexpr (M == 64) {
-            const uint32_t x0 = __shfl_sync(0xffffffffu, sb0, c & 31u);
-            const uint32_t x1 = __shfl_sync(0xffffffffu, sb1, c & 31u);
-            sb = (c >> 5) ? x1 : x0;
-        } else {
-            sb = __shfl_sync(0xffffffffu, sb0, c);
+        bool valid = true;
+        if constexpr (!FULL) {
+            const uint32_t e = ew + j * 32u;
+            valid = e >= lo && e < hi;
         }
-        if (valid) stage[sb + ((rk[j >> 1] >> (16 * (j & 1))) & 0xffffu)] = v[j];
+        if (valid) stage[wb[d(v[j])] + ((rk[j >> 1] >> (16 * (j & 1))) & 0xffffu)] = v[j];
     }
     fence_proxy_async_smem();
     __syncthreads();  // (C)
@@ -631,6 +624,20 @@ __device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[ITEMS
         if (off != 0xffffffffu) *out.at(sh.run_dst[c] + off) = stage[s + off];
     }
     return true;
+}
+
+template <class V, class D, int M, int THREADS, bool FORWARD, class OUT, class AfterCounts,
+          int ITEMS>
+__device__ __forceinline__ bool tile_scatter_wide(const D& d, const V (&v)[ITEMS],
+                                                  uint32_t lo, uint32_t hi, bool full, V* stage,
+                                                  uint32_t* wtab, TileShared<M>& sh, uint32_t par,
+                                                  const OUT& out, bool ok,
+                                                  AfterCounts after_counts) {
+    if (full)
+        return tile_scatter_wide_impl<V, D, M, THREADS, FORWARD, true>(d, v, lo, hi, stage, wtab, sh,
+                                                                     par, out, ok, after_counts);
+    return tile_scatter_wide_impl<V, D, M, THREADS, FORWARD, false>(d, v, lo, hi, stage, wtab, sh,
+                                                                  par, out, ok, after_counts);
 }
 
 }  // namespace mdx
