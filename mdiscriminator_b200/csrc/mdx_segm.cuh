@@ -593,28 +593,17 @@ __device__ void seg_group_cta(const SegArgs& a, const D& d, const uint64_t* cmod
     if (active) {
         uint32_t q = q0, nxt = gs.hpos[q0 + 1];
         D dc = d0;
-        uint32_t x = lo;
-        for (;;) {
-            // the piece [x, end) lies in segment q: no head test per element,
-            // four loads in flight
-            const uint32_t end = min(nxt, hi);
-            for (; x + 4u <= end; x += 4u) {
-                const V v0 = src[x], v1 = src[x + 1], v2 = src[x + 2], v3 = src[x + 3];
-                tail.inc(dc(v0));
-                tail.inc(dc(v1));
-                tail.inc(dc(v2));
-                tail.inc(dc(v3));
+        for (uint32_t x = lo; x < hi; x++) {
+            if (x == nxt) {
+                if (inner) close(q, tail);
+                else pre = tail;
+                inner = true;
+                tail.zero();
+                q++;
+                nxt = gs.hpos[q + 1];
+                dc = group_discr(a, d, cmod, gs.msz[q]);
             }
-            for (; x < end; x++) tail.inc(dc(src[x]));
-            if (x >= hi) break;
-            // x == nxt: segment q + 1 starts here
-            if (inner) close(q, tail);
-            else pre = tail;
-            inner = true;
-            tail.zero();
-            q++;
-            nxt = gs.hpos[q + 1];
-            dc = group_discr(a, d, cmod, gs.msz[q]);
+            tail.inc(dc(src[x]));
         }
         if (inner && hi == nxt) close(q, tail);
         if (!inner) pre = tail;
@@ -679,30 +668,20 @@ __device__ void seg_group_cta(const SegArgs& a, const D& d, const uint64_t* cmod
 #pragma unroll
         for (int w = 0; w < NW; w++) cur.w[w] = gs.base[q0][w] + carry.w[w];
         D dc = d0;
-        uint32_t x = lo;
-        auto place = [&](const V& v) {
+        for (uint32_t x = lo; x < hi; x++) {
+            if (x == nxt) {
+                q++;
+                xh = x;
+                nxt = gs.hpos[q + 1];
+#pragma unroll
+                for (int w = 0; w < NW; w++) cur.w[w] = gs.base[q][w];
+                dc = group_discr(a, d, cmod, gs.msz[q]);
+            }
+            const V v = src[x];
             const uint32_t c = dc(v);
             const uint32_t pos = xh + cur.get(c);
             cur.inc(c);
             if (pos < L) dst[pos] = v;
-        };
-        for (;;) {
-            const uint32_t end = min(nxt, hi);  // the piece of segment q
-            for (; x + 4u <= end; x += 4u) {
-                const V v0 = src[x], v1 = src[x + 1], v2 = src[x + 2], v3 = src[x + 3];
-                place(v0);
-                place(v1);
-                place(v2);
-                place(v3);
-            }
-            for (; x < end; x++) place(src[x]);
-            if (x >= hi) break;
-            q++;  // x == nxt: segment q + 1 starts here
-            xh = x;
-            nxt = gs.hpos[q + 1];
-#pragma unroll
-            for (int w = 0; w < NW; w++) cur.w[w] = gs.base[q][w];
-            dc = group_discr(a, d, cmod, gs.msz[q]);
         }
     }
 }
