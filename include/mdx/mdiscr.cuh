@@ -35,6 +35,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -74,7 +75,15 @@ inline void check(mdx_status s, const char* file, int line) {
 #endif
 }
 
-// One zero-initialised workspace per device, grown on demand.
+// Host-side fault injection for tests: the nth growth of the workspace from
+// now on fails as if cudaMalloc had run out of memory (0: off).
+inline std::atomic<int>& workspace_fail_countdown() {
+    static std::atomic<int> c{0};
+    return c;
+}
+
+// One zero-initialised workspace per device, grown on demand.  A failed
+// growth leaves none, so the next call tries again.
 inline unsigned char* workspace(size_t need) {
     static std::mutex mu;
     static void* ptr[64] = {};
@@ -86,6 +95,8 @@ inline unsigned char* workspace(size_t need) {
         if (ptr[dev] != nullptr) cudaFree(ptr[dev]);  // waits for work still using it
         ptr[dev] = nullptr;
         bytes[dev] = 0;
+        const int fc = workspace_fail_countdown().load();
+        if (fc > 0 && workspace_fail_countdown().fetch_sub(1) == 1) return nullptr;
         if (cudaMalloc(&ptr[dev], need) != cudaSuccess) return nullptr;
         if (cudaMemset(ptr[dev], 0, need) != cudaSuccess) return nullptr;
         bytes[dev] = need;
@@ -203,6 +214,12 @@ TupleT order_rows(uint64_t n, unsigned char* ws, const RowsLayout& R) {
 }
 
 }  // namespace detail
+
+// Test hook (no reference counterpart; host side, no GPU fault): the nth
+// growth of the per-device workspace from now on fails as if device memory
+// were exhausted, so the call reports MDX_ERR_CUDA (exit, or
+// std::runtime_error under MDX_NO_EXIT); 0 turns it off.
+inline void test_inject_workspace_failure(int nth) { detail::workspace_fail_countdown().store(nth); }
 
 template <class DISCR>
 typename DISCR::TupleType mdiscr(const unsigned int num_elems, const unsigned int num_hwd_thds,

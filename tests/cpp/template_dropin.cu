@@ -3,10 +3,14 @@
 // include/mdx/mdiscr.cuh instead.  Functors follow the reference's concept:
 // InType, TupleType {cardinal, operator[]}, padelm, static apply on the device.
 // Each case is checked against a plain CPU stable partition.  Prints one line
-// per case and exits non-zero on the first mismatch.
+// per case and exits non-zero on the first mismatch.  Built with MDX_NO_EXIT,
+// so a failing call throws instead of exiting: the first case injects a
+// workspace allocation failure (host side) and expects exactly that.
+#define MDX_NO_EXIT 1
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <vector>
 
 #include "mdx/mdiscr.cuh"
@@ -257,8 +261,38 @@ static int tuple_case(const char* name, unsigned n) {
     return ok ? 0 : 1;
 }
 
+// The first call of the program grows the (empty) workspace; with the
+// growth made to fail it must report the failure (std::runtime_error under
+// MDX_NO_EXIT) and leave nothing behind, and the next call must succeed.
+static int alloc_failure_case() {
+    const unsigned n = 100000;
+    std::vector<unsigned> h(n);
+    for (unsigned i = 0; i < n; i++) h[i] = i * 2654435761u;
+    unsigned *d = nullptr, *o = nullptr;
+    cudaMalloc(&d, n * 4);
+    cudaMalloc(&o, n * 4);
+    cudaMemcpy(d, h.data(), n * 4, cudaMemcpyHostToDevice);
+    mdx::test_inject_workspace_failure(1);
+    bool threw = false;
+    try {
+        (void)mdiscr<LowBits8>(n, 1024, d, o);
+    } catch (const std::runtime_error&) {
+        threw = true;
+    }
+    mdx::test_inject_workspace_failure(0);
+    Counts<8> sz = mdiscr<LowBits8>(n, 1024, d, o);  // the workspace grows now
+    unsigned total = 0;
+    for (unsigned c = 0; c < 8; c++) total += sz[c];
+    cudaFree(d);
+    cudaFree(o);
+    const bool ok = threw && total == n;
+    std::printf("workspace allocation failure: %s\n", ok ? "REPORTED" : "NOT REPORTED");
+    return ok ? 0 : 1;
+}
+
 int main() {
     int bad = 0;
+    bad |= alloc_failure_case();
     bad |= plain_case<LowBits8>("mdiscr<LowBits8>", 1u << 20);
     bad |= plain_case<Remainder<5>>("mdiscr<Remainder<5>>", 3000017u);
     bad |= plain_case<Remainder<40>>("mdiscr<Remainder<40>>", 777777u);
