@@ -29,12 +29,16 @@ def test_grid_barrier_wait_runs_out_and_is_reported(cuda_ready):
     ws = mdx.new_workspace(mdx.workspace_size(n, mdx.ELEM_U32, m))
     out = torch.full((n,), -1, dtype=torch.int32, device="cuda")
     sizes = torch.empty(m, dtype=torch.uint32, device="cuda")
+    # the one-kernel path whatever the tuning table picks for this size
+    mdx.set_tuning(mdx.ELEM_U32, m, 0, 33, plain_two_kernel=0)
     L.mdx_test_set_barrier_shortfall(1, 20_000_000)
     try:
         mdx.partition(d, ("mod", m), out=out, sizes=sizes, ws=ws)
         torch.cuda.synchronize()
     finally:
         L.mdx_test_set_barrier_shortfall(0, 0)
+        mdx.set_tuning(mdx.ELEM_U32, m, 0, 33)
+        mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
     assert ws.error() == mdx.MDX_ERR_TIMEOUT
     assert bool((out == -1).all())  # no CTA scattered from an incomplete count
     mdx._check(L.mdx_workspace_init(ctypes.c_void_p(ws.ptr), ws.nbytes, None), "mdx_workspace_init")

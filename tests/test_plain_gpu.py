@@ -209,24 +209,33 @@ def test_single_class_is_a_copy(cuda_ready):
 
 @pytest.mark.parametrize("m", [2, 5, 8, 16, 32, 64])
 def test_one_kernel_and_two_kernel_paths_agree_with_oracle(cuda_ready, m):
-    """The plain call runs as one cooperative kernel (count, grid barrier,
-    scatter) unless an event is recorded between counting and scattering,
-    which selects the two-kernel path: both against the oracle, for values and
-    records, at sizes with one tile per CTA, many tiles per CTA and a ragged
-    last tile."""
+    """The three launch forms of the plain call against the oracle: one
+    cooperative kernel (count, grid barrier, scatter), count + scatter with
+    programmatic dependent launch, and count + scatter with an event recorded
+    between them; for values and records, at sizes with one tile per CTA,
+    many tiles per CTA and a ragged last tile."""
     import mdiscriminator_b200 as mdx
     torch = cuda_ready
-    for n in (4096, 300_001, 5 << 20, (1 << 24) + 13):
-        for rec in (False, True):
-            x = records(n, n + m) if rec else oracle.fill_uniform_u32(n, n + m)
-            d = torch.from_numpy(x).cuda()
-            eo, es, ef = oracle.partition(x, m, kind=oracle.DISCR_MOD, headflags=True)
-            for two_kernel in (False, True):
-                ev = torch.cuda.Event() if two_kernel else None
-                out, sizes, hf = mdx.partition(d, ("mod", m), headflags=True, count_done_event=ev)
-                torch.cuda.synchronize()
-                what = f"n={n} m={m} rec={rec} two_kernel={two_kernel}"
-                assert np.array_equal(sizes.cpu().numpy(), es), what
-                assert np.array_equal(out.cpu().numpy(), eo), what
-                assert np.array_equal(hf.cpu().numpy(), ef), what
-    assert mdx.workspace(0).error() == mdx.MDX_OK
+    forms = [("one_kernel", 0, False), ("dependent_launch", 1, False), ("event", 1, True)]
+    try:
+        for n in (4096, 300_001, 5 << 20, (1 << 24) + 13):
+            for rec in (False, True):
+                x = records(n, n + m) if rec else oracle.fill_uniform_u32(n, n + m)
+                d = torch.from_numpy(x).cuda()
+                eo, es, ef = oracle.partition(x, m, kind=oracle.DISCR_MOD, headflags=True)
+                for form, two, with_event in forms:
+                    mdx.set_tuning(mdx.ELEM_REC8 if rec else mdx.ELEM_U32, m, 0, 33,
+                                   plain_two_kernel=two)
+                    ev = torch.cuda.Event() if with_event else None
+                    out, sizes, hf = mdx.partition(d, ("mod", m), headflags=True,
+                                                   count_done_event=ev)
+                    torch.cuda.synchronize()
+                    what = f"n={n} m={m} rec={rec} form={form}"
+                    assert np.array_equal(sizes.cpu().numpy(), es), what
+                    assert np.array_equal(out.cpu().numpy(), eo), what
+                    assert np.array_equal(hf.cpu().numpy(), ef), what
+        assert mdx.workspace(0).error() == mdx.MDX_OK
+    finally:
+        for elem in (mdx.ELEM_U32, mdx.ELEM_REC8):
+            mdx.set_tuning(elem, m, 0, 33)
+        mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
