@@ -639,7 +639,7 @@ def main():
     ap.add_argument("--impl", default="mdx", choices=["mdx", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--m", type=int, default=M_DEFAULT)
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other plain configurations")
@@ -751,8 +751,10 @@ def main():
 
     # end to end through the public API: every step copies its input from
     # pinned host memory, partitions it and copies the result and the sizes
-    # back.  Two buffer sets on two streams, so one step's device-to-host
-    # copy overlaps the next step's host-to-device copy (PCIe is full duplex).
+    # back.  Three streams (host-to-device copies, partitions, device-to-host
+    # copies) and two buffer sets, ordered by events, so that in steady state
+    # one step's input and an earlier step's result cross PCIe at the same
+    # time in the two directions while the partition runs in between.
     e2e_sets = []
     for k in range(2):
         h_in = torch.empty(n, dtype=torch.int32, pin_memory=True)
@@ -763,16 +765,28 @@ def main():
             "d_in": torch.empty_like(d_in), "d_out": torch.empty_like(d_in),
             "sizes": torch.empty(m, dtype=torch.uint32, device=dev),
             "ws": mdx.new_workspace(mdx.workspace_size(n, mdx.ELEM_U32, m), dev),
-            "stream": torch.cuda.Stream(device=dev)})
+            "in_ready": torch.cuda.Event(), "part_done": torch.cuda.Event(),
+            "out_done": torch.cuda.Event()})
+    s_h2d, s_cmp, s_d2h = (torch.cuda.Stream(device=dev) for _ in range(3))
 
     def e2e_step(i):
         b = e2e_sets[i % 2]
-        with torch.cuda.stream(b["stream"]):
+        if i >= 2:  # d_in of this set is free once step i - 2's partition read it
+            s_h2d.wait_event(b["part_done"])
+        with torch.cuda.stream(s_h2d):
             b["d_in"].copy_(b["h_in"], non_blocking=True)
-            mdx.partition(b["d_in"], discr, out=b["d_out"], sizes=b["sizes"], ws=b["ws"],
-                          stream=b["stream"])
+            b["in_ready"].record(s_h2d)
+        s_cmp.wait_event(b["in_ready"])
+        if i >= 2:  # d_out of this set is free once step i - 2's result left
+            s_cmp.wait_event(b["out_done"])
+        mdx.partition(b["d_in"], discr, out=b["d_out"], sizes=b["sizes"], ws=b["ws"],
+                      stream=s_cmp)
+        b["part_done"].record(s_cmp)
+        s_d2h.wait_event(b["part_done"])
+        with torch.cuda.stream(s_d2h):
             b["h_out"].copy_(b["d_out"], non_blocking=True)
             b["h_sizes"].copy_(b["sizes"], non_blocking=True)
+            b["out_done"].record(s_d2h)
 
     for i in range(2):
         e2e_step(i)
@@ -780,12 +794,12 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for b in e2e_sets:
-        b["stream"].wait_event(e0)
+    for st in (s_h2d, s_cmp, s_d2h):
+        st.wait_event(e0)
     for i in range(args.e2e_steps):
         e2e_step(i)
-    for b in e2e_sets:
-        stream.wait_stream(b["stream"])
+    for st in (s_h2d, s_cmp, s_d2h):
+        stream.wait_stream(st)
     e1.record(stream)
     barrier()
     e2e_s = e0.elapsed_time(e1) * 1e-3
@@ -797,20 +811,20 @@ def main():
     # sanity: the last result equals the device result of the same input
     assert torch.equal(e2e_sets[(args.e2e_steps - 1) % 2]["h_out"].to(dev), d_out)
     # the bound of the e2e leg: the same two copies alone, in both directions at
-    # once (pinned memory, the same two streams), no partition
+    # once (pinned memory, the same copy streams), no partition
     a, b = e2e_sets
     c0 = torch.cuda.Event(enable_timing=True)
     c1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     c0.record(stream)
-    a["stream"].wait_event(c0)
-    b["stream"].wait_event(c0)
-    with torch.cuda.stream(a["stream"]):
+    s_h2d.wait_event(c0)
+    s_d2h.wait_event(c0)
+    with torch.cuda.stream(s_h2d):
         a["d_in"].copy_(a["h_in"], non_blocking=True)
-    with torch.cuda.stream(b["stream"]):
+    with torch.cuda.stream(s_d2h):
         b["h_out"].copy_(b["d_out"], non_blocking=True)
-    stream.wait_stream(a["stream"])
-    stream.wait_stream(b["stream"])
+    stream.wait_stream(s_h2d)
+    stream.wait_stream(s_d2h)
     c1.record(stream)
     torch.cuda.synchronize()
     copy_s = c0.elapsed_time(c1) * 1e-3
