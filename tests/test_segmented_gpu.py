@@ -240,7 +240,8 @@ def test_head_flag_form_matches_offsets_form(cuda_ready):
 
 
 def test_repeated_calls_reuse_workspace(cuda_ready):
-    # epoch-tagged look-back words: back-to-back calls on one workspace
+    # back-to-back calls on one workspace: every ticket, count and list the
+    # planner resets must be reset (nothing is cleared between calls)
     lengths = lognormal_lengths(400, 61)
     offs = offsets_from_lengths(lengths)
     x = oracle.fill_uniform_u32(int(offs[-1]), 62)
