@@ -31,8 +31,10 @@ instead, on rank 0 only, with every host thread, on the same seeded input.
 
 Multi-GPU (torchrun, one process per GPU): every rank partitions its own
 N = 2^28 array (independent units, no data-path collective; weak scaling);
-the step time is the max over ranks.  --distributed instead partitions one
-array spread over the ranks (count all-gather + scatter into peer chunks).
+the step time is the max over ranks.  The same run then partitions the
+ranks' arrays as ONE array spread over them (count all-gather + scatter into
+peer chunks) and reports it under "distributed"; --distributed runs only
+that.
 """
 from __future__ import annotations
 
@@ -524,6 +526,47 @@ def cpu_baseline(x, m: int, reps: int, seq_sample: int = 1 << 25):
     return res, None
 
 
+def distributed_leg(args, torch, dist, dev, world, x, m, discr):
+    """With more than one rank: the ranks' arrays taken as ONE array of
+    world * N elements (rank r holds chunk r) and partitioned across them by
+    mdiscriminator_b200.distributed (class counts, an all-gather of the
+    counts over NCCL, the scatter kernel storing into every rank's output
+    chunk through IPC peer mappings) -- the exchange step of the sharded
+    path, next to the independent arrays of the headline.  The first call
+    checks the device error status; device time by CUDA events, max over
+    ranks.  Every rank takes the same collective steps; an error is reported
+    in the line instead of ending the run."""
+    from mdiscriminator_b200 import distributed as D
+    try:
+        out, _ = D.partition_distributed(x, discr, out=None)
+        for _ in range(2):
+            out, _ = D.partition_distributed(x, discr, out=out, check=False)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            out, _ = D.partition_distributed(x, discr, out=out, check=False)
+        e1.record()
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1) / args.steps], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        res = {"metric": "Gelem/s, one array over the ranks (distributed partition)",
+               "value": world * x.numel() / ms / 1e6, "unit": "Gelem/s", "ms_per_step": ms,
+               "workload": f"one array of {world} x {x.numel()} int32 (rank r holds chunk r), "
+                           f"m={m}; output in balanced chunks across the ranks",
+               "transport": "count all-gather (NCCL) + scatter into peer chunks (CUDA IPC)"}
+    except Exception as e:  # noqa: BLE001 -- reported, not fatal to the headline line
+        res = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+    finally:
+        try:
+            D.close_peer_maps()
+        except Exception:  # noqa: BLE001
+            pass
+    return res
+
+
 def distributed_main(args, torch, dist, mdx, dev, world, rank):
     """--distributed: one array of world * N elements, rank r holding the r-th
     chunk of N (weak scaling), partitioned by the "p2p" transport of
@@ -831,6 +874,7 @@ def main():
     pcie_gbs = n * 4 / copy_s / 1e9        # per direction, both directions busy
     e2e_bound = world * n / copy_s / 1e9   # elements/s if the copies were all a step cost
     del e2e_sets, a, b
+    dist_leg = distributed_leg(args, torch, dist, dev, world, d_in, m, discr) if world > 1 else None
 
     if rank == 0:
         peak, peak_src = peaks()
@@ -911,6 +955,8 @@ def main():
             "clocks": clk,
             "gpu_launches": 2 * args.steps,
         }
+        if dist_leg is not None:
+            line["distributed"] = dist_leg
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
