@@ -8,9 +8,10 @@
 //    counters in a register (local rank = number of its earlier elements of
 //    the same class; the 16th element is kept aside so no lane can reach 16)
 //    and publishes its per-class counts to a [class][thread] u16 matrix;
-//  * row scans: warp w scans rows w and w + W of the matrix (exclusive prefix
-//    over threads = stable order); every warp derives the tile's class runs
-//    (lanes = classes) and folds each run's stage slot into its rows;
+//  * row scans: warp w < m/2 scans rows w and w + m/2 of the matrix at once,
+//    packed in u16 pairs (exclusive prefix over threads = stable order); those
+//    warps derive the tile's class runs (lanes = classes) and fold each run's
+//    stage slot into their rows;
 //  * pass 2: element -> stage slot = row prefix + local rank;
 //  * write-out: each class run sits in the stage at the same 16-byte phase as
 //    its destination, so its aligned interior leaves by one bulk store
@@ -174,6 +175,7 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[ITEMS], ui
     constexpr int LR = (ITEMS + 7) / 8;
     static_assert(M <= 16 && M >= 2, "class bound");
     static_assert(M <= 2 * W, "each warp scans at most two rows");
+    static_assert((M & (M - 1)) == 0, "rows paired as w and w + M/2");
     static_assert(ITEMS == 16 || ITEMS == 8 || ITEMS == 4 || ITEMS == 2, "thread elements");
     static_assert(PER == 8, "row scans load 8 entries per lane");
 
@@ -211,34 +213,40 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[ITEMS], ui
     if (__syncthreads_or(!ok)) return false;  // (A)
     after_counts();
 
-    // ---- row scans: warp w owns rows w and w + W
-    uint32_t pre[2][PER];
+    // ---- row scans: warp w < M/2 scans rows w and w + M/2 at once, the two
+    // rows' u16 counts packed in one word (row w low, row w + M/2 high; a
+    // row's sum is at most the tile, < 2^16); the other warps idle here
+    constexpr int H = M / 2;
+    const bool scans = warp < H;
+    uint32_t pre[PER];  // packed exclusive prefixes of this lane's 8 threads
+    if (scans) {
+        const uint4 xa = *reinterpret_cast<const uint4*>(cnt_sm + warp * THREADS + lane * PER);
+        const uint4 xb = *reinterpret_cast<const uint4*>(cnt_sm + (warp + H) * THREADS + lane * PER);
+        const uint32_t x[8] = {__byte_perm(xa.x, xb.x, 0x5410), __byte_perm(xa.x, xb.x, 0x7632),
+                               __byte_perm(xa.y, xb.y, 0x5410), __byte_perm(xa.y, xb.y, 0x7632),
+                               __byte_perm(xa.z, xb.z, 0x5410), __byte_perm(xa.z, xb.z, 0x7632),
+                               __byte_perm(xa.w, xb.w, 0x5410), __byte_perm(xa.w, xb.w, 0x7632)};
+        uint32_t tot = 0;
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-        const int c = warp + h * W;
-        if (c < M) {
-            const uint4 xw = *reinterpret_cast<const uint4*>(cnt_sm + c * THREADS + lane * PER);
-            const uint32_t x[8] = {xw.x & 0xffffu, xw.x >> 16, xw.y & 0xffffu, xw.y >> 16,
-                                   xw.z & 0xffffu, xw.z >> 16, xw.w & 0xffffu, xw.w >> 16};
-            uint32_t tot = 0;
+        for (int q = 0; q < 8; q++) tot += x[q];
+        const uint32_t incl = warp_incl_scan(tot);
+        uint32_t run = incl - tot;
 #pragma unroll
-            for (int q = 0; q < 8; q++) tot += x[q];
-            const uint32_t incl = warp_incl_scan(tot);
-            uint32_t run = incl - tot;
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                pre[h][q] = run;
-                run += x[q];
-            }
-            if (lane == 31) sh.rowtot[c] = incl;
+        for (int q = 0; q < 8; q++) {
+            pre[q] = run;
+            run += x[q];
+        }
+        if (lane == 31) {
+            sh.rowtot[warp] = incl & 0xffffu;
+            sh.rowtot[warp + H] = incl >> 16;
         }
     }
     __syncthreads();  // (B)
 
-    // ---- class runs (every warp, lanes = classes): destination of run c and
-    // its stage slot, at the destination's 16-byte phase within kAU slots of
-    // slack per run
-    {
+    // ---- class runs (the scanning warps, lanes = classes): destination of
+    // run c and its stage slot, at the destination's 16-byte phase within kAU
+    // slots of slack per run; each scanning warp folds the slots into its rows
+    if (scans) {
         const uint32_t c = static_cast<uint32_t>(lane);
         const bool cls = c < static_cast<uint32_t>(M);
         const uint32_t cc = cls ? sh.rowtot[c] : 0u;
@@ -247,20 +255,18 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[ITEMS], ui
         const uint32_t room = cc + (cls ? AU : 0u);
         const uint32_t q0 = warp_incl_scan(room) - room;
         const uint32_t st = q0 + (((out.phase() + dst) - q0) & (AU - 1u));
+        // slots < kStageElems < 2^16: the two rows' slots stay packed
+        const uint32_t add = __shfl_sync(0xffffffffu, st, warp) |
+                             (__shfl_sync(0xffffffffu, st, warp + H) << 16);
+        uint32_t p[8];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int row = warp + h * W;
-            if (row < M) {
-                // slots < kStageElems < 2^16: pairs of u16 prefixes per word
-                const uint32_t add = __shfl_sync(0xffffffffu, st, row);
-                const uint32_t add2 = add | (add << 16);
-                *reinterpret_cast<uint4*>(cnt_sm + row * THREADS + lane * PER) =
-                    make_uint4((pre[h][0] | (pre[h][1] << 16)) + add2,
-                               (pre[h][2] | (pre[h][3] << 16)) + add2,
-                               (pre[h][4] | (pre[h][5] << 16)) + add2,
-                               (pre[h][6] | (pre[h][7] << 16)) + add2);
-            }
-        }
+        for (int q = 0; q < 8; q++) p[q] = pre[q] + add;
+        *reinterpret_cast<uint4*>(cnt_sm + warp * THREADS + lane * PER) =
+            make_uint4(__byte_perm(p[0], p[1], 0x5410), __byte_perm(p[2], p[3], 0x5410),
+                       __byte_perm(p[4], p[5], 0x5410), __byte_perm(p[6], p[7], 0x5410));
+        *reinterpret_cast<uint4*>(cnt_sm + (warp + H) * THREADS + lane * PER) =
+            make_uint4(__byte_perm(p[0], p[1], 0x7632), __byte_perm(p[2], p[3], 0x7632),
+                       __byte_perm(p[4], p[5], 0x7632), __byte_perm(p[6], p[7], 0x7632));
         if (warp == 0 && cls) {
             sh.cursor[par ^ 1u][c] = FORWARD ? cur + cc : dst;
             sh.run_start[c] = st;
