@@ -160,6 +160,15 @@ cudaError_t pinned_alloc(T** p, size_t bytes) {
     return cudaMallocHost(reinterpret_cast<void**>(p), bytes);
 }
 
+// A spin-wait hint to the core (lets its sibling hyperthread run).
+inline void cpu_relax() {
+#if defined(__x86_64__) || defined(__i386__)
+    __builtin_ia32_pause();
+#elif defined(__aarch64__)
+    asm volatile("yield" ::: "memory");
+#endif
+}
+
 using Clock = std::chrono::steady_clock;
 inline double now_s() {
     return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
@@ -350,7 +359,7 @@ void poll_loop(Server* s) {
             any = any || res[i] != cudaErrorNotReady;
         }
         if (!any) {
-            for (int k = 0; k < 64; k++) __builtin_ia32_pause();
+            for (int k = 0; k < 64; k++) cpu_relax();
             lk.lock();
             continue;
         }
