@@ -414,7 +414,7 @@ def time_calls(torch, fn, reps, warmup, flush=None):
     return statistics.median(ms), statistics.mean(ms)
 
 
-def configs_measurement(torch, mdx, dev, peak, reps=10, warmup=3):
+def configs_measurement(torch, mdx, dev, peak, reps=20, warmup=3):
     """The plain configurations of the benchmark list other than the headline,
     each on its own seeded input generated on the device
     (mdiscriminator_b200.workloads), timed call by call with CUDA events."""
