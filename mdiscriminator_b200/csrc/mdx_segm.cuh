@@ -149,15 +149,25 @@ __device__ __forceinline__ bool group_head(const SegArgs& a, uint64_t s, uint64_
     return s == 0 || a.offsets[s - 1] / GW != a0 / GW || (s % kGroupSegs) == 0;
 }
 
-// A segment [a0, a1) longer than one tile is medium when the tiles that hold
-// it, counted from the 128-byte row of its first element (a tile is
-// P * sizeof(V) = 16 KB, so a row is P / 128 elements), number at most
-// mid_tiles: seg_mid then reads it once.  The longer ones are cut into runs.
+// A segment's tiles start at the 128-byte row holding its first element (a
+// tile is P * sizeof(V) = 16 KB, so a row is P / 128 elements): the TMA box
+// needs a row start, and tiles counted from there leave only the last one
+// short.
+template <int P>
+__device__ __forceinline__ uint64_t seg_row_start(uint64_t a0) {
+    return a0 & ~(static_cast<uint64_t>(P) / 128u - 1u);
+}
+template <int P>
+__device__ __forceinline__ uint32_t seg_tiles(uint64_t a0, uint64_t a1) {
+    return static_cast<uint32_t>((a1 - seg_row_start<P>(a0) + P - 1u) / P);
+}
+
+// A segment [a0, a1) longer than one tile is medium when its tiles number at
+// most mid_tiles: seg_mid then reads it once.  The longer ones are cut into
+// runs of run_tiles of those tiles (every run but the last is whole tiles).
 template <int P>
 __device__ __forceinline__ bool is_mid(const SegArgs& a, uint64_t a0, uint64_t a1) {
-    constexpr uint64_t kPerRow = static_cast<uint64_t>(P) / 128u;
-    const uint64_t rb = a0 & ~(kPerRow - 1u);
-    return a.mid_tiles > 0u && (a1 - rb + P - 1u) / P <= a.mid_tiles;
+    return a.mid_tiles > 0u && seg_tiles<P>(a0, a1) <= a.mid_tiles;
 }
 
 __device__ __forceinline__ uint64_t seg_count(const SegArgs& a) {
@@ -188,8 +198,7 @@ __global__ void __launch_bounds__(THREADS) seg_plan_spans(SegArgs a) {
                 if (is_mid<P>(a, a0, a1)) {
                     mid = 1;
                 } else {
-                    const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
-                    runs = (span + a.run_tiles - 1) / a.run_tiles;
+                    runs = (seg_tiles<P>(a0, a1) + a.run_tiles - 1) / a.run_tiles;
                 }
             } else {
                 head = group_head<P>(a, s, a0) ? 1u : 0u;
@@ -295,18 +304,17 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
                     const uint32_t pos = moff + a.mid_loc[s];
                     if (pos < num_mids) a.mids[pos] = static_cast<uint32_t>(s);
                 } else if (a1 - a0 > static_cast<uint64_t>(P)) {
-                    const uint32_t span = static_cast<uint32_t>((a1 - 1) / P - a0 / P + 1);
-                    const uint32_t nr = (span + a.run_tiles - 1) / a.run_tiles;
+                    const uint32_t nr = (seg_tiles<P>(a0, a1) + a.run_tiles - 1) / a.run_tiles;
                     const uint32_t pos = roff + a.run_loc[s];
                     if (nr <= 16) {  // this thread emits the runs itself
                         if (static_cast<uint64_t>(pos) + nr <= num_runs) {
-                            const uint64_t w0 = a0 / P;
+                            const uint64_t rb = seg_row_start<P>(a0);
+                            const uint64_t len = static_cast<uint64_t>(a.run_tiles) * P;
                             for (uint32_t r = 0; r < nr; r++) {
-                                const uint64_t wa = w0 + static_cast<uint64_t>(r) * a.run_tiles;
                                 RunEntry e;
                                 e.seg = static_cast<uint32_t>(s);
-                                e.p0 = static_cast<uint32_t>(max(a0, wa * P));
-                                e.p1 = static_cast<uint32_t>(min(a1, (wa + a.run_tiles) * P));
+                                e.p0 = static_cast<uint32_t>(max(a0, rb + r * len));
+                                e.p1 = static_cast<uint32_t>(min(a1, rb + (r + 1) * len));
                                 e.jlast = pos + nr - 1u;
                                 a.runs[pos + r] = e;
                             }
@@ -336,13 +344,13 @@ __global__ void __launch_bounds__(THREADS) seg_plan_emit(SegArgs a) {
             const uint32_t seg = list_seg[q], pos = list_pos[q], nr = list_runs[q];
             if (static_cast<uint64_t>(pos) + nr > num_runs) continue;  // malformed offsets
             const uint64_t a0 = a.offsets[seg], a1 = a.offsets[seg + 1];
-            const uint64_t w0 = a0 / P;
+            const uint64_t rb = seg_row_start<P>(a0);
+            const uint64_t len = static_cast<uint64_t>(a.run_tiles) * P;
             for (uint32_t r = tid; r < nr; r += THREADS) {
-                const uint64_t wa = w0 + static_cast<uint64_t>(r) * a.run_tiles;
                 RunEntry e;
                 e.seg = seg;
-                e.p0 = static_cast<uint32_t>(max(a0, wa * P));
-                e.p1 = static_cast<uint32_t>(min(a1, (wa + a.run_tiles) * P));
+                e.p0 = static_cast<uint32_t>(max(a0, rb + r * len));
+                e.p1 = static_cast<uint32_t>(min(a1, rb + (r + 1) * len));
                 e.jlast = pos + nr - 1u;
                 a.runs[pos + r] = e;
             }
