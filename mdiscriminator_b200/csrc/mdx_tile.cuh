@@ -526,14 +526,16 @@ __device__ __forceinline__ bool tile_scatter_wide_impl(const D& d, const V (&v)[
 #pragma unroll
         for (int i = 0; i < 5; i++) com &= __ballot_sync(0xffffffffu, (c >> i) & 1u) ^ inv[i];
         uint32_t peers, base;
-        const uint32_t x = __shfl_sync(0xffffffffu, runs, c & 31u);
+        // a shuffle's source lane is taken mod 32: c selects lane c mod 32
+        const uint32_t x = __shfl_sync(0xffffffffu, runs, c);
         if constexpr (B == 6) {
-            const uint32_t b5 = __ballot_sync(0xffffffffu, (c >> 5) & 1u);
+            const uint32_t hi = (c >> 5) & 1u;
+            const uint32_t b5 = __ballot_sync(0xffffffffu, hi);
             const uint32_t com1 = com & b5;
             // lanes of class (c mod 32) with the same sixth bit as c
-            const uint32_t p = __shfl_sync(0xffffffffu, com, c & 31u);
-            peers = p & ((c & 32u) ? b5 : ~b5);
-            base = (x >> ((c & 32u) >> 1)) & 0xffffu;
+            const uint32_t p = __shfl_sync(0xffffffffu, com, c);
+            peers = p & (b5 ^ (hi - 1u));
+            base = __byte_perm(x, 0u, 0x4410u + hi * 0x22u);  // low or high 16 bits
             const uint32_t n1 = static_cast<uint32_t>(__popc(com1));
             runs += (static_cast<uint32_t>(__popc(com)) - n1) + (n1 << 16);
         } else {
