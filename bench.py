@@ -956,7 +956,10 @@ def main():
             "served": served,
             "sort_baseline": sort_ref,
             "clocks": clk,
-            "gpu_launches": 2 * args.steps,
+            # kernels of this repository per timed step: count + scatter, or
+            # the one cooperative kernel
+            "gpu_launches": (2 if mdx.get_tuning(mdx.ELEM_U32, m, n)["plain_two_kernel"] else 1)
+            * args.steps,
         }
         if dist_leg is not None:
             line["distributed"] = dist_leg
