@@ -386,6 +386,10 @@ typedef struct {
     uint32_t tile_bytes;         /* plain path: bytes of a tile per thread, 64 (default, 0) or 32
                                     (tiles half as long: more CTAs busy on short inputs; count +
                                     scatter as two kernels; 4- and 8-byte elements) */
+    uint32_t tile_threads;       /* plain path: threads of a scatter CTA, 256 (default, 0) or 512
+                                    (64-byte tiles twice as long, half the per-tile steps; count +
+                                    scatter as two kernels; 4- and 8-byte elements, m <= 16;
+                                    takes precedence over tile_bytes) */
 } mdx_tuning;
 
 mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_t log2_n_hi,

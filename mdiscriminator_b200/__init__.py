@@ -67,7 +67,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("plain_ctas_per_sm", ctypes.c_uint32), ("run_tiles", ctypes.c_uint32),
                 ("group_batch", ctypes.c_uint32), ("plain_two_kernel", ctypes.c_uint32),
                 ("pool_pct", ctypes.c_uint32), ("mid_tiles", ctypes.c_uint32),
-                ("tile_bytes", ctypes.c_uint32)]
+                ("tile_bytes", ctypes.c_uint32), ("tile_threads", ctypes.c_uint32)]
 
 
 TUNING_PATH = os.path.join(HERE, "tuning.json")
@@ -101,7 +101,8 @@ def load_tuning(path: str, missing_ok: bool = False) -> int:
         set_tuning(elem, e["m"], lo, hi, **{x: e[x] for x in ("plain_ctas_per_sm", "run_tiles",
                                                              "group_batch", "plain_two_kernel",
                                                              "pool_pct", "mid_tiles",
-                                                             "tile_bytes") if x in e})
+                                                             "tile_bytes", "tile_threads")
+                                                  if x in e})
         k += 1
     return k
 

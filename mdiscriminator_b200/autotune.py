@@ -40,10 +40,12 @@ import mdiscriminator_b200 as mdx  # noqa: E402
 # installed for); 8-byte records are timed at half the count (same bytes)
 BUCKETS = [(1 << 20, (0, 21)), (1 << 24, (22, 25)), (1 << 28, (26, 33))]
 
-# plain-path candidates: (plain_two_kernel, plain_ctas_per_sm, pool_pct, tile_bytes)
-PLAIN_CANDIDATES = [(1, 4, 0, 64), (1, 3, 0, 64), (1, 0, 0, 64), (1, 4, 0, 32), (1, 0, 0, 32),
-                    (0, 4, 100, 64), (0, 4, 10, 64), (0, 4, 20, 64), (0, 4, 33, 64),
-                    (0, 3, 10, 64)]
+# plain-path candidates: (plain_two_kernel, plain_ctas_per_sm, pool_pct, tile_bytes,
+# tile_threads)
+PLAIN_CANDIDATES = [(1, 4, 0, 64, 256), (1, 3, 0, 64, 256), (1, 0, 0, 64, 256),
+                    (1, 4, 0, 32, 256), (1, 0, 0, 32, 256), (1, 0, 0, 64, 512),
+                    (0, 4, 100, 64, 256), (0, 4, 10, 64, 256), (0, 4, 20, 64, 256),
+                    (0, 4, 33, 64, 256), (0, 3, 10, 64, 256)]
 
 
 def timeit(fn, torch, reps=20, warm=3):
@@ -96,20 +98,22 @@ def main(argv=None):
             for M in bounds:
                 sizes = torch.empty(M, dtype=torch.uint32, device=dev)
                 best = None
-                for two, k, pool, tb in PLAIN_CANDIDATES:
+                for two, k, pool, tb, tt in PLAIN_CANDIDATES:
                     mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=k, plain_two_kernel=two,
-                                   pool_pct=pool, tile_bytes=tb)
+                                   pool_pct=pool, tile_bytes=tb, tile_threads=tt)
                     ms = timeit(lambda: mdx.partition(d, ("mask", M), out=out, sizes=sizes, ws=ws),
                                 torch)
                     if ws.error() != mdx.MDX_OK:
                         raise SystemExit(f"device error while tuning {ename} m={M}")
                     if best is None or ms < best[0]:
-                        best = (ms, k, two, pool, tb)
+                        best = (ms, k, two, pool, tb, tt)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "plain",
                                 "plain_ctas_per_sm": best[1], "plain_two_kernel": best[2],
-                                "pool_pct": best[3], "tile_bytes": best[4], "ms": best[0]})
+                                "pool_pct": best[3], "tile_bytes": best[4],
+                                "tile_threads": best[5], "ms": best[0]})
                 mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=best[1],
-                               plain_two_kernel=best[2], pool_pct=best[3], tile_bytes=best[4])
+                               plain_two_kernel=best[2], pool_pct=best[3], tile_bytes=best[4],
+                               tile_threads=best[5])
             del d, out, ws
         seg_bounds = [2, 4, 8, 16]
         for n4, (lo, hi) in buckets:
@@ -130,7 +134,7 @@ def main(argv=None):
                           if e["elem"] == ename and e["m"] == M and e["path"] == "plain"
                           and e["log2_n"] == [lo, hi])
                 plain_k, plain_two, pool = pe["plain_ctas_per_sm"], pe["plain_two_kernel"], pe["pool_pct"]
-                tb = pe["tile_bytes"]
+                tb, tt = pe["tile_bytes"], pe["tile_threads"]
                 best = None
                 # (run_tiles, group_batch) without medium segments, then the
                 # winner with the medium-segment kernel on
@@ -138,18 +142,20 @@ def main(argv=None):
                     rt, gb, mid = cand if cand is not None else (best[1], best[2], 2)
                     mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
                                    plain_two_kernel=plain_two, pool_pct=pool, tile_bytes=tb,
-                                   run_tiles=rt, group_batch=gb, mid_tiles=mid)
+                                   tile_threads=tt, run_tiles=rt, group_batch=gb, mid_tiles=mid)
                     ms = timeit(lambda: mdx.partition_segmented(d, do, ("mask", M), out=out,
                                                                 seg_sizes=ss, ws=ws), torch)
                     if best is None or ms < best[0]:
                         best = (ms, rt, gb, mid)
                 entries.append({"elem": ename, "m": M, "log2_n": [lo, hi], "path": "segmented",
                                 "plain_ctas_per_sm": plain_k, "plain_two_kernel": plain_two,
-                                "pool_pct": pool, "tile_bytes": tb, "run_tiles": best[1],
+                                "pool_pct": pool, "tile_bytes": tb, "tile_threads": tt,
+                                "run_tiles": best[1],
                                 "group_batch": best[2], "mid_tiles": best[3], "ms": best[0]})
                 mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=plain_k,
                                plain_two_kernel=plain_two, pool_pct=pool, tile_bytes=tb,
-                               run_tiles=best[1], group_batch=best[2], mid_tiles=best[3])
+                               tile_threads=tt, run_tiles=best[1], group_batch=best[2],
+                               mid_tiles=best[3])
             del d, out, ws
     # one entry per key: the segmented entry (it carries the plain knob too)
     merged = {}

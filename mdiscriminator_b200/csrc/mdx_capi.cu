@@ -450,7 +450,8 @@ mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_
         return MDX_ERR_INVALID;
     if (t->run_tiles > 64 || t->group_batch > 1024 || t->plain_two_kernel > 1 || t->pool_pct > 100 ||
         t->mid_tiles > static_cast<uint32_t>(kMidTiles) ||
-        (t->tile_bytes != 0 && t->tile_bytes != 32 && t->tile_bytes != 64))
+        (t->tile_bytes != 0 && t->tile_bytes != 32 && t->tile_bytes != 64) ||
+        (t->tile_threads != 0 && t->tile_threads != 256 && t->tile_threads != 512))
         return MDX_ERR_INVALID;
     TuningTable& tt = tuning_table();
     std::lock_guard<std::mutex> lk(tt.mu);
@@ -463,6 +464,7 @@ mdx_status mdx_set_tuning(mdx_elem elem, uint32_t m, uint32_t log2_n_lo, uint32_
         x.pool_pct = t->pool_pct;
         x.mid_tiles = t->mid_tiles;
         x.tile_bytes = t->tile_bytes;
+        x.tile_threads = t->tile_threads;
     }
     return MDX_OK;
 }
@@ -478,6 +480,7 @@ mdx_status mdx_get_tuning(mdx_elem elem, uint32_t m, uint64_t n, mdx_tuning* t) 
     t->pool_pct = x.pool_pct ? x.pool_pct : kFusedPoolPct;
     t->mid_tiles = x.mid_tiles >= 2 ? x.mid_tiles : 1u;
     t->tile_bytes = x.tile_bytes == 32 ? 32u : 64u;
+    t->tile_threads = x.tile_threads == 512 ? 512u : 256u;
     return MDX_OK;
 }
 

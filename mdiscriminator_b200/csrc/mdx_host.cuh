@@ -130,7 +130,8 @@ inline OccCache& occ_cache() {
     return c;
 }
 
-inline cudaError_t occupancy(const void* fn, size_t dyn_smem, int* blocks, int* sms) {
+inline cudaError_t occupancy(const void* fn, size_t dyn_smem, int* blocks, int* sms,
+                             int threads = kThreads) {
     OccCache& C = occ_cache();
     std::mutex& g_occ_mu = C.mu;
     OccEntry* g_occ = C.e;
@@ -153,7 +154,7 @@ inline cudaError_t occupancy(const void* fn, size_t dyn_smem, int* blocks, int* 
         if (err != cudaSuccess) return err;
     }
     int b = 0, s = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, dyn_smem);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, threads, dyn_smem);
     if (err != cudaSuccess) return err;
     err = cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev);
     if (err != cudaSuccess) return err;
@@ -223,6 +224,7 @@ struct Tuning {
     uint32_t pool_pct = 0;          // one-kernel path: % of every chunk drained by ticket (0: default)
     uint32_t mid_tiles = 0;         // segmented: medium segments up to this many tiles (0, 1: none)
     uint32_t tile_bytes = 0;        // plain path: tile bytes per thread (0, 64: 64; 32: 32)
+    uint32_t tile_threads = 0;      // plain path: threads of a scatter CTA (0, 256: 256; 512)
 };
 struct TuningTable {
     std::mutex mu;
@@ -276,28 +278,30 @@ static_assert(kFusedBarOffset >= kDistSkipOffset + 4 && kFusedBarOffset + 16 <= 
               "barrier words inside the header");
 
 // BPT: bytes of a tile per thread (64: the tiles of every path; 32: tiles
-// half as long, two-kernel path only, for the sizes where the tuning table
-// picks them).
-template <class V, class D, int M, int BPT>
+// half as long); TS: threads of a scatter CTA (256, or 512 for tiles twice
+// as long).  Geometries other than 64 bytes x 256 threads run the two-kernel
+// path only, for the sizes where the tuning table picks them.
+template <class V, class D, int M, int BPT, int TS>
 mdx_status run_plain_g(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
                        uint32_t* d_sizes, uint32_t* d_headflags, unsigned char* ws,
                        const PlainLayout& L, cudaStream_t stream, cudaEvent_t ev_mid,
                        PlainStep step, const DistOut* dist, bool allow_fused) {
     constexpr int ITEMS = BPT / static_cast<int>(sizeof(V));
-    constexpr int TILE = kThreads * ITEMS;
+    constexpr int TILE = TS * ITEMS;
+    constexpr bool kBase = BPT == 64 && TS == kThreads;  // the geometry of every path
     static_assert(BPT != 64 || ITEMS == ElemCfg<V>::kItems, "64-byte tiles");
     auto count = plain_count_kernel<V, D, M, kThreads, TILE>;
     const void* scatter_fn;
     size_t smem;
     {
-        using SL = ScatterTmaSmem<V, kThreads, kStages, M, BPT>;
+        using SL = ScatterTmaSmem<V, TS, kStages, M, BPT>;
         static_assert(SL::kTile == TILE, "both kernels use the same tiles");
         scatter_fn = reinterpret_cast<const void*>(
-            plain_scatter_tma_kernel<V, D, M, kThreads, kStages, OutFlat<V>, BPT>);
+            plain_scatter_tma_kernel<V, D, M, TS, kStages, OutFlat<V>, BPT>);
         smem = SL::kBytes;
     }
     int blocks = 0, sms = 0;
-    if (occupancy(scatter_fn, smem, &blocks, &sms) != cudaSuccess) return MDX_ERR_CUDA;
+    if (occupancy(scatter_fn, smem, &blocks, &sms, TS) != cudaSuccess) return MDX_ERR_CUDA;
     const uint32_t nt = static_cast<uint32_t>((n + TILE - 1) / TILE);
     const Tuning tun = tuning_for(sizeof(V) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_U32, M, n);
     if (tun.plain_ctas_per_sm > 0 && static_cast<int>(tun.plain_ctas_per_sm) < blocks)
@@ -339,7 +343,7 @@ mdx_status run_plain_g(const void* d_in, void* d_out, uint64_t n, D d, uint32_t 
         if (ev_mid != nullptr && cudaEventRecord(ev_mid, stream) != cudaSuccess) return MDX_ERR_CUDA;
         return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     }
-    if constexpr (BPT == 64) {  // the one-kernel path has 64-byte tiles only
+    if constexpr (kBase) {  // the one-kernel path has the base geometry only
         if (step == PlainStep::kBoth && dist == nullptr && ev_mid == nullptr && allow_fused &&
             tun.plain_two_kernel == 0) {
             // one cooperative kernel: count, grid barrier, scatter (mdx_fused.cuh)
@@ -411,20 +415,20 @@ mdx_status run_plain_g(const void* d_in, void* d_out, uint64_t n, D d, uint32_t 
     }
     if (step == PlainStep::kCount) return cudaGetLastError() == cudaSuccess ? MDX_OK : MDX_ERR_CUDA;
     {
-        using SL = ScatterTmaSmem<V, kThreads, kStages, M, BPT>;
+        using SL = ScatterTmaSmem<V, TS, kStages, M, BPT>;
         CUtensorMap map;
         a.use_tma = make_row_map(&map, d_in, n, sizeof(V), SL::kRows, M <= 16) ? 1 : 0;
         if (dist == nullptr) {
             const OutFlat<V> o{static_cast<V*>(d_out),
                                static_cast<uint32_t>((reinterpret_cast<uintptr_t>(d_out) / sizeof(V)) &
                                                      (16u / sizeof(V) - 1u))};
-            auto scatter = plain_scatter_tma_kernel<V, D, M, kThreads, kStages, OutFlat<V>, BPT>;
+            auto scatter = plain_scatter_tma_kernel<V, D, M, TS, kStages, OutFlat<V>, BPT>;
             if (step == PlainStep::kBoth && ev_mid == nullptr) {
                 // programmatic dependent launch: scheduled while the count grid
                 // drains, it starts its first tile copies before waiting for it
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3(G);
-                cfg.blockDim = dim3(kThreads);
+                cfg.blockDim = dim3(TS);
                 cfg.dynamicSmemBytes = smem;
                 cfg.stream = stream;
                 cudaLaunchAttribute attr[1];
@@ -434,10 +438,10 @@ mdx_status run_plain_g(const void* d_in, void* d_out, uint64_t n, D d, uint32_t 
                 cfg.numAttrs = 1;
                 if (cudaLaunchKernelEx(&cfg, scatter, a, d, map, o) != cudaSuccess) return MDX_ERR_CUDA;
             } else {
-                scatter<<<G, kThreads, smem, stream>>>(a, d, map, o);
+                scatter<<<G, TS, smem, stream>>>(a, d, map, o);
             }
-        } else if constexpr (sizeof(V) == 16 || BPT != 64) {
-            return MDX_ERR_UNSUPPORTED;  // no sharded 16-byte record kernels; sharded: 64-byte tiles
+        } else if constexpr (sizeof(V) == 16 || !kBase) {
+            return MDX_ERR_UNSUPPORTED;  // no sharded 16-byte record kernels; sharded: base tiles
         } else {
             // the sharded instantiation is a kernel of its own: give it the
             // shared-memory attribute too (the grid stays the count's G, the
@@ -471,12 +475,21 @@ mdx_status run_plain(const void* d_in, void* d_out, uint64_t n, D d, uint32_t m,
                      const DistOut* dist = nullptr, bool allow_fused = true) {
     if constexpr (sizeof(V) <= 8) {
         const Tuning tun = tuning_for(sizeof(V) == 8 ? MDX_ELEM_REC8 : MDX_ELEM_U32, M, n);
-        if (tun.tile_bytes == 32 && dist == nullptr && step == PlainStep::kBoth)
-            return run_plain_g<V, D, M, 32>(d_in, d_out, n, d, m, d_sizes, d_headflags, ws, L,
-                                            stream, ev_mid, step, dist, allow_fused);
+        if (dist == nullptr && step == PlainStep::kBoth) {
+            if constexpr (M <= 16) {  // the warp-rank step spills at 512 threads
+                if (tun.tile_threads == 512)
+                    return run_plain_g<V, D, M, 64, 512>(d_in, d_out, n, d, m, d_sizes, d_headflags,
+                                                         ws, L, stream, ev_mid, step, dist,
+                                                         allow_fused);
+            }
+            if (tun.tile_bytes == 32)
+                return run_plain_g<V, D, M, 32, kThreads>(d_in, d_out, n, d, m, d_sizes,
+                                                          d_headflags, ws, L, stream, ev_mid, step,
+                                                          dist, allow_fused);
+        }
     }
-    return run_plain_g<V, D, M, 64>(d_in, d_out, n, d, m, d_sizes, d_headflags, ws, L, stream,
-                                    ev_mid, step, dist, allow_fused);
+    return run_plain_g<V, D, M, 64, kThreads>(d_in, d_out, n, d, m, d_sizes, d_headflags, ws, L,
+                                              stream, ev_mid, step, dist, allow_fused);
 }
 
 template <class V, class D>

@@ -353,7 +353,7 @@ struct ScatterTmaSmem {
 // output chunks of several ranks (distributed partition).  BPT: bytes of a
 // tile per thread (64, or 32 for tiles half as long).
 template <class V, class D, int M, int THREADS, int STAGES, class OUT = OutFlat<V>, int BPT = 64>
-__global__ void __launch_bounds__(THREADS, 4)  // 4 CTAs (32 warps) per SM: <= 64 registers
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)  // 32 warps per SM: <= 64 registers
     plain_scatter_tma_kernel(PlainArgs a, D d, const __grid_constant__ CUtensorMap tmap,
                              const __grid_constant__ OUT out) {
     using L = ScatterTmaSmem<V, THREADS, STAGES, M, BPT>;

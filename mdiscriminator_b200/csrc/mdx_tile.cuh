@@ -177,7 +177,7 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[ITEMS], ui
     static_assert(M <= 2 * W, "each warp scans at most two rows");
     static_assert((M & (M - 1)) == 0, "rows paired as w and w + M/2");
     static_assert(ITEMS == 16 || ITEMS == 8 || ITEMS == 4 || ITEMS == 2, "thread elements");
-    static_assert(PER == 8, "row scans load 8 entries per lane");
+    static_assert(PER == 8 || PER == 16, "row scans load 8 or 16 entries per lane");
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t e0 = tid * ITEMS;
@@ -215,24 +215,36 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[ITEMS], ui
 
     // ---- row scans: warp w < M/2 scans rows w and w + M/2 at once, the two
     // rows' u16 counts packed in one word (row w low, row w + M/2 high; a
-    // row's sum is at most the tile, < 2^16); the other warps idle here
+    // row's sum is at most the tile, < 2^16); the other warps idle here.  A
+    // lane holds PER consecutive threads' entries (8 at 256 threads, 16 at 512)
     constexpr int H = M / 2;
+    constexpr int NV = PER / 8;  // 16-byte loads per row and lane
     const bool scans = warp < H;
-    uint32_t pre[PER];  // packed exclusive prefixes of this lane's 8 threads
+    uint32_t pre[PER];  // packed exclusive prefixes of this lane's threads
     if (scans) {
-        const uint4 xa = *reinterpret_cast<const uint4*>(cnt_sm + warp * THREADS + lane * PER);
-        const uint4 xb = *reinterpret_cast<const uint4*>(cnt_sm + (warp + H) * THREADS + lane * PER);
-        const uint32_t x[8] = {__byte_perm(xa.x, xb.x, 0x5410), __byte_perm(xa.x, xb.x, 0x7632),
-                               __byte_perm(xa.y, xb.y, 0x5410), __byte_perm(xa.y, xb.y, 0x7632),
-                               __byte_perm(xa.z, xb.z, 0x5410), __byte_perm(xa.z, xb.z, 0x7632),
-                               __byte_perm(xa.w, xb.w, 0x5410), __byte_perm(xa.w, xb.w, 0x7632)};
+        uint32_t x[PER];
+#pragma unroll
+        for (int u = 0; u < NV; u++) {
+            const uint4 xa =
+                *reinterpret_cast<const uint4*>(cnt_sm + warp * THREADS + lane * PER + 8 * u);
+            const uint4 xb =
+                *reinterpret_cast<const uint4*>(cnt_sm + (warp + H) * THREADS + lane * PER + 8 * u);
+            x[8 * u + 0] = __byte_perm(xa.x, xb.x, 0x5410);
+            x[8 * u + 1] = __byte_perm(xa.x, xb.x, 0x7632);
+            x[8 * u + 2] = __byte_perm(xa.y, xb.y, 0x5410);
+            x[8 * u + 3] = __byte_perm(xa.y, xb.y, 0x7632);
+            x[8 * u + 4] = __byte_perm(xa.z, xb.z, 0x5410);
+            x[8 * u + 5] = __byte_perm(xa.z, xb.z, 0x7632);
+            x[8 * u + 6] = __byte_perm(xa.w, xb.w, 0x5410);
+            x[8 * u + 7] = __byte_perm(xa.w, xb.w, 0x7632);
+        }
         uint32_t tot = 0;
 #pragma unroll
-        for (int q = 0; q < 8; q++) tot += x[q];
+        for (int q = 0; q < PER; q++) tot += x[q];
         const uint32_t incl = warp_incl_scan(tot);
         uint32_t run = incl - tot;
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
+        for (int q = 0; q < PER; q++) {
             pre[q] = run;
             run += x[q];
         }
@@ -258,15 +270,18 @@ __device__ __forceinline__ bool tile_scatter(const D& d, const V (&v)[ITEMS], ui
         // slots < kStageElems < 2^16: the two rows' slots stay packed
         const uint32_t add = __shfl_sync(0xffffffffu, st, warp) |
                              (__shfl_sync(0xffffffffu, st, warp + H) << 16);
-        uint32_t p[8];
 #pragma unroll
-        for (int q = 0; q < 8; q++) p[q] = pre[q] + add;
-        *reinterpret_cast<uint4*>(cnt_sm + warp * THREADS + lane * PER) =
-            make_uint4(__byte_perm(p[0], p[1], 0x5410), __byte_perm(p[2], p[3], 0x5410),
-                       __byte_perm(p[4], p[5], 0x5410), __byte_perm(p[6], p[7], 0x5410));
-        *reinterpret_cast<uint4*>(cnt_sm + (warp + H) * THREADS + lane * PER) =
-            make_uint4(__byte_perm(p[0], p[1], 0x7632), __byte_perm(p[2], p[3], 0x7632),
-                       __byte_perm(p[4], p[5], 0x7632), __byte_perm(p[6], p[7], 0x7632));
+        for (int u = 0; u < NV; u++) {
+            uint32_t p[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) p[q] = pre[8 * u + q] + add;
+            *reinterpret_cast<uint4*>(cnt_sm + warp * THREADS + lane * PER + 8 * u) =
+                make_uint4(__byte_perm(p[0], p[1], 0x5410), __byte_perm(p[2], p[3], 0x5410),
+                           __byte_perm(p[4], p[5], 0x5410), __byte_perm(p[6], p[7], 0x5410));
+            *reinterpret_cast<uint4*>(cnt_sm + (warp + H) * THREADS + lane * PER + 8 * u) =
+                make_uint4(__byte_perm(p[0], p[1], 0x7632), __byte_perm(p[2], p[3], 0x7632),
+                           __byte_perm(p[4], p[5], 0x7632), __byte_perm(p[6], p[7], 0x7632));
+        }
         if (warp == 0 && cls) {
             sh.cursor[par ^ 1u][c] = FORWARD ? cur + cc : dst;
             sh.run_start[c] = st;

@@ -19,7 +19,7 @@ def test_tuning_table_roundtrip_and_validation():
                    plain_ctas_per_sm=2)
     t = mdx.get_tuning(mdx.ELEM_U32, 7, 3000)  # m=7 -> class bound 8, log2 3000 -> 12
     assert t == {"plain_ctas_per_sm": 2, "run_tiles": 4, "group_batch": 16, "plain_two_kernel": 1,
-                 "pool_pct": 10, "mid_tiles": 1, "tile_bytes": 64}
+                 "pool_pct": 10, "mid_tiles": 1, "tile_bytes": 64, "tile_threads": 256}
     assert mdx.get_tuning(mdx.ELEM_U32, 7, 1 << 20) == other_bucket   # other bucket untouched
     assert mdx.get_tuning(mdx.ELEM_REC8, 7, 3000) == other_layout     # other element layout
     with pytest.raises(mdx.MdxError):
@@ -34,6 +34,8 @@ def test_tuning_table_roundtrip_and_validation():
         mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, mid_tiles=3)  # more than seg_mid's slab holds
     with pytest.raises(mdx.MdxError):
         mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, tile_bytes=48)  # no such tile geometry
+    with pytest.raises(mdx.MdxError):
+        mdx.set_tuning(mdx.ELEM_U32, 4, 0, 10, tile_threads=384)
     mdx.set_tuning(mdx.ELEM_U32, 5, 10, 12)  # back to the defaults
     mdx.load_tuning(mdx.TUNING_PATH, missing_ok=True)
 
@@ -79,10 +81,11 @@ def test_results_do_not_depend_on_knobs(cuda_ready, knobs):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("rec", [False, True])
-@pytest.mark.parametrize("tile_bytes", [32, 64])
-def test_tile_geometries_match_oracle(cuda_ready, tile_bytes, rec):
-    """Both tile geometries of the plain path (64 and 32 bytes of a tile per
-    thread) give the oracle's permutation, sizes and head flags: every class
+@pytest.mark.parametrize("tile_bytes,tile_threads", [(32, 256), (64, 256), (64, 512)])
+def test_tile_geometries_match_oracle(cuda_ready, tile_bytes, tile_threads, rec):
+    """Every tile geometry of the plain path (64 or 32 bytes of a tile per
+    thread at 256 threads, 64 bytes at 512 threads) gives the oracle's
+    permutation, sizes and head flags: every class
     bound (m = 2 filter step, nibble steps, warp-rank steps up to 64), one
     tile and less, a partial last tile, an unaligned input view and a length
     whose tail is not a whole 128-byte row."""
@@ -92,8 +95,10 @@ def test_tile_geometries_match_oracle(cuda_ready, tile_bytes, rec):
     try:
         for m in (2, 3, 8, 13, 16, 32, 64):
             saved[m] = mdx.get_tuning(elem, m, 1 << 20)
-            mdx.set_tuning(elem, m, 0, 33, plain_two_kernel=1, tile_bytes=tile_bytes)
-            assert mdx.get_tuning(elem, m, 1 << 20)["tile_bytes"] == tile_bytes
+            mdx.set_tuning(elem, m, 0, 33, plain_two_kernel=1, tile_bytes=tile_bytes,
+                           tile_threads=tile_threads)
+            got = mdx.get_tuning(elem, m, 1 << 20)
+            assert got["tile_bytes"] == tile_bytes and got["tile_threads"] == tile_threads
             for n, off in ((1000, 0), (2048 + 7, 0), ((1 << 20) + 5, 0), ((1 << 18) + 3, 1)):
                 x = oracle.fill_uniform_u32(n + off, 1000 * m + n)
                 if rec:
