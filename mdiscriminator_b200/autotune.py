@@ -99,6 +99,8 @@ def main(argv=None):
                 sizes = torch.empty(M, dtype=torch.uint32, device=dev)
                 best = None
                 for two, k, pool, tb, tt in PLAIN_CANDIDATES:
+                    if tt == 512 and M > 16:  # 512-thread tiles serve m <= 16 only
+                        continue
                     mdx.set_tuning(elem, M, lo, hi, plain_ctas_per_sm=k, plain_two_kernel=two,
                                    pool_pct=pool, tile_bytes=tb, tile_threads=tt)
                     ms = timeit(lambda: mdx.partition(d, ("mask", M), out=out, sizes=sizes, ws=ws),
